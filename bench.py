@@ -1,0 +1,338 @@
+'''Benchmark: semi-naive Datalog on B200 through libsrdl.
+
+Default workload (one step = one srdl_run of the plan over one input):
+  triangle  -- count-only 3-way WCOJ over an R-MAT graph, scale 20,
+               16,777,216 draws, (a,b,c,d) = (0.57,0.19,0.19,0.05), seed 3,
+               oriented x<y, deduplicated (15,701,388 edges).
+Others (--workload): tc (20k edges over 5k nodes, seed 1) and sg (windowed
+forest, n = 10,000, seed 2; the stated 200k-node forest outgrows HBM).
+
+value : tuples/s with the input already in HBM (srdl_load_device_rows),
+        CUDA events on the database stream, L2 flushed between steps.
+e2e   : same metric through the C ABI from pinned host rows (srdl_load_rows
+        + srdl_run, which uploads them), result read back to the host.
+Multi-GPU (torchrun): independent replicas, one per GPU; value = total
+tuples over the max per-rank time.
+--impl reference: the CPU restatement of the reference's evaluation on
+the host cores, on a bounded sample of the same workload.
+'''
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(REPO, 'srdatalog-python_b200'), os.path.join(REPO, 'oracle')]
+
+import numpy as np  # noqa: E402
+
+PEAKS_PATH = os.path.join(REPO, 'MEASURED_PEAKS.json')
+FALLBACK_HBM_GBS = 6650.0
+
+WORKLOADS = {
+  'triangle': dict(plan='triangle', rel='KnowsInput', out='TriangleJoin', kind='count',
+                   desc='triangle count, R-MAT scale 20, 16,777,216 draws, '
+                        '(a,b,c,d)=(0.57,0.19,0.19,0.05), seed 3, oriented x<y, dedup'),
+  'tc': dict(plan='tc', rel='ArcInput', out='Path', kind='size',
+             desc='transitive closure, 20,000 distinct uniform edges over 5,000 nodes, seed 1'),
+  'sg': dict(plan='sg', rel='Arc', out='Sg', kind='size',
+             desc='same generation, windowed forest n=10,000 (parent in [i-1000,i-1]) '
+                  '+ 10% cross edges, seed 2'),
+}
+
+
+def make_edges(name: str) -> np.ndarray:
+  from srdatalog_b200 import workloads as W
+  cache = os.path.join('/tmp', f'srdl_bench_{name}.npy')
+  if os.path.exists(cache):
+    return np.load(cache)
+  e = {'triangle': lambda: W.rmat_edges(20, 1 << 24, seed=3),
+       'tc': lambda: W.tc_small(1),
+       'sg': lambda: W.sg_forest(10000, seed=2)}[name]()
+  try:
+    np.save(cache, e)
+  except OSError:
+    pass
+  return e
+
+
+def load_plan(name: str) -> dict:
+  with open(os.path.join(REPO, 'tests', 'golden', 'plans', f'{name}.json')) as f:
+    return json.load(f)
+
+
+def result_units(db, wl) -> int:
+  return db.count(wl['out']) if wl['kind'] == 'count' else db.size(wl['out'])
+
+
+class ClockSampler:
+  '''nvidia-smi clocks + throttle reasons sampled during the timed region.'''
+
+  FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+            'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+            'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+  def __init__(self, gpu_index: int):
+    self.gpu = gpu_index
+    self.proc = None
+    self.lines: list[str] = []
+
+  def start(self):
+    try:
+      self.proc = subprocess.Popen(['nvidia-smi', f'--query-gpu={self.FIELDS}', '--format=csv,noheader,nounits',
+                                    '-i', str(self.gpu), '-lms', '200'], stdout=subprocess.PIPE,
+                                   stderr=subprocess.DEVNULL, text=True)
+      self.t = threading.Thread(target=self._read, daemon=True)
+      self.t.start()
+    except (OSError, FileNotFoundError):
+      self.proc = None
+
+  def _read(self):
+    for line in self.proc.stdout:
+      self.lines.append(line.strip())
+
+  def stop(self) -> dict:
+    if not self.proc:
+      return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+    time.sleep(0.25)
+    self.proc.terminate()
+    try:
+      self.proc.wait(timeout=5)
+    except subprocess.TimeoutExpired:
+      self.proc.kill()
+    sm, mx, reasons = [], None, set()
+    names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+    for ln in self.lines:
+      f = [x.strip() for x in ln.split(',')]
+      if len(f) < 9:
+        continue
+      try:
+        sm.append(float(f[1]))
+        mx = float(f[2])
+      except ValueError:
+        continue
+      for nm, v in zip(names, f[5:9]):
+        if v.lower() == 'active':
+          reasons.add(nm)
+    return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': mx,
+            'samples': len(sm), 'reasons': sorted(reasons)}
+
+
+def hbm_peak():
+  try:
+    with open(PEAKS_PATH) as f:
+      return float(json.load(f)['hbm_gbs']), 'measured'
+  except (OSError, KeyError, ValueError):
+    return FALLBACK_HBM_GBS, 'fallback'
+
+
+def cpu_baseline(wl_name: str, edges: np.ndarray) -> dict:
+  '''The oracle (CPU restatement of the reference's evaluation) on the host
+  cores, on a bounded sample; returns tuples/s for the same metric.'''
+  import oracle
+  cores = oracle.num_threads()
+  if wl_name == 'triangle':
+    stride = 4
+    c, t_sort, t_join = oracle.triangle_count_sample(edges, stride)
+    # full-workload estimate: one index build + stride x the sampled join
+    t_est = t_sort + stride * t_join
+    value = (c * stride) / t_est
+    sample = (f'index build over all {edges.shape[0]} edges ({t_sort:.2f} s) + join over every '
+              f'{stride}th edge ({t_join:.2f} s, {c} triangles); extrapolated x{stride}')
+  else:
+    t0 = time.perf_counter()
+    if wl_name == 'tc':
+      keys, _, _ = oracle.tc(edges)
+    else:
+      keys, _, _ = oracle.sg(edges)
+    dt = time.perf_counter() - t0
+    value = keys.shape[0] / dt
+    sample = f'full fixpoint ({dt:.2f} s, {keys.shape[0]} tuples)'
+  return {'value': value, 'unit': 'tuples/s', 'cores': cores, 'kind': 'port', 'sample': sample}
+
+
+def run_reference(args, rank, world):
+  wl = WORKLOADS[args.workload]
+  if rank != 0:
+    return
+  edges = make_edges(args.workload)
+  vals = []
+  for i in range(args.warmup + args.steps):
+    cb = cpu_baseline(args.workload, edges)
+    if i >= args.warmup:
+      vals.append(cb['value'])
+  v = statistics.median(vals)
+  cb['value'] = v
+  line = {'impl': 'reference', 'metric': f'tuples/s ({args.workload})', 'value': v,
+          'unit': 'tuples/s', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+          'ms_per_step': None, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+          'dtype': 'u32', 'data': 'synthetic',
+          'config': {'workload': wl['desc']}, 'cpu_baseline': cb,
+          'e2e': {'value': v, 'unit': 'tuples/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+  print(json.dumps(line), flush=True)
+
+
+def main():
+  ap = argparse.ArgumentParser()
+  ap.add_argument('--gpus', type=int, default=1)
+  ap.add_argument('--steps', type=int, default=10)
+  ap.add_argument('--warmup', type=int, default=3)
+  ap.add_argument('--impl', default='srdl', choices=['srdl', 'reference'])
+  ap.add_argument('--workload', default='triangle', choices=sorted(WORKLOADS))
+  ap.add_argument('--no-cpu-baseline', action='store_true')
+  args = ap.parse_args()
+  args.warmup = max(args.warmup, 3)
+
+  rank = int(os.environ.get('RANK', '0'))
+  world = int(os.environ.get('WORLD_SIZE', '1'))
+  local = int(os.environ.get('LOCAL_RANK', '0'))
+  if args.impl == 'reference':
+    return run_reference(args, rank, world)
+
+  import torch
+  dist = None
+  if world > 1:
+    import datetime
+
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+  dev = torch.device('cuda', local)
+  torch.cuda.set_device(dev)
+
+  from srdatalog_b200 import Database, native
+  wl = WORKLOADS[args.workload]
+  plan = load_plan(wl['plan'])
+  edges = make_edges(args.workload)
+  n = edges.shape[0]
+  stream = torch.cuda.current_stream(dev)
+
+  # ---------------- kernel-resident path (value)
+  d_edges = torch.from_numpy(edges.view(np.int32).reshape(-1)).to(dev)
+  db = Database(plan, device=local)
+  db.set_stream(stream.cuda_stream)
+  db.load_device_rows(wl['rel'], d_edges.data_ptr(), n)
+  db.set_profiling(True)
+  flush = torch.empty(64 << 20, dtype=torch.int32, device=dev)  # 256 MB > 126 MB L2
+  for _ in range(args.warmup):
+    db.run()
+  units = result_units(db, wl)
+  kernels: dict = {}
+  step_ms = []
+  launches = 0
+  sampler = ClockSampler(local)
+  if dist:
+    dist.barrier()
+  torch.cuda.synchronize(dev)
+  sampler.start()
+  for i in range(args.steps):
+    flush.fill_(i)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = native.lib().srdl_launch_count()
+    ev0.record(stream)
+    db.run()
+    ev1.record(stream)
+    ev1.synchronize()
+    launches += native.lib().srdl_launch_count() - l0
+    step_ms.append(ev0.elapsed_time(ev1))
+    for k, s in db.stats()['kernels'].items():
+      agg = kernels.setdefault(k, {'ms': 0.0, 'bytes': 0.0, 'units': 0.0, 'scopes': 0})
+      for f in agg:
+        agg[f] += s[f]
+    assert result_units(db, wl) == units
+  torch.cuda.synchronize(dev)
+  clocks = sampler.stop()
+  if dist:
+    dist.barrier()
+  total_ms = sum(step_ms)
+  if dist:
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+  value = units * args.steps * world / (total_ms / 1e3)
+  stats = db.stats()
+  db.close()
+  del d_edges
+
+  # ---------------- end-to-end path through the C ABI with host inputs (e2e)
+  db2 = Database(plan, device=local)
+  db2.set_stream(stream.cuda_stream)
+  db2.load_rows(wl['rel'], edges)
+  for _ in range(args.warmup):
+    db2.run()
+  e2e_ms = []
+  if dist:
+    dist.barrier()
+  torch.cuda.synchronize(dev)
+  for i in range(args.steps):
+    flush.fill_(i)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    db2.run()
+    got = result_units(db2, wl)  # result read back to the host
+    ev1.record(stream)
+    ev1.synchronize()
+    e2e_ms.append(ev0.elapsed_time(ev1))
+    assert got == units
+  e2e_total = sum(e2e_ms)
+  if dist:
+    t = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_total = float(t.item())
+  db2.close()
+
+  if dist:
+    dist.barrier()
+    dist.destroy_process_group()
+  if rank != 0:
+    return
+
+  # ---------------- roofline of the dominant kernel family
+  top = max(kernels.items(), key=lambda kv: kv[1]['ms'])
+  name, k = top
+  peak, peak_kind = hbm_peak()
+  achieved = (k['bytes'] / (k['ms'] / 1e3)) / 1e9 if k['ms'] else 0.0
+  traffic = None
+  prof = os.path.join(REPO, 'profiles', 'traffic.json')
+  if os.path.exists(prof):
+    tr = json.load(open(prof)).get(args.workload, {}).get(name)
+    if tr:
+      traffic = tr['dram_bytes_per_unit'] * k['units'] / max(1, k['scopes'])
+  roof = {'bound': 'hbm', 'kernel': name, 'achieved': achieved, 'peak': peak,
+          'peak_source': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
+          'traffic': traffic, 'bytes_per_launch': k['bytes'] / max(1, k['scopes']),
+          'ms_per_launch': k['ms'] / max(1, k['scopes']),
+          'share_of_step': k['ms'] / total_ms if world == 1 else None}
+  line = {
+    'metric': f'tuples/s ({args.workload})', 'value': value, 'unit': 'tuples/s', 'n_gpus': world,
+    'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
+    'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'u32',
+    'data': 'synthetic',
+    'config': {'workload': wl['desc'], 'edges': int(n), 'tuples_per_step': int(units),
+               'parallelism': f'replicas{world}', 'l2': 'flushed between steps (256 MB write)',
+               'inputs': 'HBM-resident for value; pinned host rows for e2e'},
+    'e2e': {'value': units * args.steps * world / (e2e_total / 1e3), 'unit': 'tuples/s',
+            'ms_per_step': e2e_total / args.steps, 'h2d_bytes_per_step': int(n) * 8,
+            'd2h_bytes_per_step': 8},
+    'gpu_launches': int(launches),
+    'roofline': roof,
+    'kernels': {k2: {'ms_per_step': v['ms'] / args.steps,
+                     'gbs': (v['bytes'] / (v['ms'] / 1e3) / 1e9) if v['ms'] else 0.0}
+                for k2, v in sorted(kernels.items(), key=lambda kv: -kv[1]['ms'])},
+    'iterations': [s['iterations'] for s in stats['steps']],
+    'clocks': clocks,
+  }
+  if world == 1 and not args.no_cpu_baseline:
+    line['cpu_baseline'] = cpu_baseline(args.workload, edges)
+  print(json.dumps(line), flush=True)
+
+
+if __name__ == '__main__':
+  main()

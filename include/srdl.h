@@ -1,0 +1,149 @@
+/*
+ * srdl.h -- C ABI of libsrdl, the sm_100a semi-naive Datalog runtime.
+ *
+ * Plain pointers and sizes only.  All functions return 0 on success unless
+ * stated otherwise; on failure srdl_last_error() describes the error of the
+ * calling thread.  Status codes: 1 bad argument, 2 bad state, 3 CUDA error,
+ * 4 malformed plan, 5 capacity exceeded, 6 I/O error, 7 unsupported
+ * construct, 8 timed out.
+ *
+ * Two layers:
+ *  - database handles (srdl_open ... srdl_close) that interpret a plan JSON
+ *    produced from the srdatalog MIR; the per-program shim emitted by
+ *    srdatalog_b200.build_project wraps one handle behind the reference's
+ *    srdatalog_* names;
+ *  - stream-ordered, allocation-free kernel primitives on device pointers
+ *    (index build, delta, merge) for callers that keep their own relations.
+ */
+#ifndef SRDL_H
+#define SRDL_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SRDL_ABI_VERSION 1
+
+typedef struct srdl_db srdl_db;
+
+/* Message for the last failed call on this thread (never NULL). */
+const char* srdl_last_error(void);
+int srdl_version(void);
+
+/* Parse a plan and create a database bound to CUDA device `device`.  No GPU
+ * work happens until srdl_init_device / srdl_run.  Replaces the
+ * per-program SemiNaiveDatabase the generated shim allocates lazily
+ * (src/srdatalog/codegen/jit/main_file.py:680-695). */
+int srdl_open(const char* plan_json, int device, srdl_db** out);
+
+/* Free every host and device resource of the database.  Replaces
+ * srdatalog_shutdown (main_file.py:772-775). */
+int srdl_close(srdl_db* db);
+
+/* Select the device, create the stream and memory pool.  Replaces
+ * srdatalog_init -> SRDatalog::GPU::init_cuda (main_file.py:683-688;
+ * RT/gpu/init.h:50). */
+int srdl_init_device(srdl_db* db);
+
+/* Stage n_rows row-major uint32 rows of an input relation (host memory;
+ * copied to the device by srdl_run).  No reference counterpart: the
+ * reference only loads files. */
+int srdl_load_rows(srdl_db* db, const char* rel, const uint32_t* rows, uint64_t n_rows);
+
+/* Stage one CSV file for an input relation.  Replaces srdatalog_load_csv
+ * (main_file.py:690-727) -> SRDatalog::load_from_file (RT/runtime/io.h:384). */
+int srdl_load_csv(srdl_db* db, const char* rel, const char* path);
+
+/* Stage `dir`/<input_file> for every input relation.  Replaces
+ * srdatalog_load_all -> <Runner>::load_data (main_file.py:729-741, 204-213). */
+int srdl_load_all(srdl_db* db, const char* dir);
+
+/* Stage n_rows row-major uint32 pairs that already live in device memory
+ * (binary input relations only).  They are copied once, on the database's
+ * stream; srdl_run then starts from HBM-resident inputs.  No reference
+ * counterpart. */
+int srdl_load_device_rows(srdl_db* db, const char* rel, const uint32_t* d_rows, uint64_t n_rows);
+
+/* Launch all further work of `db` on `stream` (a cudaStream_t owned by the
+ * caller, who keeps it alive until srdl_close); device state of earlier runs
+ * is released first.  No reference counterpart. */
+int srdl_set_stream(srdl_db* db, void* stream);
+
+/* Record CUDA events around every kernel family of srdl_run and report their
+ * device time and algorithmic bytes in srdl_stats_json ("kernels"). */
+int srdl_set_profiling(srdl_db* db, int enable);
+
+/* Kernels this process has launched through libsrdl so far. */
+uint64_t srdl_launch_count(void);
+
+/* Rows currently staged for `rel` by the load calls (host-side count). */
+uint64_t srdl_staged_rows(srdl_db* db, const char* rel);
+
+/* Copy staged inputs to the device and evaluate the plan; recursive strata
+ * stop at an empty delta or after max_iters iterations (0 = unlimited).
+ * Results stay on the device until the next run or srdl_close.  Replaces
+ * srdatalog_run (main_file.py:743-753) -> copy_host_to_device
+ * (RT/gpu/runtime/query.h:107) + <Runner>::run. */
+int srdl_run(srdl_db* db, uint64_t max_iters);
+
+/* Rows in the FULL version of `rel` (canonical index).  Replaces
+ * srdatalog_size (main_file.py:755-767), which read the host DB. */
+uint64_t srdl_size(srdl_db* db, const char* rel);
+
+/* Bindings counted by a count-only rule (with_count) in the last run.
+ * Replaces the ">>>> <Rule> count: N" stdout line of the generated runner
+ * (tests/fixtures/jit/lsqb_triangle_count/orchestrator.cpp:40-47). */
+uint64_t srdl_count(srdl_db* db, const char* rule);
+
+/* Copy up to cap_rows rows of FULL(rel) into out_rows (row-major uint32, in
+ * declared column order, lexicographically sorted) and return the total
+ * row count (negative status on error; out_rows may be NULL to query the
+ * size).  No reference counterpart: the reference cannot read results back. */
+int64_t srdl_dump(srdl_db* db, const char* rel, uint32_t* out_rows, uint64_t cap_rows);
+
+/* JSON run statistics (iterations per step, timings, derived rows). */
+int srdl_stats_json(srdl_db* db, char* buf, uint64_t cap);
+
+/* ------------------------------------------------------------------------
+ * Kernel primitives.  Keys are uint64 = (index column 0 << 32) | column 1;
+ * every value must be < 2^value_bits.  Pointers are device pointers, work
+ * is enqueued on `stream` (a cudaStream_t, NULL = legacy default stream),
+ * the result count is written to device memory, and nothing is allocated:
+ * temporaries live in the caller's scratch region.
+ * ---------------------------------------------------------------------- */
+
+/* Scratch bytes srdl_sort_unique_u64 needs for n keys. */
+uint64_t srdl_sort_unique_scratch_bytes(uint64_t n, int value_bits);
+
+/* Sort n keys ascending and drop duplicates: d_out gets the distinct keys,
+ * *d_n_out their count.  d_out needs room for n keys and may alias d_in.
+ * Replaces rebuild_index_fn (RT/gpu/runtime/gpu_mir_helpers.h:204-232) ->
+ * zip_sort_columns (RT/gpu/sort.h:297-302) + deduplicate_aggregate_and_unique
+ * (RT/gpu/deduplication.h:178-258). */
+int srdl_sort_unique_u64(const uint64_t* d_in, uint64_t n, int value_bits, uint64_t* d_out,
+                         uint64_t* d_n_out, void* d_scratch, uint64_t scratch_bytes,
+                         void* stream);
+
+/* Scratch bytes srdl_set_difference_u64 needs for na keys of `a`. */
+uint64_t srdl_set_difference_scratch_bytes(uint64_t na);
+
+/* d_out = a - b for sorted duplicate-free arrays; *d_n_out = |d_out|.
+ * Replaces compute_delta_index_fn (gpu_mir_helpers.h:88-122) ->
+ * DSAI::set_difference_update (RT/gpu/device_sorted_array_index.ipp:966-1130). */
+int srdl_set_difference_u64(const uint64_t* d_a, uint64_t na, const uint64_t* d_b, uint64_t nb,
+                            uint64_t* d_out, uint64_t* d_n_out, void* d_scratch,
+                            uint64_t scratch_bytes, void* stream);
+
+/* d_out = a U b for disjoint sorted duplicate-free arrays (na + nb keys).
+ * Replaces merge_index_fn (gpu_mir_helpers.h:136-159) -> DSAI::merge
+ * (RT/gpu/device_sorted_array_index.ipp:709-847). */
+int srdl_merge_u64(const uint64_t* d_a, uint64_t na, const uint64_t* d_b, uint64_t nb,
+                   uint64_t* d_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SRDL_H */

@@ -1,0 +1,296 @@
+'''Python side of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline /
+reference arm import this module.  The product never routes through it.
+
+Parity status: UNPINNED against the reference's own outputs (the
+reference ships no tuple-level golden vectors and its runtime cannot be
+built here).  Pins used instead: known-answer graphs and an independent
+linear-algebra restatement (tests/test_oracle.py).
+
+Two restatements of the reference's semi-naive evaluation live here:
+
+* `liboracle.so` (oracle.c): fast C/OpenMP evaluators for the TC, SG and
+  triangle plans, plus sort+unique / set difference / merge.
+* `run_plan`: a small pure-Python interpreter for ANY plan this runtime
+  accepts, for tiny inputs; it walks the MIR op sequence literally
+  (src/srdatalog/hir/lower.py:442-789) with Python sets.
+'''
+
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import itertools
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+class _Result(ctypes.Structure):
+  _fields_ = [('keys', ctypes.POINTER(ctypes.c_uint64)), ('n', ctypes.c_uint64),
+              ('iterations', ctypes.c_uint64), ('derived', ctypes.c_uint64)]
+
+
+def build() -> str:
+  path = os.path.join(HERE, 'liboracle.so')
+  src = os.path.join(HERE, 'oracle.c')
+  if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+    subprocess.run(['make', '-s', '-C', HERE], check=True)
+  return path
+
+
+def lib():
+  global _LIB
+  if _LIB is None:
+    L = ctypes.CDLL(build())
+    u64, p64 = ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)
+    L.orc_sort_unique_u64.argtypes = [p64, u64]
+    L.orc_sort_unique_u64.restype = u64
+    L.orc_set_difference_u64.argtypes = [p64, u64, p64, u64, p64]
+    L.orc_set_difference_u64.restype = u64
+    L.orc_merge_u64.argtypes = [p64, u64, p64, u64, p64]
+    L.orc_merge_u64.restype = u64
+    for f in (L.orc_tc, L.orc_sg):
+      f.argtypes = [p64, u64, u64, ctypes.POINTER(_Result)]
+      f.restype = ctypes.c_int
+    L.orc_triangle_count.argtypes = [p64, u64]
+    L.orc_triangle_count.restype = u64
+    L.orc_triangle_count_sample.argtypes = [p64, u64, u64, u64, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_double)]
+    L.orc_triangle_count_sample.restype = u64
+    L.orc_free.argtypes = [ctypes.c_void_p]
+    L.orc_num_threads.restype = ctypes.c_int
+    _LIB = L
+  return _LIB
+
+
+def _p64(a: np.ndarray):
+  return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+
+def pack(edges: np.ndarray, order=(0, 1)) -> np.ndarray:
+  '''(m,2) uint32 rows -> uint64 keys in the given index column order.'''
+  e = np.asarray(edges, dtype=np.uint32)
+  return (e[:, order[0]].astype(np.uint64) << np.uint64(32)) | e[:, order[1]].astype(np.uint64)
+
+
+def unpack(keys: np.ndarray, order=(0, 1)) -> np.ndarray:
+  '''uint64 keys in index order -> (n,2) uint32 rows in declared column order.'''
+  k = np.asarray(keys, dtype=np.uint64)
+  out = np.empty((k.shape[0], 2), np.uint32)
+  out[:, order[0]] = (k >> np.uint64(32)).astype(np.uint32)
+  out[:, order[1]] = (k & np.uint64(0xffffffff)).astype(np.uint32)
+  return out
+
+
+def sort_unique(keys: np.ndarray) -> np.ndarray:
+  a = np.array(keys, dtype=np.uint64, copy=True)
+  n = lib().orc_sort_unique_u64(_p64(a), a.shape[0])
+  return a[:n]
+
+
+def set_difference(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+  a = np.ascontiguousarray(a, np.uint64)
+  b = np.ascontiguousarray(b, np.uint64)
+  out = np.empty(max(1, a.shape[0]), np.uint64)
+  n = lib().orc_set_difference_u64(_p64(a), a.shape[0], _p64(b), b.shape[0], _p64(out))
+  return out[:n]
+
+
+def merge(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+  a = np.ascontiguousarray(a, np.uint64)
+  b = np.ascontiguousarray(b, np.uint64)
+  out = np.empty(max(1, a.shape[0] + b.shape[0]), np.uint64)
+  n = lib().orc_merge_u64(_p64(a), a.shape[0], _p64(b), b.shape[0], _p64(out))
+  return out[:n]
+
+
+def _run(fn, edges: np.ndarray, max_iters: int):
+  keys = np.ascontiguousarray(pack(edges), np.uint64)
+  r = _Result()
+  rc = fn(_p64(keys), keys.shape[0], max_iters or (2**31 - 1), ctypes.byref(r))
+  if rc != 0:
+    raise RuntimeError(f'oracle failed: {rc}')
+  out = np.ctypeslib.as_array(r.keys, shape=(r.n,)).copy() if r.n else np.zeros(0, np.uint64)
+  lib().orc_free(ctypes.cast(r.keys, ctypes.c_void_p))
+  return out, int(r.iterations), int(r.derived)
+
+
+def tc(edges: np.ndarray, max_iters: int = 0):
+  '''Path relation keys in canonical index order (1,0), iterations, derived rows.'''
+  return _run(lib().orc_tc, edges, max_iters)
+
+
+def sg(edges: np.ndarray, max_iters: int = 0):
+  '''Sg relation keys in canonical index order (0,1), iterations, derived rows.'''
+  return _run(lib().orc_sg, edges, max_iters)
+
+
+def triangle_count(edges: np.ndarray) -> int:
+  keys = np.ascontiguousarray(pack(edges), np.uint64)
+  return int(lib().orc_triangle_count(_p64(keys), keys.shape[0]))
+
+
+def triangle_count_sample(edges: np.ndarray, stride: int, phase: int = 0):
+  '''(sampled count, sort seconds, sampled-join seconds) over every stride-th edge.'''
+  keys = np.ascontiguousarray(pack(edges), np.uint64)
+  ts, tj = ctypes.c_double(), ctypes.c_double()
+  c = lib().orc_triangle_count_sample(_p64(keys), keys.shape[0], stride, phase, ctypes.byref(ts),
+                                      ctypes.byref(tj))
+  return int(c), ts.value, tj.value
+
+
+def num_threads() -> int:
+  return int(lib().orc_num_threads())
+
+
+def dump_hash(rows: np.ndarray) -> str:
+  '''SHA-256 of a relation dump: rows sorted lexicographically in declared
+  column order, serialised row-major as little-endian uint32.'''
+  r = np.ascontiguousarray(rows, dtype='<u4')
+  if r.shape[0]:
+    order = np.lexsort(tuple(r[:, c] for c in reversed(range(r.shape[1]))))
+    r = np.ascontiguousarray(r[order])
+  return hashlib.sha256(r.tobytes()).hexdigest()
+
+
+# ---------------------------------------------------------------------------
+# Generic pure-Python plan interpreter (tiny inputs only)
+# ---------------------------------------------------------------------------
+
+def _filter_fn(code: str):
+  import re
+  body = code.strip()[len('return'):-1].strip()
+  terms = []
+  for part in body.split('&&'):
+    m = re.match(r'^\(?\s*(\w+)\s*(!=|==|<=|>=|<|>)\s*(\w+)\s*\)?$', part.strip())
+    if not m:
+      raise ValueError(f'unsupported filter {code!r}')
+    terms.append(m.groups())
+  ops = {'!=': lambda a, b: a != b, '==': lambda a, b: a == b, '<': lambda a, b: a < b,
+         '<=': lambda a, b: a <= b, '>': lambda a, b: a > b, '>=': lambda a, b: a >= b}
+
+  def ev(bind):
+    def val(t):
+      return int(t) if t.isdigit() else bind[t]
+    return all(ops[o](val(a), val(b)) for a, o, b in terms)
+  return ev
+
+
+def run_plan(plan: dict, inputs: dict, max_iters: int = 0):
+  '''Evaluate `plan` over `inputs` ({relation: (m,k) uint32 rows}).
+
+  Returns ({relation: sorted list of tuples in declared column order},
+  {rule: count} for count-only rules).  Semantics:
+  insert_into adds to NEW; rebuild_index dedups NEW; compute_delta_index
+  sets DELTA = NEW - FULL (gpu_mir_helpers.h:88-122); merge_index sets
+  FULL |= DELTA (gpu_mir_helpers.h:136-159); recursive steps loop until
+  the delta of every relation the step computes is empty, iteration 0
+  reading FULL for DELTA (gpu_mir_helpers.h:419-426).
+  '''
+  rels = {r['name']: r for r in plan['relations']}
+  db = {(n, v): set() for n in rels for v in ('FULL', 'DELTA', 'NEW')}
+  for name, rows in inputs.items():
+    db[(name, 'FULL')] = {tuple(int(x) for x in r) for r in np.asarray(rows).reshape(-1, rels[name]['arity'])}
+  counts: dict[str, int] = {}
+  cap = max_iters or (2**31 - 1)
+
+  def values(src, bind, iteration):
+    ver = src['ver']
+    if ver == 'DELTA' and iteration == 0:
+      ver = 'FULL'
+    idx = src['index']
+    pre = [bind[v] for v in src['prefix']]
+    col = idx[len(pre)]
+    out = set()
+    for t in db[(src['rel'], ver)]:
+      if all(t[idx[i]] == pre[i] for i in range(len(pre))):
+        out.add(t[col])
+    return out
+
+  def execute(op, iteration):
+    binds = [dict()]
+    for p in op['pipeline']:
+      k = p['op']
+      nb = []
+      if k == 'scan':
+        for b in binds:
+          ver = 'FULL' if (p['ver'] == 'DELTA' and iteration == 0) else p['ver']
+          for t in db[(p['rel'], ver)]:
+            c = dict(b)
+            ok = True
+            # Scan vars follow the index's access order (generate_scan,
+            # src/srdatalog/hir/lower.py:46-60): vars[j] <-> column index[j].
+            for j, v in enumerate(p['vars']):
+              val = t[p['index'][j]]
+              if v in c and c[v] != val:
+                ok = False
+              c[v] = val
+            if ok:
+              nb.append(c)
+      elif k == 'column_join':
+        for b in binds:
+          vs = None
+          for s in p['sources']:
+            x = values(s, b, iteration)
+            vs = x if vs is None else (vs & x)
+          for v in sorted(vs):
+            c = dict(b)
+            c[p['var']] = v
+            nb.append(c)
+      elif k == 'cartesian_join':
+        for b in binds:
+          lists = []
+          for s, vars_ in zip(p['sources'], p['var_from_source']):
+            if vars_:
+              lists.append((vars_[0], sorted(values(s, b, iteration))))
+          for combo in itertools.product(*[lst for _, lst in lists]):
+            c = dict(b)
+            for (v, _), val in zip(lists, combo):
+              c[v] = val
+            nb.append(c)
+      elif k == 'filter':
+        ev = _filter_fn(p['code'])
+        nb = [b for b in binds if ev(b)]
+      elif k == 'insert_into':
+        if op['count']:
+          counts[op['rule']] = counts.get(op['rule'], 0) + len(binds)
+        else:
+          tgt = db[(p['rel'], 'NEW')]
+          for b in binds:
+            tgt.add(tuple(b[v] for v in p['vars']))
+        nb = binds
+      binds = nb
+
+  def run_ops(ops, iteration):
+    for op in ops:
+      k = op['op']
+      if k == 'execute_pipeline':
+        execute(op, iteration)
+      elif k == 'compute_delta_index':
+        db[(op['rel'], 'DELTA')] = db[(op['rel'], 'NEW')] - db[(op['rel'], 'FULL')]
+      elif k == 'merge_index':
+        db[(op['rel'], 'FULL')] = db[(op['rel'], 'FULL')] | db[(op['rel'], 'DELTA')]
+      elif k == 'clear_relation':
+        if op['ver'] == 'NEW':
+          db[(op['rel'], 'NEW')] = set()
+        # DELTA is cleared right before compute_delta_index overwrites it
+        # (lower.py: ClearRelation(DELTA) precedes ComputeDeltaIndex).
+
+  for step in plan['steps']:
+    ops = step['ops']
+    if not step['recursive']:
+      run_ops(ops, 0)
+      continue
+    computed = {op['rel'] for op in ops if op['op'] == 'compute_delta_index'}
+    for it in range(cap):
+      if it > 0 and sum(len(db[(r, 'DELTA')]) for r in computed) == 0:
+        break
+      run_ops(ops, it)
+  out = {n: sorted(db[(n, 'FULL')]) for n in rels}
+  return out, counts

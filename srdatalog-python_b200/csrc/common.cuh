@@ -1,0 +1,171 @@
+// common.cuh -- shared definitions for the srdl sm_100a runtime.
+//
+// Data layout in HBM.  Every materialised relation version holds ONE
+// sorted, duplicate-free array of uint64 keys per index permutation:
+//     key = (value of index column 0) << 32 | (value of index column 1)
+// which is the lexicographic order of the reference's column-major sorted
+// arrays (src/srdatalog/runtime/generalized_datalog/gpu/device_sorted_array_index.h:337).
+// Joins additionally read a "trie view" of an index: the child column as a
+// dense uint32 array, the distinct first-column values (roots) and, when the
+// value domain is small, a dense directory dir[v] = first row whose first
+// column is >= v, so that the rows with prefix v are [dir[v], dir[v+1]).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+namespace srdl {
+
+constexpr int kWarp = 32;
+constexpr unsigned kAllLanes = 0xffffffffu;
+
+// Status codes returned through the C ABI.
+enum Status : int {
+  kOk = 0,
+  kErrArg = 1,
+  kErrState = 2,
+  kErrCuda = 3,
+  kErrPlan = 4,
+  kErrCapacity = 5,
+  kErrIo = 6,
+  kErrUnsupported = 7,
+  kErrTimeout = 8,
+};
+
+void set_error(const std::string& msg);
+const char* last_error();
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define SRDL_CUDA(call)                                                             \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess)                                                          \
+      throw ::srdl::Error{::srdl::kErrCuda, std::string(#call) + ": " +             \
+                                                cudaGetErrorString(e_) + " at " +   \
+                                                __FILE__ + ":" + std::to_string(__LINE__)}; \
+  } while (0)
+
+#define SRDL_REQUIRE(cond, code, msg)                                 \
+  do {                                                                \
+    if (!(cond)) throw ::srdl::Error{(code), std::string(msg)};       \
+  } while (0)
+
+// Read-only view of one sorted index used by the join kernels.
+struct TrieView {
+  const uint64_t* keys = nullptr;   // n sorted unique keys
+  const uint32_t* lo = nullptr;     // n child values (low words of keys)
+  const uint32_t* roots = nullptr;  // n_roots distinct first-column values
+  const uint32_t* dir = nullptr;    // dense directory, dir_n = domain + 2 entries, or null
+  uint64_t n = 0;
+  uint32_t n_roots = 0;
+  uint32_t dir_n = 0;
+  int arity = 2;
+};
+
+__device__ __forceinline__ uint64_t lower_bound_u64(const uint64_t* a, uint64_t lo,
+                                                    uint64_t hi, uint64_t key) {
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) >> 1;
+    if (a[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t lo,
+                                                    uint32_t hi, uint32_t key) {
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Rows whose first index column equals v: [b, e).  Same contract as
+// NodeHandle::prefix (RT/gpu/device_sorted_array_index.ipp:67-157) for a
+// two-column index.
+__device__ __forceinline__ void trie_range(const TrieView& t, uint32_t v, uint32_t& b,
+                                           uint32_t& e) {
+  if (t.dir) {
+    if (v + 1u < t.dir_n) {
+      b = t.dir[v];
+      e = t.dir[v + 1];
+    } else {
+      b = e = 0;
+    }
+  } else {
+    uint64_t k0 = (uint64_t)v << 32;
+    b = (uint32_t)lower_bound_u64(t.keys, 0, t.n, k0);
+    e = (v == 0xffffffffu) ? (uint32_t)t.n
+                           : (uint32_t)lower_bound_u64(t.keys, b, t.n, k0 + (1ull << 32));
+  }
+}
+
+__device__ __forceinline__ bool trie_has_root(const TrieView& t, uint32_t v) {
+  uint32_t b, e;
+  trie_range(t, v, b, e);
+  return b < e;
+}
+
+// Is v among child values lo[b..e)?
+__device__ __forceinline__ bool child_contains(const TrieView& t, uint32_t b, uint32_t e,
+                                               uint32_t v) {
+  uint32_t p = lower_bound_u32(t.lo, b, e, v);
+  return p < e && t.lo[p] == v;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    T y = __shfl_up_sync(kAllLanes, v, d);
+    if (lane >= d) v += y;
+  }
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(kAllLanes, v, d);
+  return v;
+}
+
+// Exclusive block scan; `sh` must hold blockDim.x/32 + 1 elements.  Returns
+// the exclusive prefix of v and writes the block total into *total.
+template <typename T>
+__device__ __forceinline__ T block_excl_scan(T v, T* sh, T* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  T inc = warp_incl_scan(v);
+  if (lane == 31) sh[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    T s = lane < nw ? sh[lane] : T(0);
+    T si = warp_incl_scan(s);
+    if (lane < nw) sh[lane] = si - s;
+    if (lane == nw - 1) sh[nw] = si;
+  }
+  __syncthreads();
+  T r = sh[wid] + inc - v;
+  *total = sh[nw];
+  __syncthreads();
+  return r;
+}
+
+inline int div_up(uint64_t a, uint64_t b) { return (int)((a + b - 1) / b); }
+
+}  // namespace srdl

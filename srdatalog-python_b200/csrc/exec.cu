@@ -1,0 +1,467 @@
+// exec.cu -- Database: pipeline execution, maintenance ops, fixpoint loop.
+//
+// Op semantics follow the reference's MIR helpers:
+//   rebuild_index      RT/gpu/runtime/gpu_mir_helpers.h:204-232
+//   compute_delta_index gpu_mir_helpers.h:88-122   (DELTA = NEW - FULL)
+//   merge_index        gpu_mir_helpers.h:136-159   (FULL |= DELTA)
+//   clear_relation     gpu_mir_helpers.h:308
+//   iteration-0 DELTA reads go to FULL           gpu_mir_helpers.h:419-426
+//   loop: stop when the summed delta is empty, at most max_iters joins
+//         (src/srdatalog/codegen/jit/orchestrator_jit.py:600-747).
+// When a rebuild of NEW is followed only by check_size / clear(DELTA) before
+// the compute_delta_index of the same relation, the sort's dedup pass also
+// drops the keys already in FULL, so NEW is never written out separately.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <sstream>
+
+#include "runtime.h"
+
+namespace srdl {
+
+namespace {
+
+struct FilterTerm {
+  std::string a, b;
+  int op;
+};
+
+bool is_uint(const std::string& s) {
+  if (s.empty()) return false;
+  for (char c : s)
+    if (c < '0' || c > '9') return false;
+  return true;
+}
+
+std::string trim(const std::string& s) {
+  size_t b = s.find_first_not_of(" \t\n()"), e = s.find_last_not_of(" \t\n()");
+  return b == std::string::npos ? std::string() : s.substr(b, e - b + 1);
+}
+
+// Restricted filter grammar: "return a OP b && c OP d ...;" with bound
+// variables or unsigned constants.  The reference pastes the C++ body into
+// the generated kernel; anything outside this grammar is rejected.
+std::vector<FilterTerm> parse_filter(const std::string& code) {
+  std::string s = trim(code);
+  SRDL_REQUIRE(s.rfind("return", 0) == 0 && !s.empty() && s.back() == ';', kErrUnsupported,
+               "filter '" + code + "': expected 'return <expr>;'");
+  s = s.substr(6, s.size() - 7);
+  std::vector<FilterTerm> out;
+  size_t p = 0;
+  while (true) {
+    size_t q = s.find("&&", p);
+    std::string part = trim(s.substr(p, q == std::string::npos ? std::string::npos : q - p));
+    static const char* ops[] = {"!=", "==", "<=", ">=", "<", ">"};
+    static const int codes[] = {kNe, kEq, kLe, kGe, kLt, kGt};
+    bool found = false;
+    for (int k = 0; k < 6 && !found; k++) {
+      size_t at = part.find(ops[k]);
+      if (at == std::string::npos) continue;
+      out.push_back({trim(part.substr(0, at)), trim(part.substr(at + strlen(ops[k]))), codes[k]});
+      found = true;
+    }
+    SRDL_REQUIRE(found, kErrUnsupported, "filter '" + code + "': unsupported term '" + part + "'");
+    if (q == std::string::npos) break;
+    p = q + 2;
+  }
+  return out;
+}
+
+}  // namespace
+
+void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
+  std::map<std::string, int> slot;
+  int nslots = 0;
+  auto bind = [&](const std::string& v) {
+    SRDL_REQUIRE(!slot.count(v), kErrUnsupported, "rule " + op.rule + ": variable " + v + " bound twice");
+    SRDL_REQUIRE(nslots < kMaxSlots, kErrUnsupported, "rule " + op.rule + ": too many variables");
+    slot[v] = nslots++;
+    return slot[v];
+  };
+  auto slot_of = [&](const std::string& v) {
+    auto it = slot.find(v);
+    SRDL_REQUIRE(it != slot.end(), kErrPlan, "rule " + op.rule + ": unbound variable " + v);
+    return it->second;
+  };
+  auto make_src = [&](const SourceDesc& d) {
+    Relation& r = rel(d.rel);
+    Ver v = (d.ver == kDelta && recursive && iteration == 0) ? kFull : d.ver;
+    SRDL_REQUIRE(r.arity <= 2, kErrUnsupported, "join over relation " + r.name + " of arity > 2");
+    SRDL_REQUIRE(d.prefix.size() < (size_t)std::max(r.arity, 2), kErrUnsupported,
+                 "rule " + op.rule + ": prefix too long on " + r.name);
+    Index& ix = ensure_index(r, v, d.index);
+    SrcSpec s;
+    s.t = view(r, ix);
+    s.prefix_slot = d.prefix.empty() ? -1 : slot_of(d.prefix[0]);
+    return s;
+  };
+
+  std::vector<LevelSpec> levels;
+  const PipeOp* insert = nullptr;
+  for (const PipeOp& po : op.pipeline) {
+    if (po.kind == PipeOp::Filter) {
+      SRDL_REQUIRE(!levels.empty(), kErrPlan, "rule " + op.rule + ": filter before any join");
+      LevelSpec& lv = levels.back();
+      for (auto& t : parse_filter(po.code)) {
+        SRDL_REQUIRE(lv.nfilt < kMaxFilt, kErrUnsupported, "too many filter terms");
+        FiltSpec f;
+        f.op = t.op;
+        if (is_uint(t.a)) f.a_const = (uint32_t)std::stoul(t.a); else f.a_slot = slot_of(t.a);
+        if (is_uint(t.b)) f.b_const = (uint32_t)std::stoul(t.b); else f.b_slot = slot_of(t.b);
+        lv.filt[lv.nfilt++] = f;
+      }
+      continue;
+    }
+    if (po.kind == PipeOp::Insert) {
+      insert = &po;
+      continue;
+    }
+    LevelSpec lv;
+    lv.n_in_slots = nslots;
+    if (po.kind == PipeOp::Scan) {
+      const SourceDesc& d = po.sources[0];
+      lv.kind = kScan;
+      lv.nsrc = 1;
+      lv.src[0] = make_src(d);
+      SRDL_REQUIRE(po.vars.size() == d.index.size(), kErrPlan, "scan arity mismatch");
+      for (size_t j = d.prefix.size(); j < po.vars.size(); j++) lv.scan_slot[j] = bind(po.vars[j]);
+    } else if (po.kind == PipeOp::ColumnJoin) {
+      lv.kind = kColumnJoin;
+      SRDL_REQUIRE(po.sources.size() <= (size_t)kMaxSrc && !po.sources.empty(), kErrUnsupported,
+                   "column join with too many sources");
+      for (auto& d : po.sources) lv.src[lv.nsrc++] = make_src(d);
+      lv.cj_slot = bind(po.var);
+    } else {
+      lv.kind = kCartesian;
+      SRDL_REQUIRE(po.sources.size() <= (size_t)kMaxSrc, kErrUnsupported, "cartesian too wide");
+      for (size_t i = 0; i < po.sources.size(); i++) {
+        lv.src[lv.nsrc] = make_src(po.sources[i]);
+        const auto& vs = i < po.var_from_source.size() ? po.var_from_source[i]
+                                                        : std::vector<std::string>{};
+        SRDL_REQUIRE(vs.size() <= 1, kErrUnsupported, "cartesian source binding several variables");
+        lv.src[lv.nsrc].out_slot = vs.empty() ? -1 : bind(vs[0]);
+        lv.nsrc++;
+      }
+    }
+    levels.push_back(lv);
+  }
+  SRDL_REQUIRE(insert && !levels.empty(), kErrPlan, "rule " + op.rule + ": no insert_into");
+
+  Relation* target = &rel(insert->rel);
+  if (!op.count)
+    SRDL_REQUIRE(target->arity <= 2, kErrUnsupported,
+                 "rule " + op.rule + ": materialising relations of arity > 2 is not supported");
+
+  // Walk the levels over a table of partial bindings.
+  Table cur;
+  cur.n = 1;
+  std::vector<DevBuf> cur_cols;
+  for (size_t li = 0; li < levels.size(); li++) {
+    LevelSpec& lv = levels[li];
+    const bool last = li + 1 == levels.size();
+    DevBuf wscr(join_work_scratch_bytes(cur.n), L_.stream);
+    Scratch s{wscr.as<char>(), wscr.bytes(), 0};
+    size_t pid = prof_begin("join_count");
+    JoinWork w = join_count(L_, lv, cur, s);
+    prof_end(pid, 8.0 * cur.n * (lv.n_in_slots + 3), (double)cur.n);
+    SRDL_CUDA(cudaMemcpyAsync(h_small_ + 3, w.offs + cur.n, 8, cudaMemcpyDeviceToHost, L_.stream));
+    SRDL_CUDA(cudaMemsetAsync(d_small_.as<uint64_t>() + 2, 0, 8, L_.stream));
+    SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+    const uint64_t total = h_small_[3];
+    if (last) {
+      if (op.count) {
+        lv.emit = kEmitCount;
+        pid = prof_begin("join_expand_count");
+        join_expand(L_, lv, cur, w, total, nullptr, nullptr, d_small_.as<uint64_t>() + 2);
+        // per candidate: its value (4 B) and one probed word of each other list (4 B)
+        prof_end(pid, 4.0 * total * std::max(1, lv.nsrc), (double)total);
+        counts_[op.rule] += read_scalar(2);
+      } else {
+        lv.emit = kEmitKeys;
+        lv.key_arity = target->arity;
+        for (int c = 0; c < target->arity; c++) lv.key_slot[c] = slot_of(insert->vars[insert->index[c]]);
+        Chunk ch;
+        ch.order = insert->index;
+        ch.keys = DevBuf(std::max<uint64_t>(total, 1) * 8, L_.stream);
+        pid = prof_begin("join_expand_keys");
+        join_expand(L_, lv, cur, w, total, nullptr, ch.keys.as<uint64_t>(),
+                    d_small_.as<uint64_t>() + 2);
+        ch.n = total ? read_scalar(2) : 0;
+        prof_end(pid, 4.0 * total * std::max(1, lv.nsrc) + 8.0 * ch.n, (double)total);
+        derived_ += ch.n;
+        target->v[kNew].chunks.push_back(std::move(ch));
+      }
+    } else {
+      lv.emit = kEmitTable;
+      Table next;
+      std::vector<DevBuf> cols;
+      for (int c = 0; c < nslots && c < kMaxSlots; c++) {
+        bool bound_here = c < levels[li + 1].n_in_slots;
+        if (!bound_here) break;
+        cols.emplace_back(std::max<uint64_t>(total, 1) * 4, L_.stream);
+        next.col[c] = cols.back().as<uint32_t>();
+      }
+      pid = prof_begin("join_expand_table");
+      join_expand(L_, lv, cur, w, total, &next, nullptr, d_small_.as<uint64_t>() + 2);
+      next.n = total ? read_scalar(2) : 0;
+      prof_end(pid, 4.0 * total * std::max(1, lv.nsrc) + 4.0 * next.n * levels[li + 1].n_in_slots,
+               (double)total);
+      cur = next;
+      cur_cols = std::move(cols);
+    }
+    if (!last && cur.n == 0) {
+      if (op.count) counts_[op.rule] += 0;
+      break;
+    }
+  }
+}
+
+void Database::op_rebuild(const Step& st, size_t pos, const Op& op) {
+  Relation& r = rel(op.rel);
+  RelVersion& rv = r.v[op.ver];
+  if (r.arity > 2) {
+    rv.chunks.clear();
+    rv.idx[op.index];
+    return;
+  }
+  uint64_t total = 0;
+  for (auto& c : rv.chunks) total += c.n;
+  // Gather the chunks into one buffer packed in the target order.
+  DevBuf gathered;
+  const uint64_t* in = nullptr;
+  if (rv.chunks.size() == 1 && rv.chunks[0].order == op.index) {
+    in = rv.chunks[0].keys.as<uint64_t>();
+  } else if (total) {
+    gathered = DevBuf(total * 8, L_.stream);
+    uint64_t off = 0;
+    for (auto& c : rv.chunks) {
+      if (!c.n) continue;
+      if (c.order == op.index)
+        SRDL_CUDA(cudaMemcpyAsync(gathered.as<uint64_t>() + off, c.keys.as<uint64_t>(), c.n * 8,
+                                  cudaMemcpyDeviceToDevice, L_.stream));
+      else
+        swap_halves(L_, c.keys.as<uint64_t>(), c.n, gathered.as<uint64_t>() + off);
+      off += c.n;
+    }
+    in = gathered.as<uint64_t>();
+  }
+  // Fuse with the delta computation when nothing reads NEW in between.
+  bool fuse = false;
+  if (op.ver == kNew) {
+    for (size_t i = pos + 1; i < st.ops.size(); i++) {
+      const Op& o = st.ops[i];
+      if (o.kind == Op::ComputeDelta && o.rel == op.rel && o.index == op.index) {
+        fuse = true;
+        break;
+      }
+      if (o.kind == Op::CheckSize && o.rel == op.rel) continue;
+      if (o.kind == Op::Clear && o.rel == op.rel && o.ver == kDelta) continue;
+      break;
+    }
+  }
+  if (fuse) {
+    const Index* full = nullptr;
+    if (r.v[kFull].has_index()) full = &ensure_index(r, kFull, op.index);
+    sort_into(r.pending, in ? in : nullptr, total, false, full);
+    r.pending_delta = true;
+    rv.chunks.clear();
+    rv.idx.clear();
+  } else {
+    Index fresh;
+    sort_into(fresh, in, total, false, nullptr);
+    rv.chunks.clear();
+    rv.idx.clear();
+    rv.idx[op.index] = std::move(fresh);
+  }
+}
+
+void Database::op_compute_delta(const Op& op) {
+  Relation& r = rel(op.rel);
+  r.v[kDelta].clear();
+  if (r.pending_delta) {
+    r.v[kDelta].idx[op.index] = std::move(r.pending);
+    r.pending = Index{};
+    r.pending_delta = false;
+    return;
+  }
+  if (r.arity > 2) {
+    r.v[kDelta].idx[op.index];
+    return;
+  }
+  Index& nw = ensure_index(r, kNew, op.index);
+  Index& d = r.v[kDelta].idx[op.index];
+  d.keys = DevBuf(std::max<uint64_t>(nw.n, 1) * 8, L_.stream);
+  if (!r.v[kFull].has_index() || nw.n == 0) {
+    if (nw.n)
+      SRDL_CUDA(cudaMemcpyAsync(d.keys.as<uint64_t>(), nw.keys.as<uint64_t>(), nw.n * 8,
+                                cudaMemcpyDeviceToDevice, L_.stream));
+    d.n = nw.n;
+    return;
+  }
+  Index& f = ensure_index(r, kFull, op.index);
+  DevBuf scratch(diff_scratch_bytes(nw.n) + 1024, L_.stream);
+  Scratch s{scratch.as<char>(), scratch.bytes(), 0};
+  size_t pid = prof_begin("set_difference");
+  set_difference(L_, nw.keys.as<uint64_t>(), nw.n, f.keys.as<uint64_t>(), f.n, d.keys.as<uint64_t>(),
+                 d_small_.as<uint64_t>(), s);
+  d.n = read_scalar(0);
+  prof_end(pid, 8.0 * (nw.n + f.n + d.n), (double)nw.n);
+}
+
+void Database::op_merge(const Op& op) {
+  Relation& r = rel(op.rel);
+  if (r.arity > 2) {
+    r.v[kFull].idx[op.index];
+    return;
+  }
+  RelVersion& dv = r.v[kDelta];
+  Index* d = nullptr;
+  auto it = dv.idx.find(op.index);
+  if (it != dv.idx.end()) d = &it->second;
+  else if (dv.has_index()) d = &ensure_index(r, kDelta, op.index);
+  const uint64_t dn = d ? d->n : 0;
+  if (!r.v[kFull].has_index()) {
+    Index& f = r.v[kFull].idx[op.index];
+    f.keys = DevBuf(std::max<uint64_t>(dn, 1) * 8, L_.stream);
+    if (dn)
+      SRDL_CUDA(cudaMemcpyAsync(f.keys.as<uint64_t>(), d->keys.as<uint64_t>(), dn * 8,
+                                cudaMemcpyDeviceToDevice, L_.stream));
+    f.n = dn;
+    return;
+  }
+  if (dn == 0) return;
+  Index& f = ensure_index(r, kFull, op.index);
+  Index m;
+  m.n = f.n + dn;
+  m.keys = DevBuf(m.n * 8, L_.stream);
+  size_t pid = prof_begin("merge");
+  merge_disjoint(L_, f.keys.as<uint64_t>(), f.n, d->keys.as<uint64_t>(), dn, m.keys.as<uint64_t>());
+  prof_end(pid, 16.0 * m.n, (double)m.n);
+  r.v[kFull].idx.clear();
+  r.v[kFull].idx[op.index] = std::move(m);
+}
+
+void Database::exec_ops(const Step& st, uint64_t it) {
+  for (size_t i = 0; i < st.ops.size(); i++) {
+    const Op& op = st.ops[i];
+    switch (op.kind) {
+      case Op::Execute: exec_pipeline(op, st.recursive, it); break;
+      case Op::Rebuild: op_rebuild(st, i, op); break;
+      case Op::Clear:
+        // A pending fused delta survives the clear of the old DELTA.
+        rel(op.rel).v[op.ver].clear();
+        break;
+      case Op::CheckSize: break;
+      case Op::ComputeDelta: op_compute_delta(op); break;
+      case Op::Merge: op_merge(op); break;
+      case Op::RebuildFrom: ensure_index(rel(op.rel), op.ver, op.index); break;
+      case Op::Reconstruct: break;
+    }
+  }
+}
+
+void Database::run(uint64_t max_iters) {
+  init_device();
+  reset_device_state();
+  const uint64_t launches0 = launches_total();
+  auto t0 = std::chrono::steady_clock::now();
+  upload_inputs();
+  for (size_t si = 0; si < steps_.size(); si++) {
+    const Step& st = steps_[si];
+    auto s0 = std::chrono::steady_clock::now();
+    if (!st.recursive) {
+      exec_ops(st, 0);
+      step_stats_[si].iterations = 1;
+    } else {
+      std::vector<std::string> computed;
+      for (auto& op : st.ops)
+        if (op.kind == Op::ComputeDelta) computed.push_back(op.rel);
+      for (uint64_t it = 0; it < max_iters; it++) {
+        if (it > 0) {
+          uint64_t total = 0;
+          for (auto& n : computed)
+            for (auto& kv : rel(n).v[kDelta].idx) {
+              total += kv.second.n;
+              break;
+            }
+          if (total == 0) break;
+        }
+        exec_ops(st, it);
+        step_stats_[si].iterations++;
+      }
+    }
+    SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+    step_stats_[si].ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - s0).count();
+  }
+  SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  run_ms_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  launches_ = launches_total() - launches0;
+  prof_collect();
+}
+
+uint64_t Database::size(const std::string& name) {
+  Relation& r = rel(name);
+  auto& fv = r.v[kFull];
+  auto it = fv.idx.find(r.canonical);
+  if (it != fv.idx.end()) return it->second.n;
+  for (auto& kv : fv.idx) return kv.second.n;
+  return 0;
+}
+
+uint64_t Database::count(const std::string& rule) const {
+  auto it = counts_.find(rule);
+  return it == counts_.end() ? 0 : it->second;
+}
+
+int64_t Database::dump(const std::string& name, uint32_t* out, uint64_t cap_rows) {
+  Relation& r = rel(name);
+  if (!r.v[kFull].has_index() || r.arity > 2) return 0;
+  SRDL_CUDA(cudaSetDevice(device_));
+  Index& ix = ensure_index(r, kFull, identity_perm(r.arity));
+  if (!out) return (int64_t)ix.n;
+  const uint64_t n = std::min(ix.n, cap_rows);
+  std::vector<uint64_t> keys(n);
+  if (n)
+    SRDL_CUDA(cudaMemcpyAsync(keys.data(), ix.keys.as<uint64_t>(), n * 8, cudaMemcpyDeviceToHost,
+                              L_.stream));
+  SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  for (uint64_t i = 0; i < n; i++) {
+    if (r.arity == 2) {
+      out[2 * i] = (uint32_t)(keys[i] >> 32);
+      out[2 * i + 1] = (uint32_t)keys[i];
+    } else {
+      out[i] = (uint32_t)(keys[i] >> 32);
+    }
+  }
+  return (int64_t)ix.n;
+}
+
+std::string Database::stats_json() const {
+  std::ostringstream o;
+  o << "{\"plan\":\"" << name_ << "\",\"run_ms\":" << run_ms_ << ",\"derived\":" << derived_
+    << ",\"value_bits\":" << bits_ << ",\"steps\":[";
+  for (size_t i = 0; i < step_stats_.size(); i++) {
+    o << (i ? "," : "") << "{\"recursive\":" << (steps_[i].recursive ? "true" : "false")
+      << ",\"iterations\":" << step_stats_[i].iterations << ",\"ms\":" << step_stats_[i].ms << "}";
+  }
+  o << "],\"launches\":" << launches_ << ",\"kernels\":{";
+  bool kfirst = true;
+  for (auto& kv : kstats_) {
+    o << (kfirst ? "" : ",") << "\"" << kv.first << "\":{\"ms\":" << kv.second.ms
+      << ",\"bytes\":" << kv.second.bytes << ",\"units\":" << kv.second.units
+      << ",\"scopes\":" << kv.second.scopes << "}";
+    kfirst = false;
+  }
+  o << "},\"counts\":{";
+  bool first = true;
+  for (auto& kv : counts_) {
+    o << (first ? "" : ",") << "\"" << kv.first << "\":" << kv.second;
+    first = false;
+  }
+  o << "}}";
+  return o.str();
+}
+
+}  // namespace srdl

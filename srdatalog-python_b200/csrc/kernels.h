@@ -1,0 +1,141 @@
+// kernels.h -- host-side launch wrappers for the srdl device kernels.
+//
+// Every wrapper is stream-ordered and allocation-free: temporaries come
+// from a caller-provided scratch region whose size the matching
+// *_scratch_bytes() function reports.  Sizes that the host must know
+// (unique counts, join output counts) are written to device memory; the
+// caller decides when to read them back.
+#pragma once
+
+#include "common.cuh"
+
+namespace srdl {
+
+struct Launch {
+  cudaStream_t stream = 0;
+  int num_sms = 148;
+  uint32_t* d_err = nullptr;  // device error word (bounded-wait failures etc.)
+};
+
+// Bump allocator over a caller-provided scratch region (256-byte aligned).
+struct Scratch {
+  char* base = nullptr;
+  size_t cap = 0, used = 0;
+  template <typename T>
+  T* take(size_t count) {
+    size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+    SRDL_REQUIRE(used + bytes <= cap, kErrCapacity, "scratch region too small");
+    T* p = reinterpret_cast<T*>(base + used);
+    used += bytes;
+    return p;
+  }
+};
+
+// Process-wide count of kernels this library has launched (bench evidence).
+void count_launches(int k);
+uint64_t launches_total();
+
+// Largest value in d[0..n) -> *d_max (uint32; 0 when n == 0).
+void max_u32(const Launch& L, const uint32_t* d, uint64_t n, uint32_t* d_max);
+
+// ---------------------------------------------------------------- sort
+// Bits needed to hold every value of the active domain (max value < 2^bits).
+int value_bits(uint32_t max_value);
+
+// Scratch needed by sort_dedup for n input keys.
+size_t sort_scratch_bytes(uint64_t n, int dom_bits);
+
+// Radix-sorts n uint64 keys (both 32-bit halves < 2^dom_bits; halves
+// swapped first when `swap` is set) and writes the distinct keys, in
+// ascending order, into `out`.  When `full` is given, keys present in the
+// sorted unique array full[0..n_full) are dropped as well (fused
+// DELTA = unique(NEW) - FULL).  The output count goes to *d_nout.
+// `out` needs room for n keys and may alias `in`.
+void sort_dedup(const Launch& L, const uint64_t* in, uint64_t n, int dom_bits, bool swap,
+                const uint64_t* full, uint64_t n_full, uint64_t* out, uint64_t* d_nout,
+                Scratch& s);
+
+// ------------------------------------------------------------- set ops
+size_t diff_scratch_bytes(uint64_t n);
+// out = a - b for sorted unique arrays; *d_nout = |out|; out needs room for na.
+void set_difference(const Launch& L, const uint64_t* a, uint64_t na, const uint64_t* b,
+                    uint64_t nb, uint64_t* out, uint64_t* d_nout, Scratch& s);
+
+// out = a U b (sorted unique, disjoint) by merge path; out needs na+nb.
+void merge_disjoint(const Launch& L, const uint64_t* a, uint64_t na, const uint64_t* b,
+                    uint64_t nb, uint64_t* out);
+
+// Trie view pieces for a sorted unique key array.
+size_t roots_scratch_bytes(uint64_t n);
+void build_lo(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* lo);
+void build_dir(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* dir, uint32_t dir_n);
+void build_roots(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* roots,
+                 uint64_t* d_nroots, Scratch& s);
+
+// Swap the two 32-bit halves of every key (index permutation (1,0) <-> (0,1)).
+void swap_halves(const Launch& L, const uint64_t* in, uint64_t n, uint64_t* out);
+
+// Exclusive scan of n uint64 values; out has n+1 entries (out[n] = total).
+size_t scan_scratch_bytes(uint64_t n);
+void exclusive_scan_u64(const Launch& L, const uint64_t* in, uint64_t n, uint64_t* out,
+                        Scratch& s);
+
+// ---------------------------------------------------------------- join
+constexpr int kMaxSlots = 8;
+constexpr int kMaxSrc = 4;
+constexpr int kMaxFilt = 4;
+
+enum LevelKind : int { kColumnJoin = 0, kCartesian = 1, kScan = 2 };
+enum EmitKind : int { kEmitTable = 0, kEmitKeys = 1, kEmitCount = 2 };
+enum FiltOp : int { kNe = 0, kEq = 1, kLt = 2, kLe = 3, kGt = 4, kGe = 5 };
+
+struct SrcSpec {
+  TrieView t;
+  int prefix_slot = -1;  // binding slot holding the prefix value, -1: no prefix (roots)
+  int out_slot = -1;     // cartesian: slot this source binds (-1: existence only)
+};
+
+struct FiltSpec {
+  int a_slot = -1, b_slot = -1;  // -1: use the constant
+  uint32_t a_const = 0, b_const = 0;
+  int op = kNe;
+};
+
+struct LevelSpec {
+  int kind = kColumnJoin;
+  int nsrc = 0;
+  SrcSpec src[kMaxSrc];
+  int cj_slot = -1;                     // column join: slot of the joined variable
+  int scan_slot[2] = {-1, -1};          // scan: slots for index columns 0 and 1
+  int nfilt = 0;
+  FiltSpec filt[kMaxFilt];
+  int n_in_slots = 0;                   // slots bound by the input table
+  int emit = kEmitTable;
+  int key_slot[2] = {-1, -1};           // emit keys: slots of the target index columns
+  int key_arity = 2;
+};
+
+struct Table {
+  uint32_t* col[kMaxSlots] = {};
+  uint64_t n = 0;
+};
+
+size_t join_work_scratch_bytes(uint64_t rows);
+// Pass 1: per input row, the number of work items (candidates) it expands
+// to.  Writes offsets[0..rows] (exclusive scan) and the total into
+// *d_total (= offsets[rows]).  Scratch keeps per-row driver info that
+// join_expand reads, so the same Scratch must be passed to both.
+struct JoinWork {
+  uint64_t* offs = nullptr;  // rows + 1
+  uint8_t* drv = nullptr;    // column join: driver source per row
+  uint32_t* beg = nullptr;   // column join: driver list begin per row
+};
+JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scratch& s);
+
+// Pass 2: expands `total` work items; surviving bindings are appended to
+// `out_table` (emit table), to `out_keys` (emit keys) or counted (emit
+// count) via *d_out_n, which the caller zeroes.  Output capacity = total.
+void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const JoinWork& w,
+                 uint64_t total, Table* out_table, uint64_t* out_keys, uint64_t* d_out_n);
+
+}  // namespace srdl

@@ -1,0 +1,482 @@
+// runtime.cu -- Database: plan parsing, input staging, relation indexes.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <sstream>
+
+#include "runtime.h"
+
+namespace srdl {
+
+// Dense directories are built while the value domain stays below this many
+// entries (64 MB of uint32 offsets); above it, lookups binary-search keys.
+constexpr uint64_t kDenseDirMax = 1ull << 24;
+constexpr int kSmallSlots = 16;
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+
+std::vector<int> identity_perm(int arity) {
+  std::vector<int> p(arity);
+  for (int i = 0; i < arity; i++) p[i] = i;
+  return p;
+}
+
+// ------------------------------------------------------------------ DevBuf
+
+DevBuf::DevBuf(size_t bytes, cudaStream_t st) : bytes_(bytes), st_(st) {
+  if (bytes) SRDL_CUDA(cudaMallocAsync(&p_, (bytes + 255) & ~size_t(255), st));
+}
+
+DevBuf& DevBuf::operator=(DevBuf&& o) noexcept {
+  if (this != &o) {
+    reset();
+    p_ = o.p_;
+    bytes_ = o.bytes_;
+    st_ = o.st_;
+    o.p_ = nullptr;
+    o.bytes_ = 0;
+  }
+  return *this;
+}
+
+void DevBuf::reset() {
+  if (p_) cudaFreeAsync(p_, st_);
+  p_ = nullptr;
+  bytes_ = 0;
+}
+
+// ------------------------------------------------------------------ plan
+
+static Ver parse_ver(const std::string& s) {
+  if (s == "FULL") return kFull;
+  if (s == "DELTA") return kDelta;
+  if (s == "NEW") return kNew;
+  throw Error{kErrPlan, "plan: bad version " + s};
+}
+
+static SourceDesc parse_source(const Json& j) {
+  SourceDesc s;
+  s.rel = j.at("rel").s();
+  s.ver = parse_ver(j.at("ver").s());
+  s.index = j.at("index").ints();
+  s.prefix = j.at("prefix").strs();
+  return s;
+}
+
+Database::Database(const std::string& plan_json, int device) : device_(device) {
+  parse_plan(plan_json);
+}
+
+Database::~Database() {
+  if (dev_ready_) {
+    cudaSetDevice(device_);
+    for (auto& kv : rels_)
+      for (auto& v : kv.second->v) v.clear();
+    for (auto& kv : rels_) kv.second->pending = Index{};
+    for (auto& kv : rels_) kv.second->dstaged.reset();
+    d_small_.reset();
+    cudaStreamSynchronize(L_.stream);
+    if (h_small_) cudaFreeHost(h_small_);
+    for (auto& kv : rels_)
+      if (kv.second->pinned) cudaFreeHost(kv.second->pinned);
+    for (auto& e : kev_) {
+      cudaEventDestroy(e.a);
+      cudaEventDestroy(e.b);
+    }
+    for (auto e : ev_pool_) cudaEventDestroy(e);
+    if (own_stream_) cudaStreamDestroy(L_.stream);
+  }
+}
+
+void Database::parse_plan(const std::string& plan_json) {
+  Json p = JsonParser(plan_json).parse();
+  SRDL_REQUIRE(p.at("version").i() == 1, kErrPlan, "plan: unsupported version");
+  name_ = p.has("name") ? p.at("name").s() : "plan";
+  for (auto& r : p.at("relations").a()) {
+    auto rel = std::make_unique<Relation>();
+    rel->name = r.at("name").s();
+    rel->arity = (int)r.at("arity").i();
+    SRDL_REQUIRE(rel->arity >= 1, kErrPlan, "plan: relation arity must be >= 1");
+    rel->input_file = r.at("input_file").s();
+    rel->print_size = r.at("print_size").flag();
+    rel->index_type = r.at("index_type").s();
+    rel->canonical = r.at("canonical").ints();
+    SRDL_REQUIRE((int)rel->canonical.size() == rel->arity, kErrPlan,
+                 "plan: canonical index arity mismatch for " + rel->name);
+    if (!rel->input_file.empty()) inputs_.push_back(rel->name);
+    rels_[rel->name] = std::move(rel);
+  }
+  for (auto& sj : p.at("steps").a()) {
+    Step st;
+    st.recursive = sj.at("recursive").flag();
+    for (auto& oj : sj.at("ops").a()) {
+      Op op;
+      const std::string k = oj.at("op").s();
+      if (k == "execute_pipeline") {
+        op.kind = Op::Execute;
+        op.rule = oj.at("rule").s();
+        op.count = oj.at("count").flag();
+        for (auto& pj : oj.at("pipeline").a()) {
+          PipeOp po;
+          const std::string pk = pj.at("op").s();
+          if (pk == "scan") {
+            po.kind = PipeOp::Scan;
+            po.sources.push_back(parse_source(pj));
+            po.vars = pj.at("vars").strs();
+          } else if (pk == "column_join") {
+            po.kind = PipeOp::ColumnJoin;
+            po.var = pj.at("var").s();
+            for (auto& s : pj.at("sources").a()) po.sources.push_back(parse_source(s));
+          } else if (pk == "cartesian_join") {
+            po.kind = PipeOp::Cartesian;
+            po.vars = pj.at("vars").strs();
+            for (auto& s : pj.at("sources").a()) po.sources.push_back(parse_source(s));
+            for (auto& v : pj.at("var_from_source").a()) po.var_from_source.push_back(v.strs());
+          } else if (pk == "filter") {
+            po.kind = PipeOp::Filter;
+            po.vars = pj.at("vars").strs();
+            po.code = pj.at("code").s();
+          } else if (pk == "insert_into") {
+            po.kind = PipeOp::Insert;
+            po.rel = pj.at("rel").s();
+            po.vars = pj.at("vars").strs();
+            po.index = pj.at("index").ints();
+          } else {
+            throw Error{kErrUnsupported, "plan: pipeline op '" + pk + "' is not supported"};
+          }
+          for (auto& s : po.sources)
+            SRDL_REQUIRE(rels_.count(s.rel), kErrPlan, "plan: unknown relation " + s.rel);
+          op.pipeline.push_back(std::move(po));
+        }
+      } else {
+        op.rel = oj.at("rel").s();
+        SRDL_REQUIRE(rels_.count(op.rel), kErrPlan, "plan: unknown relation " + op.rel);
+        if (k == "rebuild_index") {
+          op.kind = Op::Rebuild;
+          op.ver = parse_ver(oj.at("ver").s());
+          op.index = oj.at("index").ints();
+        } else if (k == "clear_relation") {
+          op.kind = Op::Clear;
+          op.ver = parse_ver(oj.at("ver").s());
+        } else if (k == "check_size") {
+          op.kind = Op::CheckSize;
+          op.ver = parse_ver(oj.at("ver").s());
+        } else if (k == "compute_delta_index") {
+          op.kind = Op::ComputeDelta;
+          op.index = oj.at("index").ints();
+        } else if (k == "merge_index") {
+          op.kind = Op::Merge;
+          op.index = oj.at("index").ints();
+        } else if (k == "rebuild_index_from_index") {
+          op.kind = Op::RebuildFrom;
+          op.ver = parse_ver(oj.at("ver").s());
+          op.index = oj.at("index").ints();
+          op.source_index = oj.at("source_index").ints();
+        } else if (k == "post_stratum_reconstruct") {
+          op.kind = Op::Reconstruct;
+          op.index = oj.at("index").ints();
+        } else {
+          throw Error{kErrUnsupported, "plan: op '" + k + "' is not supported"};
+        }
+      }
+      st.ops.push_back(std::move(op));
+    }
+    steps_.push_back(std::move(st));
+  }
+  step_stats_.resize(steps_.size());
+}
+
+Relation& Database::rel(const std::string& name) {
+  auto it = rels_.find(name);
+  SRDL_REQUIRE(it != rels_.end(), kErrArg, "unknown relation " + name);
+  return *it->second;
+}
+
+bool Database::any_loaded() const {
+  for (auto& kv : rels_)
+    if (kv.second->loaded) return true;
+  return false;
+}
+
+// ------------------------------------------------------------------ device
+
+void Database::init_device() {
+  SRDL_CUDA(cudaSetDevice(device_));
+  if (dev_ready_) return;
+  int sms = 0;
+  SRDL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+  L_.num_sms = sms;
+  if (own_stream_) SRDL_CUDA(cudaStreamCreateWithFlags(&L_.stream, cudaStreamNonBlocking));
+  // Keep freed blocks in the pool: iterations reuse the same sizes.
+  cudaMemPool_t pool;
+  SRDL_CUDA(cudaDeviceGetDefaultMemPool(&pool, device_));
+  uint64_t thr = ~0ull;
+  SRDL_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  SRDL_CUDA(cudaMallocHost(&h_small_, kSmallSlots * sizeof(uint64_t)));
+  d_small_ = DevBuf(kSmallSlots * sizeof(uint64_t), L_.stream);
+  dev_ready_ = true;
+}
+
+uint64_t Database::read_scalar(int slot) {
+  SRDL_CUDA(cudaMemcpyAsync(h_small_ + slot, d_small_.as<uint64_t>() + slot, sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost, L_.stream));
+  SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  return h_small_[slot];
+}
+
+void Database::set_stream(cudaStream_t s) {
+  SRDL_CUDA(cudaSetDevice(device_));
+  if (!dev_ready_) {
+    L_.stream = s;
+    own_stream_ = false;
+    return;
+  }
+  // Release everything allocated on the old stream before switching.
+  SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  reset_device_state();
+  for (auto& kv : rels_) {
+    if (kv.second->dstaged_n) SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  }
+  DevBuf keep_small(kSmallSlots * sizeof(uint64_t), s);
+  std::vector<std::pair<Relation*, DevBuf>> moved;
+  for (auto& kv : rels_) {
+    Relation& r = *kv.second;
+    if (!r.dstaged_n) continue;
+    DevBuf nb(r.dstaged_n * 8, s);
+    SRDL_CUDA(cudaMemcpyAsync(nb.as<void>(), r.dstaged.as<void>(), r.dstaged_n * 8,
+                              cudaMemcpyDeviceToDevice, L_.stream));
+    SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+    r.dstaged = std::move(nb);
+  }
+  d_small_ = std::move(keep_small);
+  SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  if (own_stream_) SRDL_CUDA(cudaStreamDestroy(L_.stream));
+  L_.stream = s;
+  own_stream_ = false;
+}
+
+cudaEvent_t make_event() {
+  cudaEvent_t e;
+  SRDL_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+size_t Database::prof_begin(const std::string& name) {
+  if (!profile_) return (size_t)-1;
+  KEvent k{name, nullptr, nullptr, 0, 0};
+  for (cudaEvent_t* e : {&k.a, &k.b}) {
+    if (!ev_pool_.empty()) {
+      *e = ev_pool_.back();
+      ev_pool_.pop_back();
+    } else {
+      *e = make_event();
+    }
+  }
+  SRDL_CUDA(cudaEventRecord(k.a, L_.stream));
+  kev_.push_back(k);
+  return kev_.size() - 1;
+}
+
+void Database::prof_end(size_t id, double bytes, double units) {
+  if (id == (size_t)-1) return;
+  SRDL_CUDA(cudaEventRecord(kev_[id].b, L_.stream));
+  kev_[id].bytes = bytes;
+  kev_[id].units = units;
+}
+
+void Database::prof_collect() {
+  SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  for (auto& k : kev_) {
+    float ms = 0;
+    SRDL_CUDA(cudaEventElapsedTime(&ms, k.a, k.b));
+    KernelStats& s = kstats_[k.name];
+    s.ms += ms;
+    s.bytes += k.bytes;
+    s.units += k.units;
+    s.scopes++;
+    ev_pool_.push_back(k.a);
+    ev_pool_.push_back(k.b);
+  }
+  kev_.clear();
+}
+
+void Database::reset_device_state() {
+  for (auto& kv : rels_) {
+    for (auto& v : kv.second->v) v.clear();
+    kv.second->pending = Index{};
+    kv.second->pending_delta = false;
+  }
+  counts_.clear();
+  kstats_.clear();
+  derived_ = 0;
+  for (auto& s : step_stats_) s = StepStats{};
+}
+
+// ------------------------------------------------------------------ loading
+
+void Database::load_rows(const std::string& name, const uint32_t* rows, uint64_t n) {
+  Relation& r = rel(name);
+  SRDL_REQUIRE(rows || n == 0, kErrArg, "load_rows: null rows");
+  SRDL_REQUIRE(r.arity <= 2, kErrUnsupported,
+               "relation " + name + ": only arity 1 and 2 relations can be materialised");
+  r.staged.insert(r.staged.end(), rows, rows + n * r.arity);
+  r.pinned_words = 0;  // page-locked mirror is stale
+  r.loaded = true;
+}
+
+void Database::load_device_rows(const std::string& name, const uint32_t* d_rows, uint64_t n) {
+  Relation& r = rel(name);
+  SRDL_REQUIRE(d_rows || n == 0, kErrArg, "load_device_rows: null rows");
+  SRDL_REQUIRE(r.arity == 2, kErrUnsupported, "load_device_rows: binary relations only");
+  SRDL_REQUIRE(r.dstaged_n == 0, kErrState, "load_device_rows: relation already has device rows");
+  init_device();
+  r.dstaged = DevBuf(std::max<uint64_t>(n, 1) * 8, L_.stream);
+  if (n)
+    SRDL_CUDA(cudaMemcpyAsync(r.dstaged.as<void>(), d_rows, n * 8, cudaMemcpyDeviceToDevice,
+                              L_.stream));
+  max_u32(L_, r.dstaged.as<uint32_t>(), n * 2, reinterpret_cast<uint32_t*>(d_small_.as<uint64_t>() + 4));
+  SRDL_CUDA(cudaMemsetAsync(reinterpret_cast<uint32_t*>(d_small_.as<uint64_t>() + 4) + 1, 0, 4, L_.stream));
+  r.dstaged_max = (uint32_t)read_scalar(4);
+  r.dstaged_n = n;
+  r.loaded = true;
+}
+
+// Sorted unique keys of `in` (packed in some order) into `out`, optionally
+// dropping keys present in `full`.
+void Database::sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full) {
+  out.keys = DevBuf(std::max<uint64_t>(n, 1) * 8, L_.stream);
+  out.trie = false;
+  if (n == 0) {
+    out.n = 0;
+    return;
+  }
+  DevBuf scratch(sort_scratch_bytes(n, bits_), L_.stream);
+  Scratch s{scratch.as<char>(), scratch.bytes(), 0};
+  const bool diff = full && full->n;
+  size_t pid = prof_begin(diff ? "sort_dedup_diff" : "sort_dedup");
+  sort_dedup(L_, in, n, bits_, swap, diff ? full->keys.as<uint64_t>() : nullptr,
+             full ? full->n : 0, out.keys.as<uint64_t>(), d_small_.as<uint64_t>(), s);
+  prof_end(pid, 0, (double)n);
+  out.n = read_scalar(0);
+  if (pid != (size_t)-1) {
+    // Algorithmic bytes: each counting pass reads and writes the packed
+    // keys once; packing reads the input; the dedup pass reads the sorted
+    // keys and writes the distinct ones (plus one probe word per key into
+    // FULL when the delta is fused).
+    const double ks = 2 * bits_ <= 32 ? 4 : 8;
+    const double passes = (2 * bits_ + 7) / 8;
+    kev_[pid].bytes = passes * 2 * ks * n + 8.0 * n + ks * n + ks * n + 8.0 * out.n +
+                      (diff ? 8.0 * n : 0);
+  }
+}
+
+void Database::upload_inputs() {
+  uint32_t mx = 0;
+  for (auto& kv : rels_) {
+    for (uint32_t x : kv.second->staged) mx = std::max(mx, x);
+    if (kv.second->dstaged_n) mx = std::max(mx, kv.second->dstaged_max);
+  }
+  dom_max_ = mx;
+  bits_ = value_bits(mx);
+  for (auto& kv : rels_) {
+    Relation& r = *kv.second;
+    if (!r.loaded) continue;
+    if (r.dstaged_n) {
+      SRDL_REQUIRE(r.staged.empty(), kErrState,
+                   "relation " + r.name + " has both host and device rows staged");
+      Index& ix = r.v[kFull].idx[r.canonical];
+      sort_into(ix, r.dstaged.as<uint64_t>(), r.dstaged_n, r.canonical == std::vector<int>{0, 1},
+                nullptr);
+      continue;
+    }
+    const uint64_t n = r.staged.size() / r.arity;
+    DevBuf raw(std::max<uint64_t>(n, 1) * 8, L_.stream);
+    bool swap = false;
+    if (r.arity == 2) {
+      // Host rows are copied once into page-locked memory so that every run
+      // uploads them with one asynchronous DMA.
+      if (r.pinned_words != r.staged.size() && n) {
+        if (r.pinned) SRDL_CUDA(cudaFreeHost(r.pinned));
+        r.pinned = nullptr;
+        SRDL_CUDA(cudaMallocHost(&r.pinned, r.staged.size() * 4));
+        memcpy(r.pinned, r.staged.data(), r.staged.size() * 4);
+        r.pinned_words = r.staged.size();
+      }
+      // A row-major (c0, c1) pair read as a little-endian uint64 is
+      // (c1 << 32) | c0, i.e. the key of permutation (1,0).
+      if (n)
+        SRDL_CUDA(cudaMemcpyAsync(raw.as<uint64_t>(), r.pinned, n * 8, cudaMemcpyHostToDevice,
+                                  L_.stream));
+      swap = (r.canonical == std::vector<int>{0, 1});
+    } else {
+      std::vector<uint64_t> k(n);
+      for (uint64_t i = 0; i < n; i++) k[i] = (uint64_t)r.staged[i] << 32;
+      SRDL_CUDA(cudaMemcpyAsync(raw.as<uint64_t>(), k.data(), n * 8, cudaMemcpyHostToDevice,
+                                L_.stream));
+      SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+    }
+    Index& ix = r.v[kFull].idx[r.canonical];
+    sort_into(ix, raw.as<uint64_t>(), n, swap, nullptr);
+  }
+}
+
+// ------------------------------------------------------------------ indexes
+
+Index& Database::ensure_index(Relation& r, Ver v, const std::vector<int>& perm) {
+  SRDL_REQUIRE((int)perm.size() == r.arity, kErrPlan, "index arity mismatch on " + r.name);
+  RelVersion& rv = r.v[v];
+  auto it = rv.idx.find(perm);
+  if (it != rv.idx.end()) return it->second;
+  Index& ix = rv.idx[perm];
+  // Build from any existing permutation of the same version.
+  for (auto& kv : rv.idx) {
+    if (&kv.second == &ix) continue;
+    SRDL_REQUIRE(r.arity == 2, kErrUnsupported, "secondary index on non-binary relation " + r.name);
+    sort_into(ix, kv.second.keys.as<uint64_t>(), kv.second.n, true, nullptr);
+    return ix;
+  }
+  ix.n = 0;
+  ix.keys = DevBuf(8, L_.stream);
+  return ix;
+}
+
+void Database::ensure_trie(Relation& r, Index& ix) {
+  (void)r;
+  if (ix.trie) return;
+  const uint64_t n = ix.n;
+  size_t pid = prof_begin("trie_build");
+  ix.lo = DevBuf(std::max<uint64_t>(n, 1) * 4, L_.stream);
+  ix.roots = DevBuf(std::max<uint64_t>(n, 1) * 4, L_.stream);
+  build_lo(L_, ix.keys.as<uint64_t>(), n, ix.lo.as<uint32_t>());
+  DevBuf scratch(roots_scratch_bytes(n) + 1024, L_.stream);
+  Scratch s{scratch.as<char>(), scratch.bytes(), 0};
+  build_roots(L_, ix.keys.as<uint64_t>(), n, ix.roots.as<uint32_t>(), d_small_.as<uint64_t>() + 1, s);
+  ix.dir_n = 0;
+  if ((uint64_t)dom_max_ + 2 <= kDenseDirMax) {
+    ix.dir_n = dom_max_ + 2;
+    ix.dir = DevBuf((size_t)ix.dir_n * 4, L_.stream);
+    build_dir(L_, ix.keys.as<uint64_t>(), n, ix.dir.as<uint32_t>(), ix.dir_n);
+  }
+  prof_end(pid, 8.0 * n + 4.0 * n + 8.0 * n + 4.0 * ix.dir_n, (double)n);
+  ix.n_roots = (uint32_t)read_scalar(1);
+  if (pid != (size_t)-1) kev_[pid].bytes += 4.0 * ix.n_roots;
+  ix.trie = true;
+}
+
+TrieView Database::view(Relation& r, Index& ix) {
+  ensure_trie(r, ix);
+  TrieView t;
+  t.keys = ix.keys.as<uint64_t>();
+  t.lo = ix.lo.as<uint32_t>();
+  t.roots = ix.roots.as<uint32_t>();
+  t.dir = ix.dir_n ? ix.dir.as<uint32_t>() : nullptr;
+  t.n = ix.n;
+  t.n_roots = ix.n_roots;
+  t.dir_n = ix.dir_n;
+  t.arity = r.arity;
+  return t;
+}
+
+}  // namespace srdl

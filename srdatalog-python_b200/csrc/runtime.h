@@ -1,0 +1,209 @@
+// runtime.h -- host-side database: plan, relation store, executor.
+//
+// Replaces the generated <Project>_Runner (step_N bodies, orchestrator_jit.py:
+// 600-747), the device DB (RT/gpu/runtime/query.h:107 copy_host_to_device)
+// and the mir_helpers primitive provider (RT/gpu/runtime/gpu_mir_helpers.h).
+// The plan is interpreted; kernels are fixed.
+#pragma once
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "json.h"
+#include "kernels.h"
+
+namespace srdl {
+
+enum Ver { kFull = 0, kDelta = 1, kNew = 2 };
+
+// Owning device allocation from the database's stream-ordered pool.
+class DevBuf {
+ public:
+  DevBuf() = default;
+  DevBuf(size_t bytes, cudaStream_t st);
+  ~DevBuf() { reset(); }
+  DevBuf(DevBuf&& o) noexcept { *this = std::move(o); }
+  DevBuf& operator=(DevBuf&& o) noexcept;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  void reset();
+  template <typename T>
+  T* as() const { return reinterpret_cast<T*>(p_); }
+  size_t bytes() const { return bytes_; }
+
+ private:
+  void* p_ = nullptr;
+  size_t bytes_ = 0;
+  cudaStream_t st_ = 0;
+};
+
+// One sorted, duplicate-free key array plus the join-side trie pieces,
+// built on first use by a join.
+struct Index {
+  DevBuf keys;
+  uint64_t n = 0;
+  bool trie = false;
+  DevBuf lo, roots, dir;
+  uint32_t n_roots = 0, dir_n = 0;
+};
+
+struct Chunk {
+  DevBuf keys;
+  uint64_t n = 0;
+  std::vector<int> order;  // index permutation the keys are packed in
+};
+
+struct RelVersion {
+  std::map<std::vector<int>, Index> idx;
+  std::vector<Chunk> chunks;  // NEW: unsorted join output
+  void clear() {
+    idx.clear();
+    chunks.clear();
+  }
+  bool has_index() const { return !idx.empty(); }
+};
+
+struct Relation {
+  std::string name;
+  int arity = 2;
+  std::string input_file;
+  bool print_size = false;
+  std::string index_type;
+  std::vector<int> canonical;
+  RelVersion v[3];
+  std::vector<uint32_t> staged;  // host rows loaded before run (row-major)
+  uint32_t* pinned = nullptr;    // page-locked copy of `staged` used for the upload
+  size_t pinned_words = 0;
+  DevBuf dstaged;                // device rows loaded before run (row-major pairs)
+  uint64_t dstaged_n = 0;
+  uint32_t dstaged_max = 0;
+  bool loaded = false;
+  bool pending_delta = false;    // NEW was sorted straight into a delta
+  Index pending;
+};
+
+// Plan-level descriptions (parsed once from JSON).
+struct SourceDesc {
+  std::string rel;
+  Ver ver;
+  std::vector<int> index;
+  std::vector<std::string> prefix;
+};
+
+struct PipeOp {
+  enum Kind { Scan, ColumnJoin, Cartesian, Filter, Insert } kind;
+  std::vector<SourceDesc> sources;           // scan: one
+  std::vector<std::string> vars;             // scan / cartesian / insert / filter vars
+  std::string var;                           // column join var
+  std::vector<std::vector<std::string>> var_from_source;
+  std::string code;                          // filter
+  std::string rel;                           // insert
+  std::vector<int> index;                    // insert dedup index
+};
+
+struct Op {
+  enum Kind { Execute, Rebuild, Clear, CheckSize, ComputeDelta, Merge, RebuildFrom, Reconstruct } kind;
+  std::string rel, rule;
+  Ver ver = kFull;
+  std::vector<int> index, source_index;
+  bool count = false;
+  std::vector<PipeOp> pipeline;
+};
+
+struct Step {
+  bool recursive = false;
+  std::vector<Op> ops;
+};
+
+// Per-kernel-family device time (CUDA events on the database stream) and
+// the algorithmic bytes / work units those launches had to process.
+struct KernelStats {
+  double ms = 0, bytes = 0, units = 0;
+  uint64_t scopes = 0;
+};
+
+struct StepStats {
+  uint64_t iterations = 0;
+  double ms = 0;
+};
+
+class Database {
+ public:
+  Database(const std::string& plan_json, int device);
+  ~Database();
+
+  void load_rows(const std::string& rel, const uint32_t* rows, uint64_t n);
+  void load_device_rows(const std::string& rel, const uint32_t* d_rows, uint64_t n);
+  void set_stream(cudaStream_t s);
+  void set_profiling(bool on) { profile_ = on; }
+  void load_csv(const std::string& rel, const std::string& path);
+  void load_all(const std::string& dir);
+  void run(uint64_t max_iters);
+  uint64_t size(const std::string& rel);
+  uint64_t count(const std::string& rule) const;
+  // Rows of FULL in declared column order, lexicographically sorted.
+  int64_t dump(const std::string& rel, uint32_t* out, uint64_t cap_rows);
+  std::string stats_json() const;
+  bool any_loaded() const;
+  uint64_t staged_rows(const std::string& name) {
+    Relation& r = rel(name);
+    return r.staged.size() / r.arity + r.dstaged_n;
+  }
+  void init_device();
+  Relation& rel(const std::string& name);
+  bool has_rel(const std::string& name) const { return rels_.count(name) > 0; }
+  const std::vector<std::string>& input_relations() const { return inputs_; }
+
+ private:
+  // ------------------------------------------------------------ state
+  int device_;
+  bool dev_ready_ = false;
+  Launch L_;
+  std::string name_;
+  std::map<std::string, std::unique_ptr<Relation>> rels_;
+  std::vector<std::string> inputs_;
+  std::vector<Step> steps_;
+  std::map<std::string, uint64_t> counts_;
+  std::vector<StepStats> step_stats_;
+  uint32_t dom_max_ = 0;
+  int bits_ = 1;
+  uint64_t derived_ = 0;
+  double run_ms_ = 0;
+  bool own_stream_ = true;
+  bool profile_ = false;
+  struct KEvent {
+    std::string name;
+    cudaEvent_t a, b;
+    double bytes, units;
+  };
+  std::vector<KEvent> kev_;
+  std::vector<cudaEvent_t> ev_pool_;
+  std::map<std::string, KernelStats> kstats_;
+  uint64_t launches_ = 0;
+  size_t prof_begin(const std::string& name);
+  void prof_end(size_t id, double bytes, double units);
+  void prof_collect();
+  DevBuf d_small_;  // device scalars read back by the host
+  uint64_t* h_small_ = nullptr;  // pinned mirror
+
+  // ------------------------------------------------------------ helpers
+  void parse_plan(const std::string& plan_json);
+  void reset_device_state();
+  void upload_inputs();
+  uint64_t read_scalar(int slot);
+  Index& ensure_index(Relation& r, Ver v, const std::vector<int>& perm);
+  void ensure_trie(Relation& r, Index& ix);
+  TrieView view(Relation& r, Index& ix);
+  void sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full);
+  void exec_ops(const Step& st, uint64_t iteration);
+  void exec_pipeline(const Op& op, bool recursive, uint64_t iteration);
+  void op_rebuild(const Step& st, size_t pos, const Op& op);
+  void op_compute_delta(const Op& op);
+  void op_merge(const Op& op);
+};
+
+std::vector<int> identity_perm(int arity);
+
+}  // namespace srdl

@@ -1,0 +1,262 @@
+// setops.cu -- merge-path union, set difference, trie views, scans.
+//
+// merge_disjoint replaces DSAI::merge (thrust::merge + set_union on root
+// keys, RT/gpu/device_sorted_array_index.ipp:709-847): FULL and DELTA are
+// disjoint sorted arrays, so FULL U DELTA is a plain merge whose output size
+// is known up front.  Each block owns one 2048-element output tile, finds
+// its two merge-path split points by binary search, stages both input
+// slices in shared memory with coalesced loads, merges 8 outputs per thread
+// and writes the tile back coalesced.
+//
+// set_difference replaces thrust::set_difference on the zipped columns
+// (.ipp:1104-1107) and the binary-probe variant (.ipp:933-1041): every
+// element of `a` is probed in the slice of `b` that its block's key range
+// can reach, then the survivors are compacted in order.
+#include <atomic>
+
+#include "compact.cuh"
+#include "kernels.h"
+
+namespace srdl {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launches(int k) { g_launches.fetch_add((uint64_t)k, std::memory_order_relaxed); }
+uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
+
+constexpr int kMgThreads = 256;
+constexpr int kMgItems = 8;
+constexpr int kMgTile = kMgThreads * kMgItems;
+
+// Number of elements taken from `a` among the first `diag` merged outputs
+// (ties resolve towards `a`).
+__device__ __forceinline__ uint64_t merge_path(const uint64_t* a, uint64_t na, const uint64_t* b,
+                                               uint64_t nb, uint64_t diag) {
+  uint64_t lo = diag > nb ? diag - nb : 0;
+  uint64_t hi = diag < na ? diag : na;
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) >> 1;
+    if (a[mid] <= b[diag - 1 - mid]) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kMgThreads) merge_kernel(const uint64_t* __restrict__ a,
+                                                           uint64_t na,
+                                                           const uint64_t* __restrict__ b,
+                                                           uint64_t nb,
+                                                           uint64_t* __restrict__ out) {
+  __shared__ uint64_t sin[kMgTile];
+  __shared__ uint64_t sout[kMgTile];
+  __shared__ uint64_t split[2];
+  const uint64_t total = na + nb;
+  const uint64_t d0 = (uint64_t)blockIdx.x * kMgTile;
+  const uint64_t d1 = d0 + kMgTile < total ? d0 + kMgTile : total;
+  if (threadIdx.x == 0) split[0] = merge_path(a, na, b, nb, d0);
+  if (threadIdx.x == 32) split[1] = merge_path(a, na, b, nb, d1);
+  __syncthreads();
+  const uint64_t i0 = split[0], i1 = split[1];
+  const uint64_t j0 = d0 - i0, j1 = d1 - i1;
+  const int la = (int)(i1 - i0), lb = (int)(j1 - j0), lt = la + lb;
+  for (int k = threadIdx.x; k < lt; k += kMgThreads) sin[k] = k < la ? a[i0 + k] : b[j0 + k - la];
+  __syncthreads();
+  const int ld = threadIdx.x * kMgItems;
+  if (ld < lt) {
+    int lo = ld > lb ? ld - lb : 0, hi = ld < la ? ld : la;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (sin[mid] <= sin[la + ld - 1 - mid]) lo = mid + 1;
+      else hi = mid;
+    }
+    int i = lo, j = ld - lo;
+#pragma unroll
+    for (int k = 0; k < kMgItems; k++) {
+      if (ld + k >= lt) break;
+      const bool take_a = (j >= lb) || (i < la && sin[i] <= sin[la + j]);
+      sout[ld + k] = take_a ? sin[i++] : sin[la + j++];
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < lt; k += kMgThreads) out[d0 + k] = sout[k];
+}
+
+void merge_disjoint(const Launch& L, const uint64_t* a, uint64_t na, const uint64_t* b,
+                    uint64_t nb, uint64_t* out) {
+  const uint64_t total = na + nb;
+  if (total == 0) return;
+  const uint64_t blocks = (total + kMgTile - 1) / kMgTile;
+  SRDL_REQUIRE(blocks < (1ull << 31), kErrCapacity, "merge: too many rows");
+  merge_kernel<<<(unsigned)blocks, kMgThreads, 0, L.stream>>>(a, na, b, nb, out);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(1);
+}
+
+size_t diff_scratch_bytes(uint64_t n) { return cp_scratch_bytes(n); }
+
+void set_difference(const Launch& L, const uint64_t* a, uint64_t na, const uint64_t* b,
+                    uint64_t nb, uint64_t* out, uint64_t* d_nout, Scratch& s) {
+  DedupDiffSel<uint64_t> sel{a, 32, false, b, nb, out};
+  compact(L, sel, na, d_nout, s);
+}
+
+__global__ void lo_kernel(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ lo) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    lo[i] = (uint32_t)keys[i];
+}
+
+__global__ void dir_kernel(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ dir,
+                           uint32_t dir_n) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < dir_n;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    dir[v] = (uint32_t)lower_bound_u64(keys, 0, n, v << 32);
+}
+
+__global__ void swap_kernel(const uint64_t* __restrict__ in, uint64_t n, uint64_t* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t k = in[i];
+    out[i] = (k << 32) | (k >> 32);
+  }
+}
+
+static int grid_for(uint64_t n, int sms) {
+  uint64_t g = (n + 255) / 256;
+  uint64_t cap = (uint64_t)sms * 16;
+  if (g > cap) g = cap;
+  return g ? (int)g : 1;
+}
+
+void build_lo(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* lo) {
+  if (!n) return;
+  lo_kernel<<<grid_for(n, L.num_sms), 256, 0, L.stream>>>(keys, n, lo);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(1);
+}
+
+void build_dir(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* dir, uint32_t dir_n) {
+  if (!dir_n) return;
+  dir_kernel<<<grid_for(dir_n, L.num_sms), 256, 0, L.stream>>>(keys, n, dir, dir_n);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(1);
+}
+
+size_t roots_scratch_bytes(uint64_t n) { return cp_scratch_bytes(n); }
+
+void build_roots(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* roots,
+                 uint64_t* d_nroots, Scratch& s) {
+  RootSel sel{keys, roots};
+  compact(L, sel, n, d_nroots, s);
+}
+
+void swap_halves(const Launch& L, const uint64_t* in, uint64_t n, uint64_t* out) {
+  if (!n) return;
+  swap_kernel<<<grid_for(n, L.num_sms), 256, 0, L.stream>>>(in, n, out);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(1);
+}
+
+__global__ void max_kernel(const uint32_t* __restrict__ d, uint64_t n, uint32_t* __restrict__ out) {
+  uint32_t m = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    m = max(m, d[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(kAllLanes, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+void max_u32(const Launch& L, const uint32_t* d, uint64_t n, uint32_t* d_max) {
+  SRDL_CUDA(cudaMemsetAsync(d_max, 0, sizeof(uint32_t), L.stream));
+  if (!n) return;
+  max_kernel<<<grid_for(n, L.num_sms), 256, 0, L.stream>>>(d, n, d_max);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(1);
+}
+
+// ------------------------------------------------------------------ scan
+
+constexpr int kScThreads = 256;
+constexpr int kScItems = 8;
+constexpr int kScTile = kScThreads * kScItems;
+
+__global__ void __launch_bounds__(kScThreads) scan_sum_kernel(const uint64_t* __restrict__ in,
+                                                              uint64_t n, uint64_t chunk,
+                                                              uint64_t* __restrict__ bsum) {
+  __shared__ uint64_t sh[kScThreads / 32 + 1];
+  const uint64_t begin = (uint64_t)blockIdx.x * chunk;
+  const uint64_t end = begin + chunk < n ? begin + chunk : n;
+  uint64_t s = 0;
+  for (uint64_t i = begin + threadIdx.x; i < end; i += kScThreads) s += in[i];
+  uint64_t tot;
+  block_excl_scan(s, sh, &tot);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+__global__ void scan_blocks_kernel(uint64_t* bsum, int nb) {
+  __shared__ uint64_t sh[1024 / 32 + 1];
+  const int per = (nb + blockDim.x - 1) / blockDim.x;
+  const int s = threadIdx.x * per, e = min(nb, s + per);
+  uint64_t sum = 0;
+  for (int i = s; i < e; i++) sum += bsum[i];
+  uint64_t tot;
+  uint64_t run = block_excl_scan(sum, sh, &tot);
+  for (int i = s; i < e; i++) {
+    uint64_t v = bsum[i];
+    bsum[i] = run;
+    run += v;
+  }
+  if (threadIdx.x == 0) bsum[nb] = tot;
+}
+
+__global__ void __launch_bounds__(kScThreads) scan_write_kernel(const uint64_t* __restrict__ in,
+                                                                uint64_t n, uint64_t chunk,
+                                                                const uint64_t* __restrict__ boff,
+                                                                uint64_t* __restrict__ out) {
+  __shared__ uint64_t sh[kScThreads / 32 + 1];
+  const uint64_t begin = (uint64_t)blockIdx.x * chunk;
+  const uint64_t end = begin + chunk < n ? begin + chunk : n;
+  uint64_t base = boff[blockIdx.x];
+  for (uint64_t tile = begin; tile < end; tile += kScTile) {
+    const uint64_t i0 = tile + (uint64_t)threadIdx.x * kScItems;
+    uint64_t v[kScItems];
+    uint64_t s = 0;
+#pragma unroll
+    for (int j = 0; j < kScItems; j++) {
+      v[j] = (i0 + j < end) ? in[i0 + j] : 0;
+      s += v[j];
+    }
+    uint64_t tot;
+    uint64_t run = base + block_excl_scan(s, sh, &tot);
+#pragma unroll
+    for (int j = 0; j < kScItems; j++) {
+      if (i0 + j < end) out[i0 + j] = run;
+      run += v[j];
+    }
+    base += tot;
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = boff[gridDim.x];
+}
+
+size_t scan_scratch_bytes(uint64_t) { return (size_t)(256 * 8 + 2) * 8 + 512; }
+
+void exclusive_scan_u64(const Launch& L, const uint64_t* in, uint64_t n, uint64_t* out,
+                        Scratch& s) {
+  if (n == 0) {
+    SRDL_CUDA(cudaMemsetAsync(out, 0, sizeof(uint64_t), L.stream));
+    return;
+  }
+  const uint64_t tiles = (n + kScTile - 1) / kScTile;
+  const uint64_t cap = (uint64_t)L.num_sms * 8;
+  const uint64_t per = (tiles + cap - 1) / cap;
+  const uint64_t chunk = (per ? per : 1) * kScTile;
+  const int nb = (int)((n + chunk - 1) / chunk);
+  uint64_t* bsum = s.take<uint64_t>(nb + 1);
+  scan_sum_kernel<<<nb, kScThreads, 0, L.stream>>>(in, n, chunk, bsum);
+  scan_blocks_kernel<<<1, 1024, 0, L.stream>>>(bsum, nb);
+  scan_write_kernel<<<nb, kScThreads, 0, L.stream>>>(in, n, chunk, bsum, out);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(3);
+}
+
+}  // namespace srdl

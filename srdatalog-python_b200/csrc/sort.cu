@@ -1,0 +1,244 @@
+// sort.cu -- index build: LSD radix sort of packed keys + fused dedup / difference.
+//
+// Replaces rebuild_index_fn -> zip_sort_columns (thrust::sort on a zip
+// iterator, a CUB merge sort: RT/gpu/sort.h:297-302) followed by
+// deduplicate_aggregate_and_unique (RT/gpu/deduplication.h:178-258) and, for
+// ComputeDeltaIndex, DSAI::set_difference_update
+// (RT/gpu/device_sorted_array_index.ipp:966-1130).
+//
+// Design.  Datalog creates no values: every value of every relation comes
+// from the loaded inputs (and rule constants), so the runtime knows a bound
+// 2^bits on all values.  A two-column key (hi, lo) is compressed to
+// (hi << bits) | lo -- 32 bits when 2*bits <= 32 -- and sorted with
+// ceil(2*bits / 8) stable counting passes.  Each pass is a histogram launch
+// (shared-memory counters per block), one single-block scan, and a scatter
+// launch in which every warp ranks its keys with __match_any_sync, the tile
+// is staged in shared memory in digit order and written out coalesced.  No
+// block ever waits on another.  The dedup (and optional "not in FULL" test)
+// runs as one order-preserving compaction over the sorted keys that also
+// expands them back to (hi << 32) | lo.
+#include "compact.cuh"
+#include "kernels.h"
+
+namespace srdl {
+
+constexpr int kRsThreads = 256;
+constexpr int kRsWarps = kRsThreads / 32;
+constexpr int kRsPerWarp = 256;                  // keys per warp per tile
+constexpr int kRsTile = kRsWarps * kRsPerWarp;   // 2048 keys per tile
+constexpr int kRsBins = 256;
+
+int value_bits(uint32_t max_value) {
+  int b = 0;
+  while (b < 32 && (uint64_t(max_value) >> b) != 0) b++;
+  return b ? b : 1;
+}
+
+__global__ void cp_scan_kernel(const uint32_t* blk_counts, int nb, uint64_t* offs,
+                               uint64_t* d_total) {
+  __shared__ uint64_t sh[1024 / 32 + 1];
+  const int per = (nb + blockDim.x - 1) / blockDim.x;
+  const int s = threadIdx.x * per, e = min(nb, s + per);
+  uint64_t sum = 0;
+  for (int i = s; i < e; i++) sum += blk_counts[i];
+  uint64_t tot;
+  uint64_t run = block_excl_scan(sum, sh, &tot);
+  for (int i = s; i < e; i++) {
+    offs[i] = run;
+    run += blk_counts[i];
+  }
+  if (threadIdx.x == 0) {
+    offs[nb] = tot;
+    *d_total = tot;
+  }
+}
+
+template <typename K>
+__global__ void rs_pack(const uint64_t* __restrict__ in, uint64_t n, int bits, bool swap,
+                        K* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t k = in[i];
+    uint64_t hi = k >> 32, lo = k & 0xffffffffull;
+    if (swap) {
+      uint64_t t = hi;
+      hi = lo;
+      lo = t;
+    }
+    out[i] = (K)((hi << bits) | lo);
+  }
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kRsThreads) rs_hist(const K* __restrict__ keys, uint64_t n,
+                                                      uint64_t chunk, int shift, int nbins,
+                                                      uint32_t* __restrict__ counts) {
+  __shared__ uint32_t h[kRsBins];
+  for (int d = threadIdx.x; d < nbins; d += kRsThreads) h[d] = 0;
+  __syncthreads();
+  const uint64_t begin = (uint64_t)blockIdx.x * chunk;
+  const uint64_t end = begin + chunk < n ? begin + chunk : n;
+  const uint32_t mask = nbins - 1;
+  for (uint64_t i = begin + threadIdx.x; i < end; i += kRsThreads)
+    atomicAdd(&h[(uint32_t)(keys[i] >> shift) & mask], 1u);
+  __syncthreads();
+  for (int d = threadIdx.x; d < nbins; d += kRsThreads) counts[(uint64_t)d * gridDim.x + blockIdx.x] = h[d];
+}
+
+// Exclusive scan of L uint32 counters in place (digit-major), one block.
+__global__ void rs_scan(uint32_t* c, uint32_t L) {
+  __shared__ uint32_t sh[1024 / 32 + 1];
+  const uint32_t per = (L + blockDim.x - 1) / blockDim.x;
+  const uint32_t s = threadIdx.x * per, e = min(L, s + per);
+  uint32_t sum = 0;
+  for (uint32_t i = s; i < e; i++) sum += c[i];
+  uint32_t tot;
+  uint32_t run = block_excl_scan(sum, sh, &tot);
+  for (uint32_t i = s; i < e; i++) {
+    uint32_t v = c[i];
+    c[i] = run;
+    run += v;
+  }
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kRsThreads) rs_scatter(const K* __restrict__ in,
+                                                         K* __restrict__ out, uint64_t n,
+                                                         uint64_t chunk, int shift, int nbins,
+                                                         const uint32_t* __restrict__ offs) {
+  __shared__ uint32_t base[kRsBins];             // global output position per digit
+  __shared__ uint32_t wcnt[kRsWarps][kRsBins];   // per-warp digit counts -> warp offsets
+  __shared__ uint32_t tstart[kRsBins];           // digit start inside the staged tile
+  __shared__ uint32_t tot[kRsBins];
+  __shared__ uint32_t scan_sh[kRsThreads / 32 + 1];
+  __shared__ K stage[kRsTile];
+
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const uint32_t mask = nbins - 1;
+  for (int d = threadIdx.x; d < kRsBins; d += kRsThreads)
+    base[d] = d < nbins ? offs[(uint64_t)d * gridDim.x + blockIdx.x] : 0;
+  const uint64_t begin = (uint64_t)blockIdx.x * chunk;
+  const uint64_t end = begin + chunk < n ? begin + chunk : n;
+
+  for (uint64_t tile = begin; tile < end; tile += kRsTile) {
+    for (int d = threadIdx.x; d < kRsWarps * kRsBins; d += kRsThreads) (&wcnt[0][0])[d] = 0;
+    __syncthreads();
+    K key[kRsPerWarp / 32];
+    uint32_t rank[kRsPerWarp / 32];
+    uint32_t dig[kRsPerWarp / 32];
+    // Warp `wid` owns keys [tile + wid*256, +256) in rounds of 32, so the
+    // (round, lane) order is the input order: ranks are stable.
+#pragma unroll
+    for (int r = 0; r < kRsPerWarp / 32; r++) {
+      const uint64_t i = tile + (uint64_t)wid * kRsPerWarp + r * 32 + lane;
+      const bool valid = i < end;
+      key[r] = valid ? in[i] : K(0);
+      const uint32_t d = valid ? ((uint32_t)(key[r] >> shift) & mask) : (uint32_t)kRsBins;
+      const unsigned peers = __match_any_sync(kAllLanes, d);
+      const int leader = __ffs(peers) - 1;
+      uint32_t old = 0;
+      if (lane == leader && valid) {
+        old = wcnt[wid][d];
+        wcnt[wid][d] = old + __popc(peers);
+      }
+      old = __shfl_sync(kAllLanes, old, leader);
+      rank[r] = old + __popc(peers & lanemask_lt());
+      dig[r] = d;
+      __syncwarp();
+    }
+    __syncthreads();
+    // Per digit: exclusive prefix over warps, and the tile total.
+    {
+      const int d = threadIdx.x;  // kRsThreads == kRsBins
+      uint32_t run = 0;
+#pragma unroll
+      for (int w = 0; w < kRsWarps; w++) {
+        uint32_t c = wcnt[w][d];
+        wcnt[w][d] = run;
+        run += c;
+      }
+      tot[d] = run;
+      uint32_t all;
+      tstart[d] = block_excl_scan(run, scan_sh, &all);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kRsPerWarp / 32; r++) {
+      if (dig[r] < (uint32_t)kRsBins) {
+        const uint32_t d = dig[r];
+        stage[tstart[d] + wcnt[wid][d] + rank[r]] = key[r];
+      }
+    }
+    __syncthreads();
+    const uint32_t cnt = (uint32_t)((end - tile) < kRsTile ? (end - tile) : kRsTile);
+    for (uint32_t j = threadIdx.x; j < cnt; j += kRsThreads) {
+      const K k = stage[j];
+      const uint32_t d = (uint32_t)(k >> shift) & mask;
+      out[base[d] + (j - tstart[d])] = k;
+    }
+    __syncthreads();
+    base[threadIdx.x] += tot[threadIdx.x];
+    __syncthreads();
+  }
+}
+
+static inline bool use32(int bits) { return 2 * bits <= 32; }
+
+size_t sort_scratch_bytes(uint64_t n, int bits) {
+  const size_t ks = use32(bits) ? 4 : 8;
+  const uint64_t chunk = ((n + kRsTile - 1) / kRsTile + 148 * 8 - 1) / (148 * 8);
+  (void)chunk;
+  const size_t counts = (size_t)kRsBins * 256 * 8 * 4;  // <= 8 blocks per SM, 256 SMs
+  return 2 * (((n * ks) + 255) & ~size_t(255)) + counts + 256 + cp_scratch_bytes(n) + 1024;
+}
+
+template <typename K>
+static void sort_dedup_t(const Launch& L, const uint64_t* in, uint64_t n, int bits, bool swap,
+                         const uint64_t* full, uint64_t n_full, uint64_t* out,
+                         uint64_t* d_nout, Scratch& s) {
+  SRDL_REQUIRE(n < (1ull << 32), kErrCapacity, "sort: more than 2^32-1 rows in one index");
+  K* a = s.take<K>(n);
+  K* b = s.take<K>(n);
+  const int pgrid = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)L.num_sms * 16);
+  rs_pack<K><<<pgrid ? pgrid : 1, 256, 0, L.stream>>>(in, n, bits, swap, a);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(1);
+
+  // Tile partition shared by the histogram and scatter launches.
+  const uint64_t tiles = (n + kRsTile - 1) / kRsTile;
+  const uint64_t cap = (uint64_t)L.num_sms * 8;
+  const uint64_t per = (tiles + cap - 1) / cap;
+  const uint64_t chunk = (per ? per : 1) * kRsTile;
+  const int nb = (int)((n + chunk - 1) / chunk);
+  uint32_t* counts = s.take<uint32_t>((size_t)kRsBins * nb);
+
+  const int total_bits = 2 * bits;
+  const int passes = (total_bits + 7) / 8;
+  int shift = 0;
+  for (int p = 0; p < passes && n > 1; p++) {
+    const int w = total_bits / passes + (p < total_bits % passes ? 1 : 0);
+    const int nbins = 1 << w;
+    rs_hist<K><<<nb, kRsThreads, 0, L.stream>>>(a, n, chunk, shift, nbins, counts);
+    rs_scan<<<1, 1024, 0, L.stream>>>(counts, (uint32_t)(nbins * nb));
+    rs_scatter<K><<<nb, kRsThreads, 0, L.stream>>>(a, b, n, chunk, shift, nbins, counts);
+    SRDL_CUDA(cudaGetLastError());
+    count_launches(3);
+    std::swap(a, b);
+    shift += w;
+  }
+  DedupDiffSel<K> sel{a, bits, true, full, n_full, out};
+  compact(L, sel, n, d_nout, s);
+}
+
+void sort_dedup(const Launch& L, const uint64_t* in, uint64_t n, int bits, bool swap,
+                const uint64_t* full, uint64_t n_full, uint64_t* out, uint64_t* d_nout,
+                Scratch& s) {
+  if (n == 0) {
+    SRDL_CUDA(cudaMemsetAsync(d_nout, 0, sizeof(uint64_t), L.stream));
+    return;
+  }
+  if (use32(bits)) sort_dedup_t<uint32_t>(L, in, n, bits, swap, full, n_full, out, d_nout, s);
+  else sort_dedup_t<uint64_t>(L, in, n, bits, swap, full, n_full, out, d_nout, s);
+}
+
+}  // namespace srdl

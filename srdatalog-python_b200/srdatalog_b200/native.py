@@ -1,0 +1,167 @@
+'''ctypes binding of libsrdl (include/srdl.h) and a Python handle wrapper.
+
+There is no fallback: if libsrdl.so is missing or fails to load, every
+entry point raises.  Build it with `make -C srdatalog-python_b200/csrc`
+or `python -c "import __graft_entry__; __graft_entry__.build()"`.
+'''
+
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, 'lib', 'libsrdl.so')
+
+_u64 = ctypes.c_uint64
+_i64 = ctypes.c_int64
+_vp = ctypes.c_void_p
+_cp = ctypes.c_char_p
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+
+# name -> (restype, argtypes); mirrors include/srdl.h
+SIGNATURES = {
+  'srdl_last_error': (_cp, []),
+  'srdl_version': (ctypes.c_int, []),
+  'srdl_open': (ctypes.c_int, [_cp, ctypes.c_int, ctypes.POINTER(_vp)]),
+  'srdl_close': (ctypes.c_int, [_vp]),
+  'srdl_init_device': (ctypes.c_int, [_vp]),
+  'srdl_load_rows': (ctypes.c_int, [_vp, _cp, _u32p, _u64]),
+  'srdl_load_csv': (ctypes.c_int, [_vp, _cp, _cp]),
+  'srdl_load_all': (ctypes.c_int, [_vp, _cp]),
+  'srdl_staged_rows': (_u64, [_vp, _cp]),
+  'srdl_load_device_rows': (ctypes.c_int, [_vp, _cp, _vp, _u64]),
+  'srdl_set_stream': (ctypes.c_int, [_vp, _vp]),
+  'srdl_set_profiling': (ctypes.c_int, [_vp, ctypes.c_int]),
+  'srdl_launch_count': (_u64, []),
+  'srdl_run': (ctypes.c_int, [_vp, _u64]),
+  'srdl_size': (_u64, [_vp, _cp]),
+  'srdl_count': (_u64, [_vp, _cp]),
+  'srdl_dump': (_i64, [_vp, _cp, _u32p, _u64]),
+  'srdl_stats_json': (ctypes.c_int, [_vp, ctypes.c_char_p, _u64]),
+  'srdl_sort_unique_scratch_bytes': (_u64, [_u64, ctypes.c_int]),
+  'srdl_sort_unique_u64': (ctypes.c_int, [_vp, _u64, ctypes.c_int, _vp, _vp, _vp, _u64, _vp]),
+  'srdl_set_difference_scratch_bytes': (_u64, [_u64]),
+  'srdl_set_difference_u64': (ctypes.c_int, [_vp, _u64, _vp, _u64, _vp, _vp, _vp, _u64, _vp]),
+  'srdl_merge_u64': (ctypes.c_int, [_vp, _u64, _vp, _u64, _vp, _vp]),
+}
+
+_LIB = None
+
+
+class SrdlError(RuntimeError):
+  def __init__(self, what: str, code: int, msg: str):
+    super().__init__(f'{what} failed with status {code}: {msg}')
+    self.code = code
+
+
+def lib() -> ctypes.CDLL:
+  '''Load libsrdl.so once; raises if it is absent (no CPU fallback exists).'''
+  global _LIB
+  if _LIB is None:
+    if not os.path.exists(LIB_PATH):
+      raise OSError(f'libsrdl.so not built ({LIB_PATH}); run make -C srdatalog-python_b200/csrc')
+    L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+    for name, (res, args) in SIGNATURES.items():
+      f = getattr(L, name)
+      f.restype = res
+      f.argtypes = args
+    _LIB = L
+  return _LIB
+
+
+def last_error() -> str:
+  return lib().srdl_last_error().decode()
+
+
+def check(rc: int, what: str) -> None:
+  if rc != 0:
+    raise SrdlError(what, rc, last_error())
+
+
+class Database:
+  '''One plan bound to one GPU (handle API of libsrdl).'''
+
+  def __init__(self, plan, device: int = 0):
+    text = plan if isinstance(plan, str) else json.dumps(plan)
+    self.plan = json.loads(text)
+    h = _vp()
+    check(lib().srdl_open(text.encode(), device, ctypes.byref(h)), 'srdl_open')
+    self._h = h
+    self._arity = {r['name']: r['arity'] for r in self.plan['relations']}
+
+  def close(self) -> None:
+    if getattr(self, '_h', None):
+      lib().srdl_close(self._h)
+      self._h = None
+
+  def __del__(self):
+    try:
+      self.close()
+    except Exception:
+      pass
+
+  def __enter__(self):
+    return self
+
+  def __exit__(self, *exc):
+    self.close()
+
+  def init_device(self) -> None:
+    check(lib().srdl_init_device(self._h), 'srdl_init_device')
+
+  def load_rows(self, rel: str, rows) -> None:
+    a = np.ascontiguousarray(rows, dtype=np.uint32)
+    n = a.shape[0] if a.ndim > 1 else (a.shape[0] // max(1, self._arity.get(rel, 1)))
+    check(lib().srdl_load_rows(self._h, rel.encode(), a.ctypes.data_as(_u32p), n),
+          f'srdl_load_rows({rel})')
+
+  def load_csv(self, rel: str, path: str) -> None:
+    check(lib().srdl_load_csv(self._h, rel.encode(), path.encode()), f'srdl_load_csv({rel})')
+
+  def load_all(self, directory: str) -> None:
+    check(lib().srdl_load_all(self._h, directory.encode()), 'srdl_load_all')
+
+  def load_device_rows(self, rel: str, ptr: int, n_rows: int) -> None:
+    '''Stage n_rows uint32 pairs already in device memory at `ptr`.'''
+    check(lib().srdl_load_device_rows(self._h, rel.encode(), ptr, n_rows),
+          f'srdl_load_device_rows({rel})')
+
+  def set_stream(self, stream_ptr: int) -> None:
+    check(lib().srdl_set_stream(self._h, stream_ptr), 'srdl_set_stream')
+
+  def set_profiling(self, on: bool = True) -> None:
+    check(lib().srdl_set_profiling(self._h, 1 if on else 0), 'srdl_set_profiling')
+
+  def staged_rows(self, rel: str) -> int:
+    return int(lib().srdl_staged_rows(self._h, rel.encode()))
+
+  def run(self, max_iters: int = 0) -> None:
+    check(lib().srdl_run(self._h, max_iters), 'srdl_run')
+
+  def size(self, rel: str) -> int:
+    return int(lib().srdl_size(self._h, rel.encode()))
+
+  def count(self, rule: str) -> int:
+    return int(lib().srdl_count(self._h, rule.encode()))
+
+  def dump(self, rel: str) -> np.ndarray:
+    '''FULL(rel) as an (n, arity) uint32 array, sorted in declared column order.'''
+    n = lib().srdl_dump(self._h, rel.encode(), None, 0)
+    if n < 0:
+      raise SrdlError(f'srdl_dump({rel})', -n, last_error())
+    k = self._arity[rel]
+    out = np.empty((n, k), np.uint32)
+    if n:
+      m = lib().srdl_dump(self._h, rel.encode(), out.ctypes.data_as(_u32p), n)
+      if m != n:
+        raise SrdlError(f'srdl_dump({rel})', -1, 'size changed')
+    return out
+
+  def stats(self) -> dict:
+    buf = ctypes.create_string_buffer(1 << 16)
+    check(lib().srdl_stats_json(self._h, buf, len(buf)), 'srdl_stats_json')
+    return json.loads(buf.value.decode())

@@ -1,0 +1,133 @@
+'''Seeded synthetic inputs for the benchmark programs (uint32 edge lists).
+
+Every generator returns an (m, 2) uint32 numpy array of directed edges
+(column 0 = source, column 1 = target) in draw order, duplicates and
+self-loops already removed where the workload says so.  numpy's
+`Generator(PCG64(seed))` is the only randomness source, so a seed fully
+determines the input on every machine.
+
+These stand in for the reference's CSV inputs (examples/tc.py `Arc.csv`,
+examples/sg.py `Arc.csv`, examples/lsqb_triangle_count.py
+`Person_knows_Person.csv`); no public dataset is used.
+'''
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def _rng(seed: int) -> np.random.Generator:
+  return np.random.Generator(np.random.PCG64(seed))
+
+
+def _dedup_in_order(src: np.ndarray, dst: np.ndarray) -> np.ndarray:
+  key = (src.astype(np.uint64) << np.uint64(32)) | dst.astype(np.uint64)
+  _, first = np.unique(key, return_index=True)
+  first.sort()
+  return np.stack([src[first], dst[first]], axis=1).astype(np.uint32)
+
+
+def uniform_edges(n_nodes: int, n_edges: int, seed: int = 1) -> np.ndarray:
+  '''TC input: draw (src,dst) uniformly in [0,n_nodes), drop self-loops,
+  keep the first `n_edges` distinct pairs in draw order.'''
+  if n_edges > n_nodes * (n_nodes - 1):
+    raise ValueError('more distinct edges requested than the graph can hold')
+  rng = _rng(seed)
+  out = np.zeros((0, 2), np.uint32)
+  batch = max(1024, int(n_edges * 1.3))
+  src_all = np.zeros(0, np.uint32)
+  dst_all = np.zeros(0, np.uint32)
+  while out.shape[0] < n_edges:
+    s = rng.integers(0, n_nodes, batch, dtype=np.uint32)
+    d = rng.integers(0, n_nodes, batch, dtype=np.uint32)
+    keep = s != d
+    src_all = np.concatenate([src_all, s[keep]])
+    dst_all = np.concatenate([dst_all, d[keep]])
+    out = _dedup_in_order(src_all, dst_all)
+  return np.ascontiguousarray(out[:n_edges])
+
+
+def tc_small(seed: int = 1) -> np.ndarray:
+  '''Transitive-closure config: 20,000 distinct directed edges over 5,000 nodes.'''
+  return uniform_edges(5000, 20000, seed)
+
+
+def sg_forest(n_nodes: int = 200_000, window: int = 1000, cross_frac: float = 0.1,
+              seed: int = 2) -> np.ndarray:
+  '''Same-generation config: node i>0 takes a parent uniform in
+  [max(0,i-window), i-1]; round(cross_frac*(n-1)) extra cross edges (u,v)
+  with u<v after ordering, self-pairs dropped; all edges deduplicated.
+  Edges point parent -> child (Arc(p, x)).'''
+  rng = _rng(seed)
+  i = np.arange(1, n_nodes, dtype=np.int64)
+  lo = np.maximum(0, i - window)
+  par = lo + (rng.random(i.shape[0]) * (i - lo)).astype(np.int64)
+  par = np.minimum(par, i - 1)
+  n_cross = int(round(cross_frac * (n_nodes - 1)))
+  u = rng.integers(0, n_nodes, n_cross, dtype=np.int64)
+  v = rng.integers(0, n_nodes, n_cross, dtype=np.int64)
+  a, b = np.minimum(u, v), np.maximum(u, v)
+  keep = a != b
+  src = np.concatenate([par, a[keep]]).astype(np.uint32)
+  dst = np.concatenate([i, b[keep]]).astype(np.uint32)
+  return _dedup_in_order(src, dst)
+
+
+def rmat_edges(scale: int = 20, n_draws: int = 1 << 24, abcd=(0.57, 0.19, 0.19, 0.05),
+               seed: int = 3, chunk: int = 1 << 22) -> np.ndarray:
+  '''Triangle config: R-MAT with 2^scale nodes and n_draws draws; each
+  edge oriented as (min, max); self-loops and duplicates removed.'''
+  a, b, c, _ = abcd
+  rng = _rng(seed)
+  srcs, dsts = [], []
+  left = n_draws
+  while left > 0:
+    k = min(chunk, left)
+    s = np.zeros(k, np.uint32)
+    d = np.zeros(k, np.uint32)
+    for level in range(scale):
+      r = rng.random(k)
+      bit = np.uint32(1 << (scale - 1 - level))
+      down = r >= a + b            # quadrant c or d: source bit set
+      right = ((r >= a) & (r < a + b)) | (r >= a + b + c)  # b or d: target bit set
+      s |= np.where(down, bit, np.uint32(0))
+      d |= np.where(right, bit, np.uint32(0))
+    srcs.append(s)
+    dsts.append(d)
+    left -= k
+  s = np.concatenate(srcs)
+  d = np.concatenate(dsts)
+  lo, hi = np.minimum(s, d), np.maximum(s, d)
+  keep = lo != hi
+  return _dedup_in_order(lo[keep], hi[keep])
+
+
+def er_instance(n_nodes: int, mean_deg: float, seed: int) -> np.ndarray:
+  '''Batched-TC instance: round(mean_deg*n) directed Erdos-Renyi draws,
+  self-loops and duplicates removed.'''
+  rng = _rng(seed)
+  m = int(round(mean_deg * n_nodes))
+  s = rng.integers(0, n_nodes, m, dtype=np.uint32)
+  d = rng.integers(0, n_nodes, m, dtype=np.uint32)
+  keep = s != d
+  return _dedup_in_order(s[keep], d[keep])
+
+
+def batched_instances(count: int = 4096, n_lo: int = 64, n_hi: int = 65536,
+                      deg_lo: float = 2.0, deg_hi: float = 8.0, seed0: int = 1000):
+  '''Batched-fixpoint config: instance j has n_j = round(exp(U[ln n_lo, ln n_hi]))
+  nodes and mean out-degree U[deg_lo, deg_hi], generated with seed seed0+j.'''
+  out = []
+  for j in range(count):
+    rng = _rng(seed0 + j)
+    n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
+    c = float(rng.uniform(deg_lo, deg_hi))
+    out.append(er_instance(n, c, seed0 + j + 1_000_000))
+  return out
+
+
+def write_csv(edges: np.ndarray, path: str, delimiter: str = '\t') -> None:
+  '''Write an edge list as the reference's loader reads it (one row per line).'''
+  np.savetxt(path, edges.astype(np.int64), fmt='%d', delimiter=delimiter)

@@ -1,0 +1,137 @@
+'''Whole programs on the GPU, bit-exact against the oracle (size + SHA-256 of
+the sorted dump, or the count for count-only rules).'''
+
+import ctypes
+
+import numpy as np
+import oracle
+import pytest
+from conftest import load_plan
+from srdatalog_b200 import native
+from srdatalog_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def run(plan_name, inputs, max_iters=0):
+  db = native.Database(load_plan(plan_name))
+  for rel, rows in inputs.items():
+    db.load_rows(rel, rows)
+  db.run(max_iters)
+  return db
+
+
+def rows_set(a):
+  return {tuple(map(int, r)) for r in a}
+
+
+def test_tc_small_config(expected):
+  exp = expected['tc_small']
+  db = run('tc', {'ArcInput': W.tc_small(1)})
+  assert db.size('Path') == exp['size']
+  rows = db.dump('Path')
+  assert oracle.dump_hash(rows) == exp['sha256']
+  rec = [s for s in db.stats()['steps'] if s['recursive']]
+  assert rec[0]['iterations'] == exp['iterations']
+
+
+@pytest.mark.parametrize('seed', range(6))
+def test_tc_random_small_vs_interpreter(seed):
+  e = W.uniform_edges(40 + 10 * seed, 90 + 30 * seed, seed)
+  db = run('tc', {'ArcInput': e})
+  want, _ = oracle.run_plan(load_plan('tc'), {'ArcInput': e})
+  assert rows_set(db.dump('Path')) == set(want['Path'])
+
+
+def test_tc_mid_and_left_recursive(expected):
+  exp = expected['tc_mid']
+  e = W.uniform_edges(2000, 6000, 7)
+  for plan in ('tc', 'tc_left'):
+    db = run(plan, {'ArcInput': e})
+    assert db.size('Path') == exp['size']
+    assert oracle.dump_hash(db.dump('Path')) == exp['sha256']
+
+
+def test_tc_edge_cases():
+  db = run('tc', {'ArcInput': np.zeros((0, 2), np.uint32)})
+  assert db.size('Path') == 0 and db.dump('Path').shape == (0, 2)
+  e = np.array([[1, 1], [1, 2], [1, 2], [2, 1]], np.uint32)   # self-loop + duplicate row
+  db = run('tc', {'ArcInput': e})
+  assert rows_set(db.dump('Path')) == {(1, 1), (1, 2), (2, 1), (2, 2)}
+  chain = np.array([(i, i + 1) for i in range(30)], np.uint32)
+  for k in (1, 2, 5):
+    db = run('tc', {'ArcInput': chain}, max_iters=k)
+    keys, _, _ = oracle.tc(chain, max_iters=k)
+    assert db.size('Path') == keys.shape[0]
+  top = 0xFFFFFFFF
+  big = np.array([[top, 5], [5, top - 1], [top - 1, top], [7, 0]], np.uint32)
+  db = run('tc', {'ArcInput': big})
+  keys, _, _ = oracle.tc(big)
+  assert rows_set(db.dump('Path')) == rows_set(oracle.unpack(keys, order=(1, 0)))
+
+
+def test_repeat_run_same_result():
+  e = W.uniform_edges(500, 1500, 3)
+  db = run('tc', {'ArcInput': e})
+  h1 = oracle.dump_hash(db.dump('Path'))
+  db.run()
+  assert oracle.dump_hash(db.dump('Path')) == h1
+
+
+@pytest.mark.parametrize('name', ['sg_2k', 'sg_10k'])
+def test_sg_configs(expected, name):
+  exp = expected[name]
+  n, seed = (2000, 4) if name == 'sg_2k' else (10000, 2)
+  db = run('sg', {'Arc': W.sg_forest(n, seed=seed)})
+  assert db.size('Sg') == exp['size']
+  assert oracle.dump_hash(db.dump('Sg')) == exp['sha256']
+
+
+def test_sg_small_vs_interpreter():
+  e = W.sg_forest(150, window=12, seed=5)
+  db = run('sg', {'Arc': e})
+  want, _ = oracle.run_plan(load_plan('sg'), {'Arc': e})
+  assert rows_set(db.dump('Sg')) == set(want['Sg'])
+
+
+def test_triangle_known_answers():
+  import math
+  for n in (3, 5, 40):
+    e = np.array([(i, j) for i in range(n) for j in range(i + 1, n)], np.uint32)
+    db = run('triangle', {'KnowsInput': e})
+    assert db.count('TriangleJoin') == math.comb(n, 3)
+  db = run('triangle', {'KnowsInput': np.zeros((0, 2), np.uint32)})
+  assert db.count('TriangleJoin') == 0
+
+
+@pytest.mark.parametrize('name,scale,draws,seed', [('triangle_rmat14', 14, 1 << 18, 5),
+                                                    ('triangle_rmat20', 20, 1 << 24, 3)])
+def test_triangle_configs(expected, name, scale, draws, seed):
+  e = W.rmat_edges(scale, draws, seed=seed)
+  db = run('triangle', {'KnowsInput': e})
+  assert db.count('TriangleJoin') == expected[name]['count']
+  assert db.size('Knows') == expected[name]['edges']
+
+
+def test_shim_end_to_end(tmp_path, expected):
+  from srdatalog_b200.build import CompilerConfig, compile_jit_project, write_project
+  proj = write_project(load_plan('tc'), 'TcPlan', cache_base=str(tmp_path))
+  br = compile_jit_project(proj, CompilerConfig())
+  assert br.ok()
+  lib = ctypes.CDLL(br.artifact)
+  lib.srdatalog_load_all.argtypes = [ctypes.c_char_p]
+  lib.srdatalog_run.argtypes = [ctypes.c_ulonglong]
+  lib.srdatalog_size.argtypes = [ctypes.c_char_p]
+  lib.srdatalog_size.restype = ctypes.c_ulonglong
+  lib.srdatalog_dump.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint32), ctypes.c_ulonglong]
+  lib.srdatalog_dump.restype = ctypes.c_longlong
+  W.write_csv(W.uniform_edges(2000, 6000, 7), str(tmp_path / 'Arc.csv'))
+  assert lib.srdatalog_init() == 0
+  assert lib.srdatalog_load_all(str(tmp_path).encode()) == 0
+  assert lib.srdatalog_run(0) == 0
+  n = lib.srdatalog_size(b'Path')
+  assert n == expected['tc_mid']['size']
+  buf = np.empty((n, 2), np.uint32)
+  assert lib.srdatalog_dump(b'Path', buf.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), n) == n
+  assert oracle.dump_hash(buf) == expected['tc_mid']['sha256']
+  assert lib.srdatalog_shutdown() == 0
