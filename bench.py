@@ -187,6 +187,8 @@ def main():
   ap.add_argument('--impl', default='srdl', choices=['srdl', 'reference'])
   ap.add_argument('--workload', default='triangle', choices=sorted(WORKLOADS))
   ap.add_argument('--no-cpu-baseline', action='store_true')
+  ap.add_argument('--quick', action='store_true',
+                  help='kernel-resident path only (no e2e, no CPU baseline): for profiler runs')
   args = ap.parse_args()
   args.warmup = max(args.warmup, 3)
 
@@ -262,6 +264,13 @@ def main():
   del d_edges
 
   # ---------------- end-to-end path through the C ABI with host inputs (e2e)
+  if args.quick:
+    if dist:
+      dist.destroy_process_group()
+    if rank == 0:
+      print(json.dumps({'metric': f'tuples/s ({args.workload})', 'value': value,
+                        'ms_per_step': total_ms / args.steps, 'quick': True}), flush=True)
+    return
   db2 = Database(plan, device=local)
   db2.set_stream(stream.cuda_stream)
   db2.load_rows(wl['rel'], edges)
