@@ -62,6 +62,11 @@ struct TrieView {
   const uint32_t* lo = nullptr;     // n child values (low words of keys)
   const uint32_t* roots = nullptr;  // n_roots distinct first-column values
   const uint32_t* dir = nullptr;    // dense directory, dir_n = domain + 2 entries, or null
+  // Hashed child lists (dense directory only): hdir[v] = first slot of the
+  // open-addressing table holding the children of v, or kNoHash; the table
+  // has hash_cap(len) slots for a list of len children.
+  const uint32_t* hdir = nullptr;
+  const uint32_t* hpool = nullptr;
   uint64_t n = 0;
   uint32_t n_roots = 0;
   uint32_t dir_n = 0;
@@ -108,6 +113,20 @@ __device__ __forceinline__ void trie_range(const TrieView& t, uint32_t v, uint32
   }
 }
 
+constexpr uint32_t kNoHash = 0xffffffffu;
+constexpr uint32_t kHashEmpty = 0xffffffffu;
+
+// log2 of the table size for a list of len children: load factor <= 1/2.
+__host__ __device__ __forceinline__ int hash_log2(uint32_t len) {
+  int k = 1;
+  while ((1u << k) < 2u * len) k++;
+  return k;
+}
+
+__host__ __device__ __forceinline__ uint32_t hash_slot(uint32_t x, int k) {
+  return (uint32_t)(((uint64_t)x * 0x9E3779B97F4A7C15ull) >> (64 - k));
+}
+
 __device__ __forceinline__ bool trie_has_root(const TrieView& t, uint32_t v) {
   uint32_t b, e;
   trie_range(t, v, b, e);
@@ -119,6 +138,30 @@ __device__ __forceinline__ bool child_contains(const TrieView& t, uint32_t b, ui
                                                uint32_t v) {
   uint32_t p = lower_bound_u32(t.lo, b, e, v);
   return p < e && t.lo[p] == v;
+}
+
+// Is v a child of prefix value pv?  Long lists answer from their hash table
+// (about two dependent loads), short ones by binary search.
+__device__ __forceinline__ bool trie_child_contains(const TrieView& t, uint32_t pv, uint32_t v) {
+  uint32_t b, e;
+  trie_range(t, pv, b, e);
+  if (b == e) return false;
+  if (t.hdir) {
+    const uint32_t off = t.hdir[pv];
+    if (off != kNoHash) {
+      const int k = hash_log2(e - b);
+      const uint32_t mask = (1u << k) - 1;
+      uint32_t h = hash_slot(v, k);
+      for (uint32_t probe = 0; probe <= mask; probe++) {
+        const uint32_t s = t.hpool[off + h];
+        if (s == v) return true;
+        if (s == kHashEmpty) return false;
+        h = (h + 1) & mask;
+      }
+      return false;
+    }
+  }
+  return child_contains(t, b, e, v);
 }
 
 __device__ __forceinline__ unsigned lanemask_lt() {

@@ -13,6 +13,7 @@
 // drops the keys already in FULL, so NEW is never written out separately.
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <sstream>
 
@@ -84,13 +85,19 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
     SRDL_REQUIRE(it != slot.end(), kErrPlan, "rule " + op.rule + ": unbound variable " + v);
     return it->second;
   };
-  auto make_src = [&](const SourceDesc& d) {
+  auto make_src = [&](const SourceDesc& d, bool probed) {
     Relation& r = rel(d.rel);
     Ver v = (d.ver == kDelta && recursive && iteration == 0) ? kFull : d.ver;
     SRDL_REQUIRE(r.arity <= 2, kErrUnsupported, "join over relation " + r.name + " of arity > 2");
     SRDL_REQUIRE(d.prefix.size() < (size_t)std::max(r.arity, 2), kErrUnsupported,
                  "rule " + op.rule + ": prefix too long on " + r.name);
     Index& ix = ensure_index(r, v, d.index);
+    // Hash long child lists of probed FULL indexes; a delta is rebuilt every
+    // iteration and is usually the short (driving) side anyway.
+    if (probed && !d.prefix.empty() && v == kFull) {
+      ensure_trie(r, ix);
+      ensure_hash(ix);
+    }
     SrcSpec s;
     s.t = view(r, ix);
     s.prefix_slot = d.prefix.empty() ? -1 : slot_of(d.prefix[0]);
@@ -123,20 +130,21 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
       const SourceDesc& d = po.sources[0];
       lv.kind = kScan;
       lv.nsrc = 1;
-      lv.src[0] = make_src(d);
+      lv.src[0] = make_src(d, false);
       SRDL_REQUIRE(po.vars.size() == d.index.size(), kErrPlan, "scan arity mismatch");
       for (size_t j = d.prefix.size(); j < po.vars.size(); j++) lv.scan_slot[j] = bind(po.vars[j]);
     } else if (po.kind == PipeOp::ColumnJoin) {
       lv.kind = kColumnJoin;
       SRDL_REQUIRE(po.sources.size() <= (size_t)kMaxSrc && !po.sources.empty(), kErrUnsupported,
                    "column join with too many sources");
-      for (auto& d : po.sources) lv.src[lv.nsrc++] = make_src(d);
+      // every list but the per-row shortest is probed: hash the long ones
+      for (auto& d : po.sources) lv.src[lv.nsrc++] = make_src(d, po.sources.size() > 1);
       lv.cj_slot = bind(po.var);
     } else {
       lv.kind = kCartesian;
       SRDL_REQUIRE(po.sources.size() <= (size_t)kMaxSrc, kErrUnsupported, "cartesian too wide");
       for (size_t i = 0; i < po.sources.size(); i++) {
-        lv.src[lv.nsrc] = make_src(po.sources[i]);
+        lv.src[lv.nsrc] = make_src(po.sources[i], false);
         const auto& vs = i < po.var_from_source.size() ? po.var_from_source[i]
                                                         : std::vector<std::string>{};
         SRDL_REQUIRE(vs.size() <= 1, kErrUnsupported, "cartesian source binding several variables");
@@ -160,7 +168,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
   for (size_t li = 0; li < levels.size(); li++) {
     LevelSpec& lv = levels[li];
     const bool last = li + 1 == levels.size();
-    DevBuf wscr(join_work_scratch_bytes(cur.n), L_.stream);
+    DevBuf wscr(join_work_scratch_bytes(cur.n) + join_expand_scratch_bytes(L_.num_sms), L_.stream);
     Scratch s{wscr.as<char>(), wscr.bytes(), 0};
     size_t pid = prof_begin("join_count");
     JoinWork w = join_count(L_, lv, cur, s);
@@ -173,7 +181,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
       if (op.count) {
         lv.emit = kEmitCount;
         pid = prof_begin("join_expand_count");
-        join_expand(L_, lv, cur, w, total, nullptr, nullptr, d_small_.as<uint64_t>() + 2);
+        join_expand(L_, lv, cur, w, total, nullptr, nullptr, d_small_.as<uint64_t>() + 2, s);
         // per candidate: its value (4 B) and one probed word of each other list (4 B)
         prof_end(pid, 4.0 * total * std::max(1, lv.nsrc), (double)total);
         counts_[op.rule] += read_scalar(2);
@@ -186,7 +194,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
         ch.keys = DevBuf(std::max<uint64_t>(total, 1) * 8, L_.stream);
         pid = prof_begin("join_expand_keys");
         join_expand(L_, lv, cur, w, total, nullptr, ch.keys.as<uint64_t>(),
-                    d_small_.as<uint64_t>() + 2);
+                    d_small_.as<uint64_t>() + 2, s);
         ch.n = total ? read_scalar(2) : 0;
         prof_end(pid, 4.0 * total * std::max(1, lv.nsrc) + 8.0 * ch.n, (double)total);
         derived_ += ch.n;
@@ -203,7 +211,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
         next.col[c] = cols.back().as<uint32_t>();
       }
       pid = prof_begin("join_expand_table");
-      join_expand(L_, lv, cur, w, total, &next, nullptr, d_small_.as<uint64_t>() + 2);
+      join_expand(L_, lv, cur, w, total, &next, nullptr, d_small_.as<uint64_t>() + 2, s);
       next.n = total ? read_scalar(2) : 0;
       prof_end(pid, 4.0 * total * std::max(1, lv.nsrc) + 4.0 * next.n * levels[li + 1].n_in_slots,
                (double)total);

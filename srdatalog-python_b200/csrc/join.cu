@@ -11,22 +11,26 @@
 //            driver), for a cartesian join the product of the lists, for a
 //            scan the scanned range;
 //   scan   : exclusive prefix sum of the counts (64-bit);
-//   expand : one thread per candidate.  Its row is found by binary search in
-//            the prefix sums, so a hub key with millions of candidates is
-//            spread over thousands of threads exactly like a leaf key with
-//            one (this replaces warp-per-root-key traversal plus the
+//   expand : one lane per candidate.  Every warp owns an equal, contiguous
+//            slice of the candidates and walks it 32 at a time, finding each
+//            lane's row by galloping forward in the prefix sums from the
+//            previous row.  A hub key with millions of candidates is thus
+//            spread over thousands of warps exactly like a leaf key with one
+//            (this replaces warp-per-root-key traversal plus the
 //            work-stealing / block-group balancing of the reference,
-//            ws_infrastructure.h and complete_runner.py:377-737).  A column
-//            join candidate is probed in every other source list by binary
-//            search; filters run next; survivors are appended with one
-//            warp-aggregated atomic per warp (row order does not matter: the
-//            next consumer is a sort), or only counted for count-only rules.
+//            ws_infrastructure.h and complete_runner.py:377-737), and no
+//            block ever synchronises.  A column-join candidate is probed in
+//            every other source list by binary search; filters run next.
+//            Final levels append keys with one warp-aggregated atomic per
+//            warp (the consumer sorts them) or only count; intermediate
+//            tables are written in input order (count pass + scan + write
+//            pass), so every binding table stays lexicographically sorted.
+
 #include "kernels.h"
 
 namespace srdl {
 
 constexpr int kJThreads = 256;
-
 // List of source s for input row r: [b, b+len) over roots (no prefix) or
 // over child values (prefix bound).
 __device__ __forceinline__ void src_list(const SrcSpec& s, const Table& in, uint64_t r,
@@ -48,9 +52,7 @@ __device__ __forceinline__ uint32_t src_value(const SrcSpec& s, uint32_t pos) {
 __device__ __forceinline__ bool src_contains(const SrcSpec& s, const Table& in, uint64_t r,
                                              uint32_t v) {
   if (s.prefix_slot < 0) return trie_has_root(s.t, v);
-  uint32_t b, e;
-  trie_range(s.t, in.col[s.prefix_slot][r], b, e);
-  return child_contains(s.t, b, e, v);
+  return trie_child_contains(s.t, in.col[s.prefix_slot][r], v);
 }
 
 __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Table in,
@@ -62,16 +64,18 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
     if (lv.kind == kColumnJoin) {
       uint32_t best = 0xffffffffu, bb = 0;
       int bd = 0;
+      bool empty = false;
       for (int s = 0; s < lv.nsrc; s++) {
         uint32_t b, len;
         src_list(lv.src[s], in, r, b, len);
+        empty |= len == 0;
         if (len < best) {
           best = len;
           bd = s;
           bb = b;
         }
       }
-      work[r] = best;
+      work[r] = empty ? 0 : best;
       drv[r] = (uint8_t)bd;
       beg[r] = bb;
     } else if (lv.kind == kCartesian) {
@@ -96,16 +100,21 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
   }
 }
 
-__device__ __forceinline__ uint64_t row_of(const uint64_t* offs, uint64_t lo, uint64_t hi,
-                                           uint64_t w) {
-  // largest r in [lo, hi) with offs[r] <= w
-  uint64_t a = lo, b = hi;
-  while (a + 1 < b) {
-    uint64_t m = (a + b) >> 1;
-    if (offs[m] <= w) a = m;
-    else b = m;
+// Largest r in [lo, n) with offs[r] <= w, given offs[lo] <= w: gallop, then bisect.
+__device__ __forceinline__ uint64_t gallop_row(const uint64_t* offs, uint64_t lo, uint64_t n,
+                                               uint64_t w) {
+  uint64_t step = 1;
+  while (lo + step < n && offs[lo + step] <= w) {
+    lo += step;
+    step <<= 1;
   }
-  return a;
+  uint64_t hi = lo + step < n ? lo + step : n;  // offs[hi] > w or hi == n
+  while (lo + 1 < hi) {
+    uint64_t m = (lo + hi) >> 1;
+    if (offs[m] <= w) lo = m;
+    else hi = m;
+  }
+  return lo;
 }
 
 __device__ __forceinline__ bool filt_ok(const FiltSpec& f, uint32_t a, uint32_t b) {
@@ -119,101 +128,100 @@ __device__ __forceinline__ bool filt_ok(const FiltSpec& f, uint32_t a, uint32_t 
   }
 }
 
-template <int EMIT>
+enum ExpandMode : int { kModeCount = 0, kModeKeys = 1, kModeTableCount = 2, kModeTableWrite = 3 };
+
+template <int MODE>
 __global__ void __launch_bounds__(kJThreads) join_expand_kernel(
     LevelSpec lv, Table in, const uint64_t* __restrict__ offs, const uint8_t* __restrict__ drv,
-    const uint32_t* __restrict__ beg, uint64_t total, Table out, uint64_t* __restrict__ out_keys,
-    unsigned long long* __restrict__ d_out_n) {
-  __shared__ uint64_t rows[2];
-  __shared__ unsigned long long red[kJThreads / 32];
+    const uint32_t* __restrict__ beg, uint64_t total, uint64_t chunk, Table out,
+    uint64_t* __restrict__ out_keys, unsigned long long* __restrict__ d_out_n,
+    uint64_t* __restrict__ warp_counts) {
   const int lane = threadIdx.x & 31;
-  unsigned long long my_count = 0;
-  for (uint64_t t0 = (uint64_t)blockIdx.x * kJThreads; t0 < total;
-       t0 += (uint64_t)gridDim.x * kJThreads) {
-    const uint64_t tlast = t0 + kJThreads - 1 < total ? t0 + kJThreads - 1 : total - 1;
-    if (threadIdx.x == 0) rows[0] = row_of(offs, 0, in.n, t0);
-    if (threadIdx.x == 32) rows[1] = row_of(offs, 0, in.n, tlast);
-    __syncthreads();
-    const uint64_t w = t0 + threadIdx.x;
-    bool ok = w < total;
-    uint64_t r = 0;
-    uint32_t nv[kMaxSrc + 1];  // values of the slots this level binds
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t c0 = gw * chunk;
+  const uint64_t c1 = c0 + chunk < total ? c0 + chunk : total;
+  unsigned long long running = 0;
+  if (MODE == kModeTableWrite) running = warp_counts[gw];
+  if (c0 < c1) {
+    uint64_t r0 = gallop_row(offs, 0, in.n, c0);
+    for (uint64_t base = c0; base < c1; base += 32) {
+      const uint64_t w = base + lane;
+      bool ok = w < c1;
+      uint64_t r = r0;
+      uint32_t nv[kMaxSrc + 1];  // values of the slots this level binds
 #pragma unroll
-    for (int i = 0; i < kMaxSrc + 1; i++) nv[i] = 0;
-    if (ok) {
-      r = row_of(offs, rows[0], rows[1] + 1, w);
-      const uint64_t local = w - offs[r];
-      if (lv.kind == kColumnJoin) {
-        const int d = drv[r];
-        const uint32_t v = src_value(lv.src[d], beg[r] + (uint32_t)local);
-        for (int s = 0; s < lv.nsrc && ok; s++)
-          if (s != d) ok = src_contains(lv.src[s], in, r, v);
-        nv[lv.cj_slot - lv.n_in_slots] = v;
-      } else if (lv.kind == kCartesian) {
-        uint64_t rem = local;
-        for (int s = lv.nsrc - 1; s >= 0; s--) {
-          const SrcSpec& sp = lv.src[s];
-          if (sp.out_slot < 0) continue;
-          uint32_t b, len;
-          src_list(sp, in, r, b, len);
-          const uint32_t idx = (uint32_t)(rem % len);
-          rem /= len;
-          nv[sp.out_slot - lv.n_in_slots] = src_value(sp, b + idx);
+      for (int i = 0; i < kMaxSrc + 1; i++) nv[i] = 0;
+      if (ok) {
+        r = gallop_row(offs, r0, in.n, w);
+        const uint64_t local = w - offs[r];
+        if (lv.kind == kColumnJoin) {
+          const int d = drv[r];
+          const uint32_t v = src_value(lv.src[d], beg[r] + (uint32_t)local);
+          for (int s = 0; s < lv.nsrc && ok; s++)
+            if (s != d) ok = src_contains(lv.src[s], in, r, v);
+          nv[lv.cj_slot - lv.n_in_slots] = v;
+        } else if (lv.kind == kCartesian) {
+          uint64_t rem = local;
+          for (int s = lv.nsrc - 1; s >= 0; s--) {
+            const SrcSpec& sp = lv.src[s];
+            if (sp.out_slot < 0) continue;
+            uint32_t b, len;
+            src_list(sp, in, r, b, len);
+            const uint32_t idx = (uint32_t)(rem % len);
+            rem /= len;
+            nv[sp.out_slot - lv.n_in_slots] = src_value(sp, b + idx);
+          }
+        } else {
+          const SrcSpec& sp = lv.src[0];
+          uint32_t b = 0;
+          if (sp.prefix_slot >= 0) {
+            uint32_t e;
+            trie_range(sp.t, in.col[sp.prefix_slot][r], b, e);
+          }
+          const uint64_t i = b + local;
+          if (lv.scan_slot[0] >= 0) nv[lv.scan_slot[0] - lv.n_in_slots] = (uint32_t)(sp.t.keys[i] >> 32);
+          if (lv.scan_slot[1] >= 0) nv[lv.scan_slot[1] - lv.n_in_slots] = (uint32_t)sp.t.keys[i];
         }
-      } else {
-        const SrcSpec& sp = lv.src[0];
-        uint32_t b = 0;
-        if (sp.prefix_slot >= 0) {
-          uint32_t e;
-          trie_range(sp.t, in.col[sp.prefix_slot][r], b, e);
-        }
-        const uint64_t i = b + local;
-        if (lv.scan_slot[0] >= 0) nv[lv.scan_slot[0] - lv.n_in_slots] = (uint32_t)(sp.t.keys[i] >> 32);
-        if (lv.scan_slot[1] >= 0) nv[lv.scan_slot[1] - lv.n_in_slots] = (uint32_t)sp.t.keys[i];
       }
-    }
-    auto val = [&](int slot) -> uint32_t {
-      return slot < lv.n_in_slots ? in.col[slot][r] : nv[slot - lv.n_in_slots];
-    };
-    for (int f = 0; f < lv.nfilt && ok; f++) {
-      const FiltSpec& fs = lv.filt[f];
-      const uint32_t a = fs.a_slot >= 0 ? val(fs.a_slot) : fs.a_const;
-      const uint32_t b = fs.b_slot >= 0 ? val(fs.b_slot) : fs.b_const;
-      ok = filt_ok(fs, a, b);
-    }
-    if (EMIT == kEmitCount) {
-      my_count += ok;
-    } else {
+      auto val = [&](int slot) -> uint32_t {
+        return slot < lv.n_in_slots ? in.col[slot][r] : nv[slot - lv.n_in_slots];
+      };
+      for (int f = 0; f < lv.nfilt && ok; f++) {
+        const FiltSpec& fs = lv.filt[f];
+        const uint32_t a = fs.a_slot >= 0 ? val(fs.a_slot) : fs.a_const;
+        const uint32_t b = fs.b_slot >= 0 ? val(fs.b_slot) : fs.b_const;
+        ok = filt_ok(fs, a, b);
+      }
       const unsigned m = __ballot_sync(kAllLanes, ok);
-      if (m) {
-        const int leader = __ffs(m) - 1;
-        unsigned long long base = 0;
-        if (lane == leader) base = atomicAdd(d_out_n, (unsigned long long)__popc(m));
-        base = __shfl_sync(kAllLanes, base, leader);
-        if (ok) {
-          const uint64_t pos = base + __popc(m & lanemask_lt());
-          if (EMIT == kEmitKeys) {
+      if (MODE == kModeCount || MODE == kModeTableCount) {
+        running += __popc(m);
+      } else if (MODE == kModeKeys) {
+        if (m) {
+          const int leader = __ffs(m) - 1;
+          unsigned long long pos0 = 0;
+          if (lane == leader) pos0 = atomicAdd(d_out_n, (unsigned long long)__popc(m));
+          pos0 = __shfl_sync(kAllLanes, pos0, leader);
+          if (ok) {
             const uint64_t hi = val(lv.key_slot[0]);
             const uint64_t lo = lv.key_arity > 1 ? val(lv.key_slot[1]) : 0;
-            out_keys[pos] = (hi << 32) | lo;
-          } else {
-            for (int c = 0; c < kMaxSlots; c++)
-              if (out.col[c]) out.col[c][pos] = val(c);
+            out_keys[pos0 + __popc(m & lanemask_lt())] = (hi << 32) | lo;
           }
         }
+      } else {  // ordered table write
+        if (ok) {
+          const uint64_t pos = running + __popc(m & lanemask_lt());
+          for (int c = 0; c < kMaxSlots; c++)
+            if (out.col[c]) out.col[c][pos] = val(c);
+        }
+        running += __popc(m);
       }
+      r0 = __shfl_sync(kAllLanes, r, 31);
     }
-    __syncthreads();
   }
-  if (EMIT == kEmitCount) {
-    unsigned long long s = warp_sum(my_count);
-    if (lane == 0) red[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      unsigned long long t = 0;
-      for (int i = 0; i < kJThreads / 32; i++) t += red[i];
-      if (t) atomicAdd(d_out_n, t);
-    }
+  if (MODE == kModeCount) {
+    if (lane == 0 && running) atomicAdd(d_out_n, running);
+  } else if (MODE == kModeTableCount) {
+    if (lane == 0) warp_counts[gw] = running;
   }
 }
 
@@ -228,6 +236,11 @@ static int jgrid(uint64_t n, int sms) {
   uint64_t cap = (uint64_t)sms * 16;
   if (g > cap) g = cap;
   return g ? (int)g : 1;
+}
+
+size_t join_expand_scratch_bytes(int num_sms) {
+  const uint64_t warps = (uint64_t)num_sms * 16 * (kJThreads / 32);
+  return 2 * ((warps + 1) * 8 + 255) + scan_scratch_bytes(warps) + 1024;
 }
 
 JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scratch& s) {
@@ -247,22 +260,35 @@ JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scrat
 }
 
 void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const JoinWork& w,
-                 uint64_t total, Table* out_table, uint64_t* out_keys, uint64_t* d_out_n) {
+                 uint64_t total, Table* out_table, uint64_t* out_keys, uint64_t* d_out_n,
+                 Scratch& s) {
   if (total == 0) return;
-  Table out = out_table ? *out_table : Table{};
-  const int g = jgrid(total, L.num_sms);
   auto* cnt = reinterpret_cast<unsigned long long*>(d_out_n);
-  if (lv.emit == kEmitCount)
-    join_expand_kernel<kEmitCount><<<g, kJThreads, 0, L.stream>>>(lv, in, w.offs, w.drv, w.beg,
-                                                                 total, out, out_keys, cnt);
-  else if (lv.emit == kEmitKeys)
-    join_expand_kernel<kEmitKeys><<<g, kJThreads, 0, L.stream>>>(lv, in, w.offs, w.drv, w.beg,
-                                                                total, out, out_keys, cnt);
-  else
-    join_expand_kernel<kEmitTable><<<g, kJThreads, 0, L.stream>>>(lv, in, w.offs, w.drv, w.beg,
-                                                                 total, out, out_keys, cnt);
+  const int g = jgrid(total, L.num_sms);
+  const uint64_t warps = (uint64_t)g * (kJThreads / 32);
+  const uint64_t chunk = ((total + warps - 1) / warps + 31) & ~uint64_t(31);
+  Table out = out_table ? *out_table : Table{};
+  if (lv.emit == kEmitCount) {
+    join_expand_kernel<kModeCount><<<g, kJThreads, 0, L.stream>>>(
+        lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, nullptr);
+    count_launches(1);
+  } else if (lv.emit == kEmitKeys) {
+    join_expand_kernel<kModeKeys><<<g, kJThreads, 0, L.stream>>>(
+        lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, nullptr);
+    count_launches(1);
+  } else {
+    uint64_t* wc = s.take<uint64_t>(warps + 1);
+    uint64_t* wo = s.take<uint64_t>(warps + 1);
+    join_expand_kernel<kModeTableCount><<<g, kJThreads, 0, L.stream>>>(
+        lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, wc);
+    SRDL_CUDA(cudaGetLastError());
+    exclusive_scan_u64(L, wc, warps, wo, s);
+    SRDL_CUDA(cudaMemcpyAsync(d_out_n, wo + warps, 8, cudaMemcpyDeviceToDevice, L.stream));
+    join_expand_kernel<kModeTableWrite><<<g, kJThreads, 0, L.stream>>>(
+        lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, wo);
+    count_launches(2);
+  }
   SRDL_CUDA(cudaGetLastError());
-  count_launches(1);
 }
 
 }  // namespace srdl

@@ -72,6 +72,18 @@ void build_dir(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* dir,
 void build_roots(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* roots,
                  uint64_t* d_nroots, Scratch& s);
 
+// Hash tables for the child lists longer than `min_len` of a dense-directory
+// trie.  Plan: sizes[v] = slots for value v (0 = no table), offs = exclusive
+// scan (dir_n entries, offs[dir_n-1] = total slots).  Build: hdir[v] = first
+// slot or kNoHash; every child of a hashed list is inserted into `pool`,
+// which the caller pre-fills with 0xff bytes.
+size_t child_hash_scratch_bytes(uint32_t dir_n);
+void child_hash_plan(const Launch& L, const uint32_t* dir, uint32_t dir_n, uint32_t min_len,
+                     uint64_t* sizes, uint64_t* offs, Scratch& s);
+void child_hash_build(const Launch& L, const uint64_t* keys, uint64_t n, const uint32_t* dir,
+                      uint32_t dir_n, const uint64_t* sizes, const uint64_t* offs, uint32_t* hdir,
+                      uint32_t* pool);
+
 // Swap the two 32-bit halves of every key (index permutation (1,0) <-> (0,1)).
 void swap_halves(const Launch& L, const uint64_t* in, uint64_t n, uint64_t* out);
 
@@ -133,9 +145,13 @@ struct JoinWork {
 JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scratch& s);
 
 // Pass 2: expands `total` work items; surviving bindings are appended to
-// `out_table` (emit table), to `out_keys` (emit keys) or counted (emit
-// count) via *d_out_n, which the caller zeroes.  Output capacity = total.
+// `out_table` (emit table, in input order: the table stays sorted), to
+// `out_keys` (emit keys, any order) or counted (emit count) via *d_out_n,
+// which the caller zeroes.  Output capacity = total.
+size_t join_expand_scratch_bytes(int num_sms);
 void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const JoinWork& w,
-                 uint64_t total, Table* out_table, uint64_t* out_keys, uint64_t* d_out_n);
+                 uint64_t total, Table* out_table, uint64_t* out_keys, uint64_t* d_out_n,
+                 Scratch& s);
+
 
 }  // namespace srdl

@@ -1,6 +1,7 @@
 // runtime.cu -- Database: plan parsing, input staging, relation indexes.
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <sstream>
 
@@ -465,6 +466,42 @@ void Database::ensure_trie(Relation& r, Index& ix) {
   ix.trie = true;
 }
 
+// Child lists longer than this many values get an open-addressing table
+// when the index is probed by a column join (SRDL_HASH_MIN overrides).
+static uint32_t hash_min_len() {
+  static const uint32_t v = [] {
+    const char* e = getenv("SRDL_HASH_MIN");
+    return e ? (uint32_t)strtoul(e, nullptr, 10) : 32u;
+  }();
+  return v;
+}
+
+void Database::ensure_hash(Index& ix) {
+  if (ix.hash_done) return;
+  ix.hash_done = true;
+  if (!ix.dir_n || ix.n == 0 || dom_max_ == 0xffffffffu) return;
+  size_t pid = prof_begin("child_hash_build");
+  DevBuf scratch(child_hash_scratch_bytes(ix.dir_n), L_.stream);
+  Scratch s{scratch.as<char>(), scratch.bytes(), 0};
+  const uint32_t nv = ix.dir_n - 1;
+  uint64_t* sizes = s.take<uint64_t>(nv);
+  uint64_t* offs = s.take<uint64_t>(nv + 1);
+  child_hash_plan(L_, ix.dir.as<uint32_t>(), ix.dir_n, hash_min_len(), sizes, offs, s);
+  SRDL_CUDA(cudaMemcpyAsync(h_small_ + 5, offs + nv, 8, cudaMemcpyDeviceToHost, L_.stream));
+  SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  const uint64_t slots = h_small_[5];
+  if (slots == 0 || slots >= 0xffffffffull) {
+    prof_end(pid, 0, 0);
+    return;
+  }
+  ix.hdir = DevBuf((size_t)nv * 4, L_.stream);
+  ix.hpool = DevBuf(slots * 4, L_.stream);
+  SRDL_CUDA(cudaMemsetAsync(ix.hpool.as<void>(), 0xff, slots * 4, L_.stream));
+  child_hash_build(L_, ix.keys.as<uint64_t>(), ix.n, ix.dir.as<uint32_t>(), ix.dir_n, sizes, offs,
+                   ix.hdir.as<uint32_t>(), ix.hpool.as<uint32_t>());
+  prof_end(pid, 8.0 * ix.n + 4.0 * slots + 16.0 * nv, (double)ix.n);
+}
+
 TrieView Database::view(Relation& r, Index& ix) {
   ensure_trie(r, ix);
   TrieView t;
@@ -472,6 +509,8 @@ TrieView Database::view(Relation& r, Index& ix) {
   t.lo = ix.lo.as<uint32_t>();
   t.roots = ix.roots.as<uint32_t>();
   t.dir = ix.dir_n ? ix.dir.as<uint32_t>() : nullptr;
+  t.hdir = ix.hdir.bytes() ? ix.hdir.as<uint32_t>() : nullptr;
+  t.hpool = ix.hpool.bytes() ? ix.hpool.as<uint32_t>() : nullptr;
   t.n = ix.n;
   t.n_roots = ix.n_roots;
   t.dir_n = ix.dir_n;

@@ -47,6 +47,8 @@ struct Index {
   bool trie = false;
   DevBuf lo, roots, dir;
   uint32_t n_roots = 0, dir_n = 0;
+  bool hash_done = false;  // hashed child lists built (or found unnecessary)
+  DevBuf hdir, hpool;
 };
 
 struct Chunk {
@@ -196,6 +198,7 @@ class Database {
   Index& ensure_index(Relation& r, Ver v, const std::vector<int>& perm);
   void ensure_trie(Relation& r, Index& ix);
   TrieView view(Relation& r, Index& ix);
+  void ensure_hash(Index& ix);
   void sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full);
   void exec_ops(const Step& st, uint64_t iteration);
   void exec_pipeline(const Op& op, bool recursive, uint64_t iteration);

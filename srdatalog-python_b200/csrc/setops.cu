@@ -156,6 +156,66 @@ void swap_halves(const Launch& L, const uint64_t* in, uint64_t n, uint64_t* out)
   count_launches(1);
 }
 
+__global__ void hash_size_kernel(const uint32_t* __restrict__ dir, uint32_t nv, uint32_t min_len,
+                                 uint64_t* __restrict__ sizes) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < nv;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t len = dir[v + 1] - dir[v];
+    sizes[v] = len > min_len ? (1ull << hash_log2(len)) : 0;
+  }
+}
+
+__global__ void hash_dir_kernel(const uint64_t* __restrict__ sizes, const uint64_t* __restrict__ offs,
+                                uint32_t nv, uint32_t* __restrict__ hdir) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < nv;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    hdir[v] = sizes[v] ? (uint32_t)offs[v] : kNoHash;
+}
+
+__global__ void hash_insert_kernel(const uint64_t* __restrict__ keys, uint64_t n,
+                                   const uint32_t* __restrict__ dir, const uint32_t* __restrict__ hdir,
+                                   uint32_t* __restrict__ pool) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = (uint32_t)(keys[i] >> 32), x = (uint32_t)keys[i];
+    const uint32_t off = hdir[v];
+    if (off == kNoHash) continue;
+    const int k = hash_log2(dir[v + 1] - dir[v]);
+    const uint32_t mask = (1u << k) - 1;
+    uint32_t h = hash_slot(x, k);
+    // at most `mask + 1` probes; the table is at most half full
+    for (uint32_t probe = 0; probe <= mask; probe++) {
+      const uint32_t old = atomicCAS(&pool[off + h], kHashEmpty, x);
+      if (old == kHashEmpty || old == x) break;
+      h = (h + 1) & mask;
+    }
+  }
+}
+
+size_t child_hash_scratch_bytes(uint32_t dir_n) {
+  return 2 * ((size_t)dir_n * 8 + 512) + scan_scratch_bytes(dir_n) + 1024;
+}
+
+void child_hash_plan(const Launch& L, const uint32_t* dir, uint32_t dir_n, uint32_t min_len,
+                     uint64_t* sizes, uint64_t* offs, Scratch& s) {
+  const uint32_t nv = dir_n - 1;
+  hash_size_kernel<<<grid_for(nv, L.num_sms), 256, 0, L.stream>>>(dir, nv, min_len, sizes);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(1);
+  exclusive_scan_u64(L, sizes, nv, offs, s);
+}
+
+void child_hash_build(const Launch& L, const uint64_t* keys, uint64_t n, const uint32_t* dir,
+                      uint32_t dir_n, const uint64_t* sizes, const uint64_t* offs, uint32_t* hdir,
+                      uint32_t* pool) {
+  const uint32_t nv = dir_n - 1;
+  hash_dir_kernel<<<grid_for(nv, L.num_sms), 256, 0, L.stream>>>(sizes, offs, nv, hdir);
+  SRDL_CUDA(cudaGetLastError());
+  if (n) hash_insert_kernel<<<grid_for(n, L.num_sms), 256, 0, L.stream>>>(keys, n, dir, hdir, pool);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(n ? 2 : 1);
+}
+
 __global__ void max_kernel(const uint32_t* __restrict__ d, uint64_t n, uint32_t* __restrict__ out) {
   uint32_t m = 0;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;

@@ -27,6 +27,7 @@ constexpr int kRsWarps = kRsThreads / 32;
 constexpr int kRsPerWarp = 256;                  // keys per warp per tile
 constexpr int kRsTile = kRsWarps * kRsPerWarp;   // 2048 keys per tile
 constexpr int kRsBins = 256;
+static_assert(kRsThreads == kRsBins, "one thread per digit in the per-tile digit loops");
 
 int value_bits(uint32_t max_value) {
   int b = 0;
@@ -85,27 +86,33 @@ __global__ void __launch_bounds__(kRsThreads) rs_hist(const K* __restrict__ keys
   for (int d = threadIdx.x; d < nbins; d += kRsThreads) counts[(uint64_t)d * gridDim.x + blockIdx.x] = h[d];
 }
 
-// Exclusive scan of L uint32 counters in place (digit-major), one block.
-__global__ void rs_scan(uint32_t* c, uint32_t L) {
-  __shared__ uint32_t sh[1024 / 32 + 1];
-  const uint32_t per = (L + blockDim.x - 1) / blockDim.x;
-  const uint32_t s = threadIdx.x * per, e = min(L, s + per);
+// Block d turns row d of the digit-major counters (one counter per
+// histogram block) into exclusive offsets within the digit, in place, and
+// writes the digit's total to digit_tot[d].
+__global__ void __launch_bounds__(kRsThreads) rs_rowscan(uint32_t* c, int nb,
+                                                         uint32_t* __restrict__ digit_tot) {
+  __shared__ uint32_t sh[kRsThreads / 32 + 1];
+  uint32_t* row = c + (uint64_t)blockIdx.x * nb;
+  const int per = (nb + kRsThreads - 1) / kRsThreads;
+  const int s = threadIdx.x * per, e = min(nb, s + per);
   uint32_t sum = 0;
-  for (uint32_t i = s; i < e; i++) sum += c[i];
+  for (int i = s; i < e; i++) sum += row[i];
   uint32_t tot;
   uint32_t run = block_excl_scan(sum, sh, &tot);
-  for (uint32_t i = s; i < e; i++) {
-    uint32_t v = c[i];
-    c[i] = run;
+  for (int i = s; i < e; i++) {
+    uint32_t v = row[i];
+    row[i] = run;
     run += v;
   }
+  if (threadIdx.x == 0) digit_tot[blockIdx.x] = tot;
 }
 
 template <typename K>
 __global__ void __launch_bounds__(kRsThreads) rs_scatter(const K* __restrict__ in,
                                                          K* __restrict__ out, uint64_t n,
                                                          uint64_t chunk, int shift, int nbins,
-                                                         const uint32_t* __restrict__ offs) {
+                                                         const uint32_t* __restrict__ offs,
+                                                         const uint32_t* __restrict__ digit_tot) {
   __shared__ uint32_t base[kRsBins];             // global output position per digit
   __shared__ uint32_t wcnt[kRsWarps][kRsBins];   // per-warp digit counts -> warp offsets
   __shared__ uint32_t tstart[kRsBins];           // digit start inside the staged tile
@@ -115,8 +122,14 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter(const K* __restrict__ i
 
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const uint32_t mask = nbins - 1;
-  for (int d = threadIdx.x; d < kRsBins; d += kRsThreads)
-    base[d] = d < nbins ? offs[(uint64_t)d * gridDim.x + blockIdx.x] : 0;
+  {
+    // digit base = keys with a smaller digit; plus this block's offset in the digit
+    const int d = threadIdx.x;  // kRsThreads == kRsBins
+    const uint32_t t = d < nbins ? digit_tot[d] : 0;
+    uint32_t all;
+    const uint32_t dbase = block_excl_scan(t, scan_sh, &all);
+    base[d] = d < nbins ? dbase + offs[(uint64_t)d * gridDim.x + blockIdx.x] : 0;
+  }
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = begin + chunk < n ? begin + chunk : n;
 
@@ -186,10 +199,8 @@ static inline bool use32(int bits) { return 2 * bits <= 32; }
 
 size_t sort_scratch_bytes(uint64_t n, int bits) {
   const size_t ks = use32(bits) ? 4 : 8;
-  const uint64_t chunk = ((n + kRsTile - 1) / kRsTile + 148 * 8 - 1) / (148 * 8);
-  (void)chunk;
   const size_t counts = (size_t)kRsBins * 256 * 8 * 4;  // <= 8 blocks per SM, 256 SMs
-  return 2 * (((n * ks) + 255) & ~size_t(255)) + counts + 256 + cp_scratch_bytes(n) + 1024;
+  return 2 * (((n * ks) + 255) & ~size_t(255)) + counts + 2048 + cp_scratch_bytes(n) + 1024;
 }
 
 template <typename K>
@@ -211,6 +222,7 @@ static void sort_dedup_t(const Launch& L, const uint64_t* in, uint64_t n, int bi
   const uint64_t chunk = (per ? per : 1) * kRsTile;
   const int nb = (int)((n + chunk - 1) / chunk);
   uint32_t* counts = s.take<uint32_t>((size_t)kRsBins * nb);
+  uint32_t* digit_tot = s.take<uint32_t>(kRsBins);
 
   const int total_bits = 2 * bits;
   const int passes = (total_bits + 7) / 8;
@@ -219,8 +231,8 @@ static void sort_dedup_t(const Launch& L, const uint64_t* in, uint64_t n, int bi
     const int w = total_bits / passes + (p < total_bits % passes ? 1 : 0);
     const int nbins = 1 << w;
     rs_hist<K><<<nb, kRsThreads, 0, L.stream>>>(a, n, chunk, shift, nbins, counts);
-    rs_scan<<<1, 1024, 0, L.stream>>>(counts, (uint32_t)(nbins * nb));
-    rs_scatter<K><<<nb, kRsThreads, 0, L.stream>>>(a, b, n, chunk, shift, nbins, counts);
+    rs_rowscan<<<nbins, kRsThreads, 0, L.stream>>>(counts, nb, digit_tot);
+    rs_scatter<K><<<nb, kRsThreads, 0, L.stream>>>(a, b, n, chunk, shift, nbins, counts, digit_tot);
     SRDL_CUDA(cudaGetLastError());
     count_launches(3);
     std::swap(a, b);
