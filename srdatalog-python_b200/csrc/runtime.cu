@@ -466,12 +466,14 @@ void Database::ensure_trie(Relation& r, Index& ix) {
   ix.trie = true;
 }
 
-// Child lists longer than this many values get an open-addressing table
-// when the index is probed by a column join (SRDL_HASH_MIN overrides).
+// With SRDL_HASH_MIN=L set, child lists longer than L values of an index
+// probed by a column join get an open-addressing table.  Off by default: on
+// the R-MAT triangle workload the binary search over sorted, co-located
+// probes measured faster (47.8 ms vs 53.0 ms per step at L = 32).
 static uint32_t hash_min_len() {
   static const uint32_t v = [] {
     const char* e = getenv("SRDL_HASH_MIN");
-    return e ? (uint32_t)strtoul(e, nullptr, 10) : 32u;
+    return e ? (uint32_t)strtoul(e, nullptr, 10) : 0u;
   }();
   return v;
 }
@@ -479,7 +481,7 @@ static uint32_t hash_min_len() {
 void Database::ensure_hash(Index& ix) {
   if (ix.hash_done) return;
   ix.hash_done = true;
-  if (!ix.dir_n || ix.n == 0 || dom_max_ == 0xffffffffu) return;
+  if (hash_min_len() == 0 || !ix.dir_n || ix.n == 0 || dom_max_ == 0xffffffffu) return;
   size_t pid = prof_begin("child_hash_build");
   DevBuf scratch(child_hash_scratch_bytes(ix.dir_n), L_.stream);
   Scratch s{scratch.as<char>(), scratch.bytes(), 0};
