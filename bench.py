@@ -269,7 +269,8 @@ def main():
       dist.destroy_process_group()
     if rank == 0:
       print(json.dumps({'metric': f'tuples/s ({args.workload})', 'value': value,
-                        'ms_per_step': total_ms / args.steps, 'quick': True}), flush=True)
+                        'ms_per_step': total_ms / args.steps, 'quick': True,
+                        'step_ms': [round(x, 3) for x in step_ms]}), flush=True)
     return
   db2 = Database(plan, device=local)
   db2.set_stream(stream.cuda_stream)
@@ -329,7 +330,8 @@ def main():
                'inputs': 'HBM-resident for value; pinned host rows for e2e'},
     'e2e': {'value': units * args.steps * world / (e2e_total / 1e3), 'unit': 'tuples/s',
             'ms_per_step': e2e_total / args.steps, 'h2d_bytes_per_step': int(n) * 8,
-            'd2h_bytes_per_step': 8},
+            'd2h_bytes_per_step': 8, 'step_ms': [round(x, 3) for x in e2e_ms]},
+    'step_ms': [round(x, 3) for x in step_ms],
     'gpu_launches': int(launches),
     'roofline': roof,
     'kernels': {k2: {'ms_per_step': v['ms'] / args.steps,

@@ -58,7 +58,8 @@ __device__ __forceinline__ bool src_contains(const SrcSpec& s, const Table& in, 
 __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Table in,
                                                                uint64_t* __restrict__ work,
                                                                uint8_t* __restrict__ drv,
-                                                               uint32_t* __restrict__ beg) {
+                                                               uint32_t* __restrict__ beg,
+                                                               uint2* __restrict__ orange) {
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < in.n;
        r += (uint64_t)gridDim.x * blockDim.x) {
     if (lv.kind == kColumnJoin) {
@@ -78,6 +79,11 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
       work[r] = empty ? 0 : best;
       drv[r] = (uint8_t)bd;
       beg[r] = bb;
+      if (lv.nsrc == 2) {
+        uint32_t ob, olen;
+        src_list(lv.src[1 - bd], in, r, ob, olen);
+        orange[r] = make_uint2(ob, ob + olen);
+      }
     } else if (lv.kind == kCartesian) {
       uint64_t prod = 1;
       for (int s = 0; s < lv.nsrc; s++) {
@@ -85,6 +91,11 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
         src_list(lv.src[s], in, r, b, len);
         if (lv.src[s].out_slot < 0) prod = len ? prod : 0;
         else prod *= len;
+        // two-source form: list 0 begin in beg, list 1 as [begin, length)
+        if (lv.nsrc == 2) {
+          if (s == 0) beg[r] = b;
+          else orange[r] = make_uint2(b, len);
+        }
       }
       work[r] = prod;
     } else {  // scan
@@ -129,6 +140,144 @@ __device__ __forceinline__ bool filt_ok(const FiltSpec& f, uint32_t a, uint32_t 
 }
 
 enum ExpandMode : int { kModeCount = 0, kModeKeys = 1, kModeTableCount = 2, kModeTableWrite = 3 };
+
+// in.col[k][r] with a compile-time slot index, so the Table parameter is
+// never copied to local memory for a runtime subscript.
+__device__ __forceinline__ uint32_t slot_value(const Table& t, int k, uint64_t r) {
+  uint32_t x = 0;
+#pragma unroll
+  for (int c = 0; c < kMaxSlots; c++)
+    if (c == k) x = t.col[c][r];
+  return x;
+}
+
+__device__ __forceinline__ void slot_store(const Table& t, int k, uint64_t pos, uint32_t x) {
+#pragma unroll
+  for (int c = 0; c < kMaxSlots; c++)
+    if (c == k) t.col[c][pos] = x;
+}
+
+// Filters of a level over the input row's slots and up to two new values.
+__device__ __forceinline__ bool level_filters(const LevelSpec& lv, const Table& in, uint64_t r,
+                                              int s0, uint32_t v0, int s1, uint32_t v1) {
+  bool ok = true;
+#pragma unroll
+  for (int f = 0; f < kMaxFilt; f++) {
+    if (f < lv.nfilt) {
+      const FiltSpec fs = lv.filt[f];
+      uint32_t a = fs.a_const, b = fs.b_const;
+      if (fs.a_slot >= 0)
+        a = fs.a_slot == s0 ? v0 : fs.a_slot == s1 ? v1 : slot_value(in, fs.a_slot, r);
+      if (fs.b_slot >= 0)
+        b = fs.b_slot == s0 ? v0 : fs.b_slot == s1 ? v1 : slot_value(in, fs.b_slot, r);
+      switch (fs.op) {
+        case kNe: ok &= a != b; break;
+        case kEq: ok &= a == b; break;
+        case kLt: ok &= a < b; break;
+        case kLe: ok &= a <= b; break;
+        case kGt: ok &= a > b; break;
+        default: ok &= a >= b; break;
+      }
+    }
+  }
+  return ok;
+}
+
+// First index p in [b, e) with a[p] >= v (e if none); branch-free halving.
+__device__ __forceinline__ uint32_t lower_bound_bf(const uint32_t* __restrict__ a, uint32_t b,
+                                                   uint32_t e, uint32_t v) {
+  uint32_t len = e - b;
+  if (len == 0) return b;
+  while (len > 1) {
+    const uint32_t half = len >> 1;
+    b = (a[b + half] < v) ? b + half : b;
+    len -= half;
+  }
+  return b + (a[b] < v ? 1u : 0u);
+}
+
+// Two-source column join without filters (the common leapfrog step): the
+// count pass stored, per row, the driver list begin and the other list's
+// range, so a candidate costs one coalesced load of its value plus a
+// branch-free binary search in the other list (or a directory check when
+// the other list is all roots of a dense index).
+template <int MODE>
+__global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
+    LevelSpec lv, Table in, const uint64_t* __restrict__ offs, const uint8_t* __restrict__ drv,
+    const uint32_t* __restrict__ beg, const uint2* __restrict__ orange, uint64_t total,
+    uint64_t chunk, Table out, uint64_t* __restrict__ out_keys,
+    unsigned long long* __restrict__ d_out_n, uint64_t* __restrict__ warp_counts) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t c0 = gw * chunk;
+  const uint64_t c1 = c0 + chunk < total ? c0 + chunk : total;
+  const uint32_t* vals0 = lv.src[0].prefix_slot < 0 ? lv.src[0].t.roots : lv.src[0].t.lo;
+  const uint32_t* vals1 = lv.src[1].prefix_slot < 0 ? lv.src[1].t.roots : lv.src[1].t.lo;
+  // a roots-list side with a dense directory answers membership in O(1)
+  const uint32_t* dir0 = lv.src[0].prefix_slot < 0 ? lv.src[0].t.dir : nullptr;
+  const uint32_t* dir1 = lv.src[1].prefix_slot < 0 ? lv.src[1].t.dir : nullptr;
+  const uint32_t dn0 = lv.src[0].t.dir_n, dn1 = lv.src[1].t.dir_n;
+  unsigned long long running = 0;
+  if (MODE == kModeTableWrite) running = warp_counts[gw];
+  if (c0 < c1) {
+    uint64_t r0 = gallop_row(offs, 0, in.n, c0);
+    for (uint64_t base = c0; base < c1; base += 32) {
+      const uint64_t w = base + lane;
+      bool ok = w < c1;
+      uint64_t r = r0;
+      uint32_t v = 0;
+      if (ok) {
+        r = gallop_row(offs, r0, in.n, w);
+        const uint32_t local = (uint32_t)(w - offs[r]);
+        const int d = drv[r];
+        v = (d == 0 ? vals0 : vals1)[beg[r] + local];
+        const uint32_t* odir = d == 0 ? dir1 : dir0;
+        if (odir) {
+          const uint32_t odn = d == 0 ? dn1 : dn0;
+          ok = v + 1u < odn && odir[v] < odir[v + 1];
+        } else {
+          const uint2 rg = orange[r];
+          const uint32_t* ov = d == 0 ? vals1 : vals0;
+          const uint32_t p = lower_bound_bf(ov, rg.x, rg.y, v);
+          ok = p < rg.y && ov[p] == v;
+        }
+      }
+      const unsigned m = __ballot_sync(kAllLanes, ok);
+      if (MODE == kModeCount || MODE == kModeTableCount) {
+        running += __popc(m);
+      } else if (MODE == kModeKeys) {
+        if (m) {
+          const int leader = __ffs(m) - 1;
+          unsigned long long pos0 = 0;
+          if (lane == leader) pos0 = atomicAdd(d_out_n, (unsigned long long)__popc(m));
+          pos0 = __shfl_sync(kAllLanes, pos0, leader);
+          if (ok) {
+            const int k0 = lv.key_slot[0], k1 = lv.key_slot[1];
+            const uint64_t hi = k0 < lv.n_in_slots ? slot_value(in, k0, r) : v;
+            const uint64_t lo =
+                lv.key_arity > 1 ? (k1 < lv.n_in_slots ? slot_value(in, k1, r) : v) : 0;
+            out_keys[pos0 + __popc(m & lanemask_lt())] = (hi << 32) | lo;
+          }
+        }
+      } else {
+        if (ok) {
+          const uint64_t pos = running + __popc(m & lanemask_lt());
+#pragma unroll
+          for (int c = 0; c < kMaxSlots; c++)
+            if (c < lv.n_in_slots) out.col[c][pos] = in.col[c][r];
+          slot_store(out, lv.cj_slot, pos, v);
+        }
+        running += __popc(m);
+      }
+      r0 = __shfl_sync(kAllLanes, r, 31);
+    }
+  }
+  if (MODE == kModeCount) {
+    if (lane == 0 && running) atomicAdd(d_out_n, running);
+  } else if (MODE == kModeTableCount) {
+    if (lane == 0) warp_counts[gw] = running;
+  }
+}
 
 template <int MODE>
 __global__ void __launch_bounds__(kJThreads) join_expand_kernel(
@@ -225,10 +374,85 @@ __global__ void __launch_bounds__(kJThreads) join_expand_kernel(
   }
 }
 
+// Two-source cartesian product (both sources bind one variable): per row the
+// count pass stored list 0's begin and list 1's [begin, length); candidate
+// `local` pairs element local / len1 of list 0 with local % len1 of list 1.
+template <int MODE>
+__global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
+    LevelSpec lv, Table in, const uint64_t* __restrict__ offs, const uint32_t* __restrict__ beg,
+    const uint2* __restrict__ orange, uint64_t total, uint64_t chunk, Table out,
+    uint64_t* __restrict__ out_keys, unsigned long long* __restrict__ d_out_n,
+    uint64_t* __restrict__ warp_counts) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t c0 = gw * chunk;
+  const uint64_t c1 = c0 + chunk < total ? c0 + chunk : total;
+  const uint32_t* vals0 = lv.src[0].prefix_slot < 0 ? lv.src[0].t.roots : lv.src[0].t.lo;
+  const uint32_t* vals1 = lv.src[1].prefix_slot < 0 ? lv.src[1].t.roots : lv.src[1].t.lo;
+  const int s0 = lv.src[0].out_slot, s1 = lv.src[1].out_slot;
+  unsigned long long running = 0;
+  if (MODE == kModeTableWrite) running = warp_counts[gw];
+  if (c0 < c1) {
+    uint64_t r0 = gallop_row(offs, 0, in.n, c0);
+    for (uint64_t base = c0; base < c1; base += 32) {
+      const uint64_t w = base + lane;
+      bool ok = w < c1;
+      uint64_t r = r0;
+      uint32_t v0 = 0, v1 = 0;
+      if (ok) {
+        r = gallop_row(offs, r0, in.n, w);
+        const uint64_t local = w - offs[r];
+        const uint2 rg = orange[r];
+        const uint32_t i0 = (uint32_t)(local / rg.y), i1 = (uint32_t)(local - (uint64_t)i0 * rg.y);
+        v0 = vals0[beg[r] + i0];
+        v1 = vals1[rg.x + i1];
+        if (lv.nfilt) ok = level_filters(lv, in, r, s0, v0, s1, v1);
+      }
+      const unsigned m = __ballot_sync(kAllLanes, ok);
+      if (MODE == kModeCount || MODE == kModeTableCount) {
+        running += __popc(m);
+      } else if (MODE == kModeKeys) {
+        if (m) {
+          const int leader = __ffs(m) - 1;
+          unsigned long long pos0 = 0;
+          if (lane == leader) pos0 = atomicAdd(d_out_n, (unsigned long long)__popc(m));
+          pos0 = __shfl_sync(kAllLanes, pos0, leader);
+          if (ok) {
+            const int k0 = lv.key_slot[0], k1 = lv.key_slot[1];
+            const uint64_t hi = k0 == s0 ? v0 : k0 == s1 ? v1 : slot_value(in, k0, r);
+            const uint64_t lo = lv.key_arity < 2 ? 0
+                                : k1 == s0       ? v0
+                                : k1 == s1       ? v1
+                                                 : slot_value(in, k1, r);
+            out_keys[pos0 + __popc(m & lanemask_lt())] = (hi << 32) | lo;
+          }
+        }
+      } else {
+        if (ok) {
+          const uint64_t pos = running + __popc(m & lanemask_lt());
+#pragma unroll
+          for (int c = 0; c < kMaxSlots; c++)
+            if (c < lv.n_in_slots) out.col[c][pos] = in.col[c][r];
+          slot_store(out, s0, pos, v0);
+          slot_store(out, s1, pos, v1);
+        }
+        running += __popc(m);
+      }
+      r0 = __shfl_sync(kAllLanes, r, 31);
+    }
+  }
+  if (MODE == kModeCount) {
+    if (lane == 0 && running) atomicAdd(d_out_n, running);
+  } else if (MODE == kModeTableCount) {
+    if (lane == 0) warp_counts[gw] = running;
+  }
+}
+
 size_t join_work_scratch_bytes(uint64_t rows) {
   rows = rows ? rows : 1;
   return ((rows * 8 + 255) & ~size_t(255)) + ((rows + 1) * 8 + 255) + ((rows + 255) & ~size_t(255)) +
-         ((rows * 4 + 255) & ~size_t(255)) + scan_scratch_bytes(rows) + 1024;
+         ((rows * 4 + 255) & ~size_t(255)) + ((rows * 8 + 255) & ~size_t(255)) +
+         scan_scratch_bytes(rows) + 1024;
 }
 
 static int jgrid(uint64_t n, int sms) {
@@ -249,9 +473,10 @@ JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scrat
   w.offs = s.take<uint64_t>(in.n + 1);
   w.drv = s.take<uint8_t>(in.n ? in.n : 1);
   w.beg = s.take<uint32_t>(in.n ? in.n : 1);
+  w.orange = s.take<uint2>(in.n ? in.n : 1);
   if (in.n) {
     join_count_kernel<<<jgrid(in.n, L.num_sms), kJThreads, 0, L.stream>>>(lv, in, work, w.drv,
-                                                                          w.beg);
+                                                                          w.beg, w.orange);
     SRDL_CUDA(cudaGetLastError());
     count_launches(1);
   }
@@ -268,6 +493,54 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
   const uint64_t warps = (uint64_t)g * (kJThreads / 32);
   const uint64_t chunk = ((total + warps - 1) / warps + 31) & ~uint64_t(31);
   Table out = out_table ? *out_table : Table{};
+  if (lv.kind == kColumnJoin && lv.nsrc == 2 && lv.nfilt == 0) {
+#define SRDL_CJ2(MODE, WC) \
+  join_cj2_kernel<MODE><<<g, kJThreads, 0, L.stream>>>(lv, in, w.offs, w.drv, w.beg, w.orange, \
+                                                       total, chunk, out, out_keys, cnt, WC)
+    if (lv.emit == kEmitCount) {
+      SRDL_CJ2(kModeCount, nullptr);
+      count_launches(1);
+    } else if (lv.emit == kEmitKeys) {
+      SRDL_CJ2(kModeKeys, nullptr);
+      count_launches(1);
+    } else {
+      uint64_t* wc = s.take<uint64_t>(warps + 1);
+      uint64_t* wo = s.take<uint64_t>(warps + 1);
+      SRDL_CJ2(kModeTableCount, wc);
+      SRDL_CUDA(cudaGetLastError());
+      exclusive_scan_u64(L, wc, warps, wo, s);
+      SRDL_CUDA(cudaMemcpyAsync(d_out_n, wo + warps, 8, cudaMemcpyDeviceToDevice, L.stream));
+      SRDL_CJ2(kModeTableWrite, wo);
+      count_launches(2);
+    }
+#undef SRDL_CJ2
+    SRDL_CUDA(cudaGetLastError());
+    return;
+  }
+  if (lv.kind == kCartesian && lv.nsrc == 2 && lv.src[0].out_slot >= 0 && lv.src[1].out_slot >= 0) {
+#define SRDL_CART2(MODE, WC) \
+  join_cart2_kernel<MODE><<<g, kJThreads, 0, L.stream>>>(lv, in, w.offs, w.beg, w.orange, total, \
+                                                         chunk, out, out_keys, cnt, WC)
+    if (lv.emit == kEmitCount) {
+      SRDL_CART2(kModeCount, nullptr);
+      count_launches(1);
+    } else if (lv.emit == kEmitKeys) {
+      SRDL_CART2(kModeKeys, nullptr);
+      count_launches(1);
+    } else {
+      uint64_t* wc = s.take<uint64_t>(warps + 1);
+      uint64_t* wo = s.take<uint64_t>(warps + 1);
+      SRDL_CART2(kModeTableCount, wc);
+      SRDL_CUDA(cudaGetLastError());
+      exclusive_scan_u64(L, wc, warps, wo, s);
+      SRDL_CUDA(cudaMemcpyAsync(d_out_n, wo + warps, 8, cudaMemcpyDeviceToDevice, L.stream));
+      SRDL_CART2(kModeTableWrite, wo);
+      count_launches(2);
+    }
+#undef SRDL_CART2
+    SRDL_CUDA(cudaGetLastError());
+    return;
+  }
   if (lv.emit == kEmitCount) {
     join_expand_kernel<kModeCount><<<g, kJThreads, 0, L.stream>>>(
         lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, nullptr);

@@ -141,6 +141,7 @@ struct JoinWork {
   uint64_t* offs = nullptr;  // rows + 1
   uint8_t* drv = nullptr;    // column join: driver source per row
   uint32_t* beg = nullptr;   // column join: driver list begin per row
+  uint2* orange = nullptr;   // two-source column join: the other list [x, y) per row
 };
 JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scratch& s);
 
