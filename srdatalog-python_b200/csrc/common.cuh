@@ -209,6 +209,27 @@ __device__ __forceinline__ T block_excl_scan(T v, T* sh, T* total) {
   return r;
 }
 
+// First i in [lo, hi) where pred(i) is false, for a predicate that is true
+// on a prefix; called by all 32 lanes of a warp.  Each round tests 32 evenly
+// spaced positions, so the number of dependent load rounds is log32(hi-lo).
+template <class Pred>
+__device__ __forceinline__ uint64_t warp_partition_point(uint64_t lo, uint64_t hi, Pred pred) {
+  const int lane = threadIdx.x & 31;
+  while (hi - lo > 32) {
+    const uint64_t step = (hi - lo + 31) / 32;
+    const uint64_t i = lo + lane * step;
+    const bool p = i < hi && pred(i);
+    const int k = __popc(__ballot_sync(kAllLanes, p));
+    const uint64_t nlo = k > 0 ? lo + (uint64_t)(k - 1) * step + 1 : lo;
+    const uint64_t cand = lo + (uint64_t)k * step;
+    hi = cand < hi ? cand : hi;
+    lo = nlo;
+  }
+  const uint64_t i = lo + lane;
+  const bool p = i < hi && pred(i);
+  return lo + __popc(__ballot_sync(kAllLanes, p));
+}
+
 inline int div_up(uint64_t a, uint64_t b) { return (int)((a + b - 1) / b); }
 
 }  // namespace srdl

@@ -156,6 +156,94 @@ struct DedupDiffSel {
   __device__ void emit(uint64_t i, uint64_t pos) const { out[pos] = expand(a[i]); }
 };
 
+// Flag pass of DedupDiffSel with FULL: the block walks its chunk one tile at
+// a time; two warps locate the tile's slice of FULL (32-ary searches), the
+// block stages the slice in shared memory when it fits, and every key is then
+// probed by binary search in shared memory instead of global memory.
+constexpr int kDdStage = 4096;  // FULL keys staged per tile (32 KB)
+
+template <typename K>
+__global__ void __launch_bounds__(kCpThreads) dd_flag_kernel(DedupDiffSel<K> sel, uint64_t n,
+                                                             uint64_t chunk, uint8_t* flags,
+                                                             uint32_t* blk_counts) {
+  __shared__ uint64_t stage[kDdStage];
+  __shared__ uint64_t rng[2];
+  __shared__ uint32_t sh[kCpThreads / 32 + 1];
+  const uint64_t begin = (uint64_t)blockIdx.x * chunk;
+  const uint64_t end = begin + chunk < n ? begin + chunk : n;
+  const int wid = threadIdx.x >> 5;
+  uint32_t cnt = 0;
+  for (uint64_t tile = begin; tile < end; tile += kCpTile) {
+    const uint64_t tend = tile + kCpTile < end ? tile + kCpTile : end;
+    if (wid == 0) {
+      const uint64_t first = sel.expand(sel.a[tile]);
+      const uint64_t f0 = warp_partition_point(0, sel.n_full,
+                                               [&](uint64_t i) { return sel.full[i] < first; });
+      if ((threadIdx.x & 31) == 0) rng[0] = f0;
+    } else if (wid == 1) {
+      const uint64_t last = sel.expand(sel.a[tend - 1]);
+      const uint64_t f1 = warp_partition_point(0, sel.n_full,
+                                               [&](uint64_t i) { return sel.full[i] <= last; });
+      if ((threadIdx.x & 31) == 0) rng[1] = f1;
+    }
+    __syncthreads();
+    const uint64_t f0 = rng[0], f1 = rng[1];
+    const uint64_t len = f1 > f0 ? f1 - f0 : 0;
+    const bool staged = len <= (uint64_t)kDdStage;
+    if (staged)
+      for (uint64_t j = threadIdx.x; j < len; j += kCpThreads) stage[j] = sel.full[f0 + j];
+    __syncthreads();
+    for (uint64_t i = tile + threadIdx.x; i < tend; i += kCpThreads) {
+      const K c = sel.a[i];
+      bool keep = !(sel.dedup && i > 0 && sel.a[i - 1] == c);
+      if (keep && len) {
+        const uint64_t k = sel.expand(c);
+        if (staged) {
+          uint32_t lo = 0, hi = (uint32_t)len;
+          while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (stage[mid] < k) lo = mid + 1;
+            else hi = mid;
+          }
+          keep = !(lo < len && stage[lo] == k);
+        } else {
+          const uint64_t p = lower_bound_u64(sel.full, f0, f1, k);
+          keep = !(p < f1 && sel.full[p] == k);
+        }
+      }
+      flags[i] = keep ? 1 : 0;
+      cnt += keep;
+    }
+    __syncthreads();
+  }
+  uint32_t tot;
+  block_excl_scan(cnt, sh, &tot);
+  if (threadIdx.x == 0) blk_counts[blockIdx.x] = tot;
+}
+
+// compact() for DedupDiffSel with a FULL array: tiled, shared-memory probes.
+template <typename K>
+void compact_diff(const Launch& L, DedupDiffSel<K> sel, uint64_t n, uint64_t* d_total, Scratch& s) {
+  if (!sel.full || sel.n_full == 0) {
+    compact(L, sel, n, d_total, s);
+    return;
+  }
+  if (n == 0) {
+    SRDL_CUDA(cudaMemsetAsync(d_total, 0, sizeof(uint64_t), L.stream));
+    return;
+  }
+  const uint64_t chunk = cp_chunk(n, L.num_sms);
+  const int nb = cp_blocks(n, chunk);
+  uint8_t* flags = s.take<uint8_t>(n);
+  uint32_t* counts = s.take<uint32_t>(nb);
+  uint64_t* offs = s.take<uint64_t>(nb + 1);
+  dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, counts);
+  cp_scan_kernel<<<1, 1024, 0, L.stream>>>(counts, nb, offs, d_total);
+  cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, offs);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(3);
+}
+
 // Distinct first-column values of a sorted key array.
 struct RootSel {
   const uint64_t* keys;

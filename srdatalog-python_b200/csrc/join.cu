@@ -403,10 +403,31 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
         r = gallop_row(offs, r0, in.n, w);
         const uint64_t local = w - offs[r];
         const uint2 rg = orange[r];
-        const uint32_t i0 = (uint32_t)(local / rg.y), i1 = (uint32_t)(local - (uint64_t)i0 * rg.y);
+        uint32_t i0, i1;
+        if (local < (1ull << 32)) {  // 32-bit division whenever it fits
+          i0 = (uint32_t)local / rg.y;
+          i1 = (uint32_t)local - i0 * rg.y;
+        } else {
+          i0 = (uint32_t)(local / rg.y);
+          i1 = (uint32_t)(local - (uint64_t)i0 * rg.y);
+        }
         v0 = vals0[beg[r] + i0];
         v1 = vals1[rg.x + i1];
         if (lv.nfilt) ok = level_filters(lv, in, r, s0, v0, s1, v1);
+      }
+      if (MODE == kModeKeys && lv.nfilt == 0) {
+        // every candidate is a result: candidate index = output position
+        if (ok) {
+          const int k0 = lv.key_slot[0], k1 = lv.key_slot[1];
+          const uint64_t hi = k0 == s0 ? v0 : k0 == s1 ? v1 : slot_value(in, k0, r);
+          const uint64_t lo = lv.key_arity < 2 ? 0
+                              : k1 == s0       ? v0
+                              : k1 == s1       ? v1
+                                               : slot_value(in, k1, r);
+          out_keys[w] = (hi << 32) | lo;
+        }
+        r0 = __shfl_sync(kAllLanes, r, 31);
+        continue;
       }
       const unsigned m = __ballot_sync(kAllLanes, ok);
       if (MODE == kModeCount || MODE == kModeTableCount) {
@@ -525,6 +546,8 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
       SRDL_CART2(kModeCount, nullptr);
       count_launches(1);
     } else if (lv.emit == kEmitKeys) {
+      if (lv.nfilt == 0)  // every candidate is written at its own index
+        SRDL_CUDA(cudaMemcpyAsync(d_out_n, w.offs + in.n, 8, cudaMemcpyDeviceToDevice, L.stream));
       SRDL_CART2(kModeKeys, nullptr);
       count_launches(1);
     } else {

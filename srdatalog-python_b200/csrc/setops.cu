@@ -41,6 +41,15 @@ __device__ __forceinline__ uint64_t merge_path(const uint64_t* a, uint64_t na, c
   return lo;
 }
 
+// Same split found by one whole warp (warp_partition_point): the predicate
+// a[i] <= b[diag-1-i] is true on a prefix of [max(0, diag-nb), min(diag, na)).
+__device__ __forceinline__ uint64_t merge_path_warp(const uint64_t* a, uint64_t na,
+                                                    const uint64_t* b, uint64_t nb, uint64_t diag) {
+  const uint64_t lo = diag > nb ? diag - nb : 0;
+  const uint64_t hi = diag < na ? diag : na;
+  return warp_partition_point(lo, hi, [&](uint64_t i) { return a[i] <= b[diag - 1 - i]; });
+}
+
 __global__ void __launch_bounds__(kMgThreads) merge_kernel(const uint64_t* __restrict__ a,
                                                            uint64_t na,
                                                            const uint64_t* __restrict__ b,
@@ -52,8 +61,13 @@ __global__ void __launch_bounds__(kMgThreads) merge_kernel(const uint64_t* __res
   const uint64_t total = na + nb;
   const uint64_t d0 = (uint64_t)blockIdx.x * kMgTile;
   const uint64_t d1 = d0 + kMgTile < total ? d0 + kMgTile : total;
-  if (threadIdx.x == 0) split[0] = merge_path(a, na, b, nb, d0);
-  if (threadIdx.x == 32) split[1] = merge_path(a, na, b, nb, d1);
+  if (threadIdx.x < 32) {
+    const uint64_t s0 = merge_path_warp(a, na, b, nb, d0);
+    if (threadIdx.x == 0) split[0] = s0;
+  } else if (threadIdx.x < 64) {
+    const uint64_t s1 = merge_path_warp(a, na, b, nb, d1);
+    if (threadIdx.x == 32) split[1] = s1;
+  }
   __syncthreads();
   const uint64_t i0 = split[0], i1 = split[1];
   const uint64_t j0 = d0 - i0, j1 = d1 - i1;
@@ -96,7 +110,7 @@ size_t diff_scratch_bytes(uint64_t n) { return cp_scratch_bytes(n); }
 void set_difference(const Launch& L, const uint64_t* a, uint64_t na, const uint64_t* b,
                     uint64_t nb, uint64_t* out, uint64_t* d_nout, Scratch& s) {
   DedupDiffSel<uint64_t> sel{a, 32, false, b, nb, out};
-  compact(L, sel, na, d_nout, s);
+  compact_diff(L, sel, na, d_nout, s);
 }
 
 __global__ void lo_kernel(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ lo) {

@@ -239,7 +239,7 @@ static void sort_dedup_t(const Launch& L, const uint64_t* in, uint64_t n, int bi
     shift += w;
   }
   DedupDiffSel<K> sel{a, bits, true, full, n_full, out};
-  compact(L, sel, n, d_nout, s);
+  compact_diff(L, sel, n, d_nout, s);
 }
 
 void sort_dedup(const Launch& L, const uint64_t* in, uint64_t n, int bits, bool swap,
