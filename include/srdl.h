@@ -142,6 +142,21 @@ int srdl_set_difference_u64(const uint64_t* d_a, uint64_t na, const uint64_t* d_
 int srdl_merge_u64(const uint64_t* d_a, uint64_t na, const uint64_t* d_b, uint64_t nb,
                    uint64_t* d_out, void* stream);
 
+/* Allocation-free variant of srdl_sort_unique_u64, for callers that may not
+ * allocate device memory on their call path (a host engine whose memory
+ * manager owns and pre-plans every device allocation, or a latency-critical
+ * caller that cannot afford cudaMalloc).  No counterpart in the reference.
+ * Same contract as srdl_sort_unique_u64 without the scratch arguments: the
+ * temporaries live in a 20 MiB file-scope device array that every GPU loading
+ * libsrdl keeps until process exit.  At most
+ * srdl_sort_unique_noalloc_max_keys() (1,048,576) keys per call; more returns
+ * status 5.  The first call on a device resolves the array's address (call it
+ * once before any stream capture).  Calls that overlap on the GPU share the
+ * array and race: serialise them.  Calls no cudaMalloc/cudaFree. */
+int srdl_sort_unique_u64_noalloc(const uint64_t* d_in, uint64_t n, int value_bits,
+                                 uint64_t* d_out, uint64_t* d_n_out, void* stream);
+uint64_t srdl_sort_unique_noalloc_max_keys(void);
+
 #ifdef __cplusplus
 }
 #endif

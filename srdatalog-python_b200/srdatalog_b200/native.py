@@ -47,6 +47,8 @@ SIGNATURES = {
   'srdl_set_difference_scratch_bytes': (_u64, [_u64]),
   'srdl_set_difference_u64': (ctypes.c_int, [_vp, _u64, _vp, _u64, _vp, _vp, _vp, _u64, _vp]),
   'srdl_merge_u64': (ctypes.c_int, [_vp, _u64, _vp, _u64, _vp, _vp]),
+  'srdl_sort_unique_u64_noalloc': (ctypes.c_int, [_vp, _u64, ctypes.c_int, _vp, _vp, _vp]),
+  'srdl_sort_unique_noalloc_max_keys': (_u64, []),
 }
 
 _LIB = None
