@@ -45,11 +45,35 @@ WORKLOADS = {
   'sg': dict(plan='sg', rel='Arc', out='Sg', kind='size',
              desc='same generation, windowed forest n=10,000 (parent in [i-1000,i-1]) '
                   '+ 10% cross edges, seed 2'),
+  'batched': dict(plan='tc', rel='ArcInput', out='Path', kind='batched',
+                  desc='4,096 independent TC instances, directed Erdos-Renyi, n log-uniform in '
+                       '[64, 1024], mean out-degree U[2,8], seed 1000+j; evaluated as one '
+                       'disjoint union'),
 }
+
+BATCH_COUNT = 4096
+BATCH_N_HI = 1024
+PLAIN_SAMPLE_STRIDE = 16
+
+
+_BATCH = None
+
+
+def make_batch():
+  '''(instances, union) of the batched workload (generated once per process).'''
+  global _BATCH
+  if _BATCH is None:
+    from srdatalog_b200 import workloads as W
+    from srdatalog_b200.batch import make_union
+    insts = [{'ArcInput': e} for e in W.batched_instances(count=BATCH_COUNT, n_hi=BATCH_N_HI)]
+    _BATCH = (insts, make_union(insts))
+  return _BATCH
 
 
 def make_edges(name: str) -> np.ndarray:
   from srdatalog_b200 import workloads as W
+  if name == 'batched':
+    return make_batch()[1].inputs['ArcInput']
   cache = os.path.join('/tmp', f'srdl_bench_{name}.npy')
   if os.path.exists(cache):
     return np.load(cache)
@@ -70,6 +94,32 @@ def load_plan(name: str) -> dict:
 
 def result_units(db, wl) -> int:
   return db.count(wl['out']) if wl['kind'] == 'count' else db.size(wl['out'])
+
+
+def plain_loop(plan, insts, stride, stream_ptr, device):
+  '''The one-query-at-a-time loop: every sampled instance through its own
+  srdl_run on one handle (host rows, result size read back).'''
+  import torch
+  from srdatalog_b200 import Database
+  db = Database(plan, device=device)
+  db.set_stream(stream_ptr)
+  sample = insts[::stride]
+  for inst in sample[:4]:  # warm-up
+    db.clear_inputs()
+    db.load_rows('ArcInput', inst['ArcInput'])
+    db.run()
+  torch.cuda.synchronize()
+  t0 = time.perf_counter()
+  sizes = []
+  for inst in sample:
+    db.clear_inputs()
+    db.load_rows('ArcInput', inst['ArcInput'])
+    db.run()
+    sizes.append(db.size('Path'))
+  dt = time.perf_counter() - t0
+  db.close()
+  return {'queries_per_s': len(sample) / dt, 'ms_per_query': 1e3 * dt / len(sample),
+          'sample': f'every {stride}th of {len(insts)} instances ({len(sample)})'}, sizes
 
 
 class ClockSampler:
@@ -138,6 +188,15 @@ def cpu_baseline(wl_name: str, edges: np.ndarray) -> dict:
   cores, on a bounded sample; returns tuples/s for the same metric.'''
   import oracle
   cores = oracle.num_threads()
+  if wl_name == 'batched':
+    insts, _ = make_batch()
+    sample = insts[::PLAIN_SAMPLE_STRIDE]
+    t0 = time.perf_counter()
+    for inst in sample:
+      oracle.tc(inst['ArcInput'])
+    dt = time.perf_counter() - t0
+    return {'value': len(sample) / dt, 'unit': 'queries/s', 'cores': cores, 'kind': 'port',
+            'sample': f'TC of every {PLAIN_SAMPLE_STRIDE}th instance ({len(sample)}), {dt:.2f} s'}
   if wl_name == 'triangle':
     stride = 4
     c, t_sort, t_join = oracle.triangle_count_sample(edges, stride)
@@ -170,12 +229,13 @@ def run_reference(args, rank, world):
       vals.append(cb['value'])
   v = statistics.median(vals)
   cb['value'] = v
-  line = {'impl': 'reference', 'metric': f'tuples/s ({args.workload})', 'value': v,
-          'unit': 'tuples/s', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+  unit = cb['unit']
+  line = {'impl': 'reference', 'metric': f'{unit} ({args.workload})', 'value': v,
+          'unit': unit, 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
           'ms_per_step': None, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
           'dtype': 'u32', 'data': 'synthetic',
           'config': {'workload': wl['desc']}, 'cpu_baseline': cb,
-          'e2e': {'value': v, 'unit': 'tuples/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+          'e2e': {'value': v, 'unit': unit, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
   print(json.dumps(line), flush=True)
 
 
@@ -226,6 +286,15 @@ def main():
   for _ in range(args.warmup):
     db.run()
   units = result_units(db, wl)
+  batched = wl['kind'] == 'batched'
+  if batched:  # one step answers every instance: the metric counts queries
+    insts, union = make_batch()
+    bounds = union.offsets.astype(np.uint32)
+    per_step = len(insts)
+  else:
+    per_step = units
+  metric_name = f'{"queries" if batched else "tuples"}/s ({args.workload})'
+  unit_name = 'queries/s' if batched else 'tuples/s'
   kernels: dict = {}
   step_ms = []
   launches = 0
@@ -258,7 +327,7 @@ def main():
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_ms = float(t.item())
-  value = units * args.steps * world / (total_ms / 1e3)
+  value = per_step * args.steps * world / (total_ms / 1e3)
   stats = db.stats()
   db.close()
   del d_edges
@@ -268,7 +337,7 @@ def main():
     if dist:
       dist.destroy_process_group()
     if rank == 0:
-      print(json.dumps({'metric': f'tuples/s ({args.workload})', 'value': value,
+      print(json.dumps({'metric': metric_name, 'value': value,
                         'ms_per_step': total_ms / args.steps, 'quick': True,
                         'step_ms': [round(x, 3) for x in step_ms]}), flush=True)
     return
@@ -287,6 +356,8 @@ def main():
     ev0.record(stream)
     db2.run()
     got = result_units(db2, wl)  # result read back to the host
+    if batched:  # every instance's size read back
+      per_inst = db2.range_counts(wl['out'], bounds)
     ev1.record(stream)
     ev1.synchronize()
     e2e_ms.append(ev0.elapsed_time(ev1))
@@ -297,6 +368,11 @@ def main():
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_total = float(t.item())
   db2.close()
+  plain = None
+  if batched and not args.no_cpu_baseline:
+    # the one-query-at-a-time loop on a sample, checked instance by instance
+    plain, sizes = plain_loop(plan, insts, PLAIN_SAMPLE_STRIDE, stream.cuda_stream, local)
+    assert [int(x) for x in per_inst[::PLAIN_SAMPLE_STRIDE]] == sizes
 
   if dist:
     dist.barrier()
@@ -321,16 +397,17 @@ def main():
           'ms_per_launch': k['ms'] / max(1, k['scopes']),
           'share_of_step': k['ms'] / total_ms if world == 1 else None}
   line = {
-    'metric': f'tuples/s ({args.workload})', 'value': value, 'unit': 'tuples/s', 'n_gpus': world,
+    'metric': metric_name, 'value': value, 'unit': unit_name, 'n_gpus': world,
     'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
     'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'u32',
     'data': 'synthetic',
     'config': {'workload': wl['desc'], 'edges': int(n), 'tuples_per_step': int(units),
                'parallelism': f'replicas{world}', 'l2': 'flushed between steps (256 MB write)',
                'inputs': 'HBM-resident for value; pinned host rows for e2e'},
-    'e2e': {'value': units * args.steps * world / (e2e_total / 1e3), 'unit': 'tuples/s',
+    'e2e': {'value': per_step * args.steps * world / (e2e_total / 1e3), 'unit': unit_name,
             'ms_per_step': e2e_total / args.steps, 'h2d_bytes_per_step': int(n) * 8,
-            'd2h_bytes_per_step': 8, 'step_ms': [round(x, 3) for x in e2e_ms]},
+            'd2h_bytes_per_step': 8 + (8 * per_step if batched else 0),
+            'step_ms': [round(x, 3) for x in e2e_ms]},
     'step_ms': [round(x, 3) for x in step_ms],
     'gpu_launches': int(launches),
     'roofline': roof,
@@ -340,6 +417,11 @@ def main():
     'iterations': [s['iterations'] for s in stats['steps']],
     'clocks': clocks,
   }
+  if batched:
+    line['config'].update(instances=per_step, tuples_per_s=units * args.steps * world / (total_ms / 1e3))
+    if plain:
+      line['plain_loop'] = plain
+      line['speedup_vs_plain_loop'] = value / plain['queries_per_s']
   if world == 1 and not args.no_cpu_baseline:
     line['cpu_baseline'] = cpu_baseline(args.workload, edges)
   print(json.dumps(line), flush=True)

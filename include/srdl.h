@@ -78,6 +78,17 @@ int srdl_set_profiling(srdl_db* db, int enable);
 /* Kernels this process has launched through libsrdl so far. */
 uint64_t srdl_launch_count(void);
 
+/* Drop every staged input (host and device rows) so the handle can be
+ * reloaded with another input; the plan stays.  No reference counterpart. */
+int srdl_clear_inputs(srdl_db* db);
+
+/* counts[j] = rows of FULL(rel) whose first declared column lies in
+ * [bounds[j], bounds[j+1]) for j < n_bounds-1 (host arrays; bounds
+ * non-decreasing).  Splits a disjoint-union batch into per-instance sizes.
+ * No reference counterpart. */
+int srdl_range_counts(srdl_db* db, const char* rel, const uint32_t* bounds, uint64_t n_bounds,
+                      uint64_t* counts);
+
 /* Rows currently staged for `rel` by the load calls (host-side count). */
 uint64_t srdl_staged_rows(srdl_db* db, const char* rel);
 

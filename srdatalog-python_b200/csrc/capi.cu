@@ -190,6 +190,17 @@ int srdl_load_device_rows(srdl_db* h, const char* rel, const uint32_t* d_rows, u
 
 uint64_t srdl_launch_count(void) { return srdl::launches_total(); }
 
+int srdl_clear_inputs(srdl_db* h) {
+  if (!h) return kErrArg;
+  SRDL_GUARD(0, h->db->clear_inputs(); return 0;)
+}
+
+int srdl_range_counts(srdl_db* h, const char* rel, const uint32_t* bounds, uint64_t n_bounds,
+                      uint64_t* counts) {
+  if (!h || !rel || (n_bounds > 1 && !counts)) return kErrArg;
+  SRDL_GUARD(0, h->db->range_counts(rel, bounds, n_bounds, counts); return 0;)
+}
+
 uint64_t srdl_staged_rows(srdl_db* h, const char* rel) {
   if (!h || !rel || !h->db->has_rel(rel)) return 0;
   return h->db->staged_rows(rel);

@@ -84,6 +84,10 @@ void child_hash_build(const Launch& L, const uint64_t* keys, uint64_t n, const u
                       uint32_t dir_n, const uint64_t* sizes, const uint64_t* offs, uint32_t* hdir,
                       uint32_t* pool);
 
+// pos[j] = first row of the sorted keys whose high word is >= bounds[j].
+void bounds_positions(const Launch& L, const uint64_t* keys, uint64_t n, const uint32_t* bounds,
+                      uint64_t n_bounds, uint64_t* pos);
+
 // Swap the two 32-bit halves of every key (index permutation (1,0) <-> (0,1)).
 void swap_halves(const Launch& L, const uint64_t* in, uint64_t n, uint64_t* out);
 

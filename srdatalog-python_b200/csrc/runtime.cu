@@ -327,6 +327,45 @@ void Database::load_rows(const std::string& name, const uint32_t* rows, uint64_t
   r.loaded = true;
 }
 
+void Database::clear_inputs() {
+  for (auto& kv : rels_) {
+    Relation& r = *kv.second;
+    r.staged.clear();
+    r.staged.shrink_to_fit();
+    r.pinned_words = 0;
+    r.dstaged.reset();
+    r.dstaged_n = 0;
+    r.dstaged_max = 0;
+    r.loaded = false;
+  }
+}
+
+void Database::range_counts(const std::string& name, const uint32_t* bounds, uint64_t n_bounds,
+                            uint64_t* counts) {
+  Relation& r = rel(name);
+  SRDL_REQUIRE(bounds || n_bounds == 0, kErrArg, "range_counts: null bounds");
+  if (n_bounds < 2) return;
+  for (uint64_t j = 0; j + 1 < n_bounds; j++)
+    SRDL_REQUIRE(bounds[j] <= bounds[j + 1], kErrArg, "range_counts: bounds must be non-decreasing");
+  if (!r.v[kFull].has_index() || r.arity > 2) {
+    for (uint64_t j = 0; j + 1 < n_bounds; j++) counts[j] = 0;
+    return;
+  }
+  SRDL_CUDA(cudaSetDevice(device_));
+  Index& ix = ensure_index(r, kFull, identity_perm(r.arity));
+  DevBuf d_bounds(n_bounds * 4, L_.stream);
+  DevBuf d_pos(n_bounds * 8, L_.stream);
+  SRDL_CUDA(cudaMemcpyAsync(d_bounds.as<void>(), bounds, n_bounds * 4, cudaMemcpyHostToDevice,
+                            L_.stream));
+  bounds_positions(L_, ix.keys.as<uint64_t>(), ix.n, d_bounds.as<uint32_t>(), n_bounds,
+                   d_pos.as<uint64_t>());
+  std::vector<uint64_t> pos(n_bounds);
+  SRDL_CUDA(cudaMemcpyAsync(pos.data(), d_pos.as<void>(), n_bounds * 8, cudaMemcpyDeviceToHost,
+                            L_.stream));
+  SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  for (uint64_t j = 0; j + 1 < n_bounds; j++) counts[j] = pos[j + 1] - pos[j];
+}
+
 void Database::load_device_rows(const std::string& name, const uint32_t* d_rows, uint64_t n) {
   Relation& r = rel(name);
   SRDL_REQUIRE(d_rows || n == 0, kErrArg, "load_device_rows: null rows");

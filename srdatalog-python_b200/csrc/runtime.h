@@ -138,6 +138,11 @@ class Database {
 
   void load_rows(const std::string& rel, const uint32_t* rows, uint64_t n);
   void load_device_rows(const std::string& rel, const uint32_t* d_rows, uint64_t n);
+  void clear_inputs();
+  // counts[j] = rows of FULL(rel) whose first declared column is in
+  // [bounds[j], bounds[j+1]), for j < n_bounds - 1.
+  void range_counts(const std::string& rel, const uint32_t* bounds, uint64_t n_bounds,
+                    uint64_t* counts);
   void set_stream(cudaStream_t s);
   void set_profiling(bool on) { profile_ = on; }
   void load_csv(const std::string& rel, const std::string& path);

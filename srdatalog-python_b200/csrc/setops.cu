@@ -230,6 +230,22 @@ void child_hash_build(const Launch& L, const uint64_t* keys, uint64_t n, const u
   count_launches(n ? 2 : 1);
 }
 
+__global__ void bounds_kernel(const uint64_t* __restrict__ keys, uint64_t n,
+                              const uint32_t* __restrict__ bounds, uint64_t nb,
+                              uint64_t* __restrict__ pos) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < nb;
+       j += (uint64_t)gridDim.x * blockDim.x)
+    pos[j] = lower_bound_u64(keys, 0, n, (uint64_t)bounds[j] << 32);
+}
+
+void bounds_positions(const Launch& L, const uint64_t* keys, uint64_t n, const uint32_t* bounds,
+                      uint64_t n_bounds, uint64_t* pos) {
+  if (!n_bounds) return;
+  bounds_kernel<<<grid_for(n_bounds, L.num_sms), 256, 0, L.stream>>>(keys, n, bounds, n_bounds, pos);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(1);
+}
+
 __global__ void max_kernel(const uint32_t* __restrict__ d, uint64_t n, uint32_t* __restrict__ out) {
   uint32_t m = 0;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;

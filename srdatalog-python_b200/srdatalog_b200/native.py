@@ -37,6 +37,8 @@ SIGNATURES = {
   'srdl_set_stream': (ctypes.c_int, [_vp, _vp]),
   'srdl_set_profiling': (ctypes.c_int, [_vp, ctypes.c_int]),
   'srdl_launch_count': (_u64, []),
+  'srdl_clear_inputs': (ctypes.c_int, [_vp]),
+  'srdl_range_counts': (ctypes.c_int, [_vp, _cp, _u32p, _u64, ctypes.POINTER(_u64)]),
   'srdl_run': (ctypes.c_int, [_vp, _u64]),
   'srdl_size': (_u64, [_vp, _cp]),
   'srdl_count': (_u64, [_vp, _cp]),
@@ -137,6 +139,18 @@ class Database:
 
   def set_profiling(self, on: bool = True) -> None:
     check(lib().srdl_set_profiling(self._h, 1 if on else 0), 'srdl_set_profiling')
+
+  def clear_inputs(self) -> None:
+    check(lib().srdl_clear_inputs(self._h), 'srdl_clear_inputs')
+
+  def range_counts(self, rel: str, bounds) -> np.ndarray:
+    '''Rows of FULL(rel) per first-column range [bounds[j], bounds[j+1]).'''
+    b = np.ascontiguousarray(bounds, dtype=np.uint32)
+    out = np.zeros(max(0, b.shape[0] - 1), np.uint64)
+    check(lib().srdl_range_counts(self._h, rel.encode(), b.ctypes.data_as(_u32p), b.shape[0],
+                                  out.ctypes.data_as(ctypes.POINTER(_u64))),
+          f'srdl_range_counts({rel})')
+    return out
 
   def staged_rows(self, rel: str) -> int:
     return int(lib().srdl_staged_rows(self._h, rel.encode()))
