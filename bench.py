@@ -188,6 +188,19 @@ def cpu_baseline(wl_name: str, edges: np.ndarray) -> dict:
   cores, on a bounded sample; returns tuples/s for the same metric.'''
   import oracle
   cores = oracle.num_threads()
+  if wl_name == 'served':
+    reqs = serve_requests(serve_pool(), 64, seed=11)
+    fn = {'tc': oracle.tc, 'sg': oracle.sg}
+    t0 = time.perf_counter()
+    for r in reqs:
+      e = list(r.inputs.values())[0]
+      if r.program == 'triangle':
+        oracle.triangle_count(e)
+      else:
+        fn[r.program](e)
+    dt = time.perf_counter() - t0
+    return {'value': len(reqs) / dt, 'unit': 'queries/s', 'cores': cores, 'kind': 'port',
+            'sample': f'first 64 requests of the served stream, one at a time ({dt:.2f} s)'}
   if wl_name == 'batched':
     insts, _ = make_batch()
     sample = insts[::PLAIN_SAMPLE_STRIDE]
@@ -218,10 +231,10 @@ def cpu_baseline(wl_name: str, edges: np.ndarray) -> dict:
 
 
 def run_reference(args, rank, world):
-  wl = WORKLOADS[args.workload]
+  wl = WORKLOADS.get(args.workload, {'desc': SERVE_DESC})
   if rank != 0:
     return
-  edges = make_edges(args.workload)
+  edges = None if args.workload == 'served' else make_edges(args.workload)
   vals = []
   for i in range(args.warmup + args.steps):
     cb = cpu_baseline(args.workload, edges)
@@ -239,13 +252,102 @@ def run_reference(args, rank, world):
   print(json.dumps(line), flush=True)
 
 
+SERVE_MIX = (('tc', 0.5), ('sg', 0.3), ('triangle', 0.2))
+SERVE_POOL = 48          # distinct inputs per program; requests draw from them
+SERVE_REQUESTS = 512
+SERVE_DESC = ('served queries: Poisson arrivals, 50% TC / 30% SG / 20% triangle count, input '
+              'edges log-uniform in [1e3, 4e6] (TC subcritical n=2m, SG forest n<=5,000, '
+              'triangle R-MAT), 120 GB admission budget, 4 workers, continuous batching')
+
+
+def serve_pool():
+  '''SERVE_POOL seeded inputs per program with log-uniform sizes (cached).'''
+  from srdatalog_b200 import workloads as W
+  from srdatalog_b200.serve import log_uniform_sizes
+  pool = {}
+  for k, (prog, _) in enumerate(SERVE_MIX):
+    cache = os.path.join('/tmp', f'srdl_serve_{prog}.npz')
+    if os.path.exists(cache):
+      z = np.load(cache)
+      pool[prog] = [z[f'a{i}'] for i in range(SERVE_POOL)]
+      continue
+    sizes = log_uniform_sizes(SERVE_POOL, 1e3, 4e6, seed=50 + k)
+    pool[prog] = [list(W.served_request_input(prog, int(m), 700 + 97 * k + i).values())[0]
+                  for i, m in enumerate(sizes)]
+    try:
+      np.savez(cache, **{f'a{i}': a for i, a in enumerate(pool[prog])})
+    except OSError:
+      pass
+  return pool
+
+
+def serve_requests(pool, n, seed):
+  from srdatalog_b200.serve import Request
+  rel = {'tc': 'ArcInput', 'sg': 'Arc', 'triangle': 'KnowsInput'}
+  rng = np.random.Generator(np.random.PCG64(seed))
+  progs = rng.choice([p for p, _ in SERVE_MIX], size=n, p=[w for _, w in SERVE_MIX])
+  picks = rng.integers(0, SERVE_POOL, n)
+  return [Request(i, str(p), {rel[str(p)]: pool[str(p)][int(j)]}) for i, (p, j) in
+          enumerate(zip(progs, picks))]
+
+
+def run_served(args, rank, world):
+  '''Served queries: the batching server vs the plain one-at-a-time loop on
+  the same seeded request stream.  One step = one replay of the stream.'''
+  import torch
+  from srdatalog_b200.serve import ProgramSpec, Server, poisson_arrivals, replay
+  if world > 1 and rank != 0:
+    return
+  progs = {'tc': ProgramSpec(load_plan('tc'), 'Path'), 'sg': ProgramSpec(load_plan('sg'), 'Sg'),
+           'triangle': ProgramSpec(load_plan('triangle'), 'TriangleJoin', count_only=True)}
+  pool = serve_pool()
+  rate = args.rate
+  offs = poisson_arrivals(SERVE_REQUESTS, rate, seed=5)
+  torch.cuda.init()
+  with Server(progs, workers=4, budget_bytes=120 << 30) as srv:
+    for w in range(args.warmup):  # warm-up replays (handles, pools, caches)
+      replay(srv, serve_requests(pool, 64, seed=900 + w), poisson_arrivals(64, rate, seed=w))
+    results, sums = None, []
+    for s in range(args.steps):
+      reqs = serve_requests(pool, SERVE_REQUESTS, seed=11)
+      st = replay(srv, reqs, offs)
+      got = [r.result for r in reqs]
+      assert results is None or got == results  # same answers every replay
+      results = got
+      sums.append(st.summary())
+  h2d = sum(int(list(r.inputs.values())[0].nbytes) for r in serve_requests(pool, SERVE_REQUESTS, 11))
+  with Server(progs, workers=1, batching=False) as plain_srv:
+    reqs = serve_requests(pool, SERVE_REQUESTS, seed=11)
+    pst = replay(plain_srv, reqs, offs).summary()
+    assert [r.result for r in reqs] == results
+  qps = statistics.median(s['queries_per_s'] for s in sums)
+  line = {
+    'metric': 'queries/s (served)', 'value': qps, 'unit': 'queries/s', 'n_gpus': 1,
+    'steps': args.steps, 'warmup': args.warmup,
+    'ms_per_step': statistics.median(s['wall_s'] for s in sums) * 1e3,
+    'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'u32',
+    'data': 'synthetic',
+    'config': {'workload': SERVE_DESC, 'offered_rate': rate, 'requests_per_step': SERVE_REQUESTS},
+    'latency_ms': {'p50': statistics.median(s['p50_ms'] for s in sums),
+                   'p99': statistics.median(s['p99_ms'] for s in sums)},
+    'mean_batch': statistics.median(s['mean_batch'] for s in sums),
+    'plain_loop': pst, 'speedup_vs_plain_loop': qps / pst['queries_per_s'],
+    'e2e': {'value': qps, 'unit': 'queries/s', 'h2d_bytes_per_step': h2d,
+            'd2h_bytes_per_step': 8 * SERVE_REQUESTS,
+            'note': 'every request is end to end: host rows in, its size/count read back'},
+    'roofline': None,
+  }
+  print(json.dumps(line), flush=True)
+
+
 def main():
   ap = argparse.ArgumentParser()
   ap.add_argument('--gpus', type=int, default=1)
   ap.add_argument('--steps', type=int, default=10)
   ap.add_argument('--warmup', type=int, default=3)
   ap.add_argument('--impl', default='srdl', choices=['srdl', 'reference'])
-  ap.add_argument('--workload', default='triangle', choices=sorted(WORKLOADS))
+  ap.add_argument('--workload', default='triangle', choices=sorted(WORKLOADS) + ['served'])
+  ap.add_argument('--rate', type=float, default=2000.0, help='served: offered load (req/s)')
   ap.add_argument('--no-cpu-baseline', action='store_true')
   ap.add_argument('--quick', action='store_true',
                   help='kernel-resident path only (no e2e, no CPU baseline): for profiler runs')
@@ -257,6 +359,8 @@ def main():
   local = int(os.environ.get('LOCAL_RANK', '0'))
   if args.impl == 'reference':
     return run_reference(args, rank, world)
+  if args.workload == 'served':
+    return run_served(args, rank, world)
 
   import torch
   dist = None

@@ -1,0 +1,277 @@
+'''Serving: a request loop that admits Datalog queries of mixed programs and
+sizes against a device-memory budget and batches them continuously.
+
+* Admission: every request carries an estimate of the device memory its
+  evaluation needs (`footprint`); it is admitted when the sum over admitted,
+  unfinished requests stays within the budget, in arrival order (a large
+  request waits; later small ones do not overtake it).
+* Continuous batching: a dispatcher hands work to whichever of the `workers`
+  is idle.  A worker takes the oldest admitted request and, with it, every
+  admitted request of the same program (up to `max_batch`), and evaluates
+  them as one disjoint-union run (srdatalog_b200.batch): their iterations share
+  launches.  Count-only programs (the triangle count) cannot be split per
+  request after a union run and are evaluated one request per run.
+* Workers own their database handles, so each has its own CUDA stream and
+  the runs of different workers overlap on the GPU; relations stay on the
+  device until the request's result (its size or count) has been read.
+
+A request's result is identical alone and in any mix: instances of a union
+cannot interact (see batch.py), and runs on different handles share nothing.
+'''
+
+from __future__ import annotations
+
+import math
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .batch import make_union
+from .native import Database
+
+
+@dataclass
+class Request:
+  rid: int
+  program: str                 # key into the server's plans
+  inputs: dict                 # relation -> (m, 2) uint32 rows
+  arrival: float = 0.0         # seconds (perf_counter clock)
+  footprint: int = 0           # estimated device bytes
+  admitted: float = -1.0
+  started: float = -1.0
+  finished: float = -1.0
+  result: int = -1             # size of the output relation, or the count
+  rows: np.ndarray | None = None
+  batch_size: int = 0
+
+  @property
+  def latency(self) -> float:
+    return self.finished - self.arrival
+
+
+@dataclass
+class ProgramSpec:
+  plan: dict
+  out: str                     # output relation (size) or rule (count)
+  count_only: bool = False
+  bytes_per_edge: int = 512    # footprint estimate per input edge
+
+
+def default_footprint(spec: ProgramSpec, req: Request) -> int:
+  m = sum(int(np.asarray(r).shape[0]) for r in req.inputs.values())
+  return max(1 << 20, m * spec.bytes_per_edge)
+
+
+@dataclass
+class ServeStats:
+  requests: list = field(default_factory=list)
+  wall_s: float = 0.0
+
+  def summary(self) -> dict:
+    lat = np.array([r.latency for r in self.requests]) * 1e3
+    bs = np.array([r.batch_size for r in self.requests])
+    return {
+      'requests': len(self.requests),
+      'queries_per_s': len(self.requests) / self.wall_s if self.wall_s else 0.0,
+      'p50_ms': float(np.percentile(lat, 50)) if lat.size else None,
+      'p99_ms': float(np.percentile(lat, 99)) if lat.size else None,
+      'mean_batch': float(bs.mean()) if bs.size else None,
+      'wall_s': self.wall_s,
+    }
+
+
+class Server:
+  '''Admission-controlled, continuously batching request loop (see module doc).'''
+
+  def __init__(self, programs: dict, device: int = 0, workers: int = 4,
+               budget_bytes: int = 120 << 30, max_batch: int = 256, batching: bool = True,
+               keep_rows: bool = False):
+    self.programs = programs
+    self.device = device
+    self.budget = budget_bytes
+    self.max_batch = max_batch if batching else 1
+    self.keep_rows = keep_rows
+    self.cv = threading.Condition()
+    self.pending: list[Request] = []   # arrived, waiting for admission (FIFO)
+    self.ready: list[Request] = []     # admitted, not started
+    self.in_use = 0
+    self.peak_in_use = 0
+    self.submitted = 0
+    self.done: list[Request] = []
+    self.errors: list[BaseException] = []
+    self.stopping = False
+    self.threads = [threading.Thread(target=self._worker, args=(w,), daemon=True)
+                    for w in range(workers)]
+    for t in self.threads:
+      t.start()
+
+  # ------------------------------------------------------------ client side
+  def submit(self, req: Request) -> None:
+    spec = self.programs[req.program]
+    if not req.footprint:
+      req.footprint = default_footprint(spec, req)
+    with self.cv:
+      self.pending.append(req)
+      self.submitted += 1
+      self._admit()
+      self.cv.notify_all()
+
+  def drain(self, timeout_s: float = 3600.0) -> None:
+    '''Wait until every submitted request has finished (or raise).'''
+    deadline = time.perf_counter() + timeout_s
+    with self.cv:
+      while len(self.done) < self.submitted and not self.errors:
+        left = deadline - time.perf_counter()
+        if left <= 0:
+          raise TimeoutError('serving did not drain in time')
+        self.cv.wait(min(left, 1.0))
+      if self.errors:
+        raise RuntimeError(f'worker failed: {self.errors[0]!r}')
+
+  def close(self) -> None:
+    with self.cv:
+      self.stopping = True
+      self.cv.notify_all()
+    for t in self.threads:
+      t.join(timeout=60)
+
+  def __enter__(self):
+    return self
+
+  def __exit__(self, *exc):
+    self.close()
+
+  # ------------------------------------------------------------ scheduling
+  def _admit(self) -> None:
+    now = time.perf_counter()
+    while self.pending:
+      r = self.pending[0]
+      # a request larger than the whole budget runs alone
+      if self.in_use + r.footprint > self.budget and self.in_use > 0:
+        break
+      self.pending.pop(0)
+      self.in_use += r.footprint
+      self.peak_in_use = max(self.peak_in_use, self.in_use)
+      r.admitted = now
+      self.ready.append(r)
+
+  def _take_batch(self) -> list:
+    first = self.ready[0]
+    spec = self.programs[first.program]
+    if spec.count_only or self.max_batch == 1:
+      batch = [first]
+    else:
+      batch, span = [], 0
+      for r in self.ready:
+        if r.program != first.program:
+          continue
+        s = _span(r)
+        if batch and (len(batch) >= self.max_batch or span + s > 0xFFFFFFFF):
+          break
+        batch.append(r)
+        span += s
+    ids = {id(r) for r in batch}
+    self.ready = [r for r in self.ready if id(r) not in ids]
+    return batch
+
+  def _worker(self, wid: int) -> None:
+    dbs: dict = {}
+    try:
+      while True:
+        with self.cv:
+          while not self.ready and not self.stopping:
+            self.cv.wait()
+          if not self.ready:
+            return
+          batch = self._take_batch()
+        t0 = time.perf_counter()
+        for r in batch:
+          r.started = t0
+          r.batch_size = len(batch)
+        self._run(dbs, batch)
+        t1 = time.perf_counter()
+        with self.cv:
+          for r in batch:
+            r.finished = t1
+            self.in_use -= r.footprint
+          self.done.extend(batch)
+          self._admit()
+          self.cv.notify_all()
+    except BaseException as e:  # surface to drain()
+      with self.cv:
+        self.errors.append(e)
+        self.cv.notify_all()
+    finally:
+      for db in dbs.values():
+        db.close()
+
+  def _run(self, dbs: dict, batch: list) -> None:
+    spec = self.programs[batch[0].program]
+    db = dbs.get(batch[0].program)
+    if db is None:
+      db = dbs[batch[0].program] = Database(spec.plan, device=self.device)
+    db.clear_inputs()
+    if len(batch) == 1:
+      r = batch[0]
+      for rel, rows in r.inputs.items():
+        db.load_rows(rel, rows)
+      db.run()
+      r.result = db.count(spec.out) if spec.count_only else db.size(spec.out)
+      if self.keep_rows and not spec.count_only:
+        r.rows = db.dump(spec.out)
+      return
+    union = make_union([r.inputs for r in batch])
+    for rel, rows in union.inputs.items():
+      db.load_rows(rel, rows)
+    db.run()
+    sizes = db.range_counts(spec.out, union.offsets.astype(np.uint32))
+    all_rows = db.dump(spec.out) if self.keep_rows else None
+    if all_rows is not None:
+      cuts = np.searchsorted(all_rows[:, 0], union.offsets.astype(np.int64), side='left')
+    for j, r in enumerate(batch):
+      r.result = int(sizes[j])
+      if all_rows is not None:
+        r.rows = (all_rows[cuts[j]:cuts[j + 1]].astype(np.uint64) - union.offsets[j]).astype(np.uint32)
+
+
+def _span(r: Request) -> int:
+  mx = -1
+  for rows in r.inputs.values():
+    a = np.asarray(rows)
+    if a.size:
+      mx = max(mx, int(a.max()))
+  return mx + 1 if mx >= 0 else 1
+
+
+def poisson_arrivals(n: int, rate: float, seed: int) -> np.ndarray:
+  '''n arrival offsets (seconds) of a Poisson process with the given rate.'''
+  rng = np.random.Generator(np.random.PCG64(seed))
+  return np.cumsum(rng.exponential(1.0 / rate, n))
+
+
+def replay(server: Server, requests: list, offsets: np.ndarray) -> ServeStats:
+  '''Open-loop client: submits request i at t0 + offsets[i] (its latency is
+  measured from that scheduled time), then waits for all to finish.'''
+  order = np.argsort(offsets, kind='stable')
+  t0 = time.perf_counter()
+  for i in order:
+    due = t0 + float(offsets[i])
+    d = due - time.perf_counter()
+    if d > 0:
+      time.sleep(d)
+    requests[i].arrival = due
+    server.submit(requests[i])
+  server.drain()
+  end = max(r.finished for r in requests)
+  return ServeStats(requests=list(requests), wall_s=end - t0)
+
+
+def log_uniform_sizes(n: int, lo: float, hi: float, seed: int) -> np.ndarray:
+  rng = np.random.Generator(np.random.PCG64(seed))
+  return np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), n))).astype(np.int64)
+
+
+__all__ = ['Request', 'ProgramSpec', 'Server', 'ServeStats', 'replay', 'poisson_arrivals',
+           'log_uniform_sizes', 'default_footprint']

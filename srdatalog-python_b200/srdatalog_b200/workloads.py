@@ -128,6 +128,23 @@ def batched_instances(count: int = 4096, n_lo: int = 64, n_hi: int = 65536,
   return out
 
 
+def served_request_input(program: str, m: int, seed: int) -> dict:
+  '''Input of one served request with about m input edges, generated as in
+  the corresponding config but kept small enough for its closure to fit:
+  TC on a subcritical Erdos-Renyi graph (n = 2m nodes, mean out-degree 1/2),
+  SG on the windowed forest with n = m/1.1 nodes (m capped at 5,500), and
+  the triangle count on an R-MAT graph with m draws (edge factor ~8).'''
+  if program == 'tc':
+    return {'ArcInput': er_instance(max(2, 2 * m), 0.5, seed)}
+  if program == 'sg':
+    n = max(16, int(round(min(m, 5_500) / 1.1)))
+    return {'Arc': sg_forest(n, window=min(1000, n - 1), seed=seed)}
+  if program == 'triangle':
+    scale = max(6, int(math.ceil(math.log2(max(m, 64) / 8))))
+    return {'KnowsInput': rmat_edges(scale, m, seed=seed, chunk=1 << 20)}
+  raise ValueError(program)
+
+
 def write_csv(edges: np.ndarray, path: str, delimiter: str = '\t') -> None:
   '''Write an edge list as the reference's loader reads it (one row per line).'''
   np.savetxt(path, edges.astype(np.int64), fmt='%d', delimiter=delimiter)

@@ -1,0 +1,54 @@
+'''Serving: admission and batch formation on the host (no GPU; no workers).'''
+
+import numpy as np
+from conftest import load_plan
+from srdatalog_b200.serve import ProgramSpec, Request, Server, poisson_arrivals
+
+
+def programs():
+  return {'tc': ProgramSpec(load_plan('tc'), 'Path'),
+          'triangle': ProgramSpec(load_plan('triangle'), 'TriangleJoin', count_only=True)}
+
+
+def req(i, prog, fp, n=4):
+  rel = 'ArcInput' if prog == 'tc' else 'KnowsInput'
+  return Request(i, prog, {rel: np.array([[0, i % n + 1]], np.uint32)}, footprint=fp)
+
+
+def test_admission_respects_budget_in_arrival_order():
+  s = Server(programs(), workers=0, budget_bytes=100)
+  for i, fp in enumerate([40, 40, 40, 10]):
+    s.submit(req(i, 'tc', fp))
+  assert [r.rid for r in s.ready] == [0, 1]       # 120 > 100: request 2 waits
+  assert [r.rid for r in s.pending] == [2, 3]     # and 3 does not overtake it
+  assert s.peak_in_use == 80
+
+
+def test_oversized_request_runs_alone():
+  s = Server(programs(), workers=0, budget_bytes=100)
+  s.submit(req(0, 'tc', 500))
+  assert [r.rid for r in s.ready] == [0]
+  s.submit(req(1, 'tc', 10))
+  assert [r.rid for r in s.pending] == [1]
+
+
+def test_batches_group_one_program_and_keep_counts_single():
+  s = Server(programs(), workers=0, budget_bytes=1 << 40, max_batch=3)
+  for i, p in enumerate(['tc', 'triangle', 'tc', 'tc', 'tc', 'triangle']):
+    s.submit(req(i, p, 1))
+  b1 = s._take_batch()
+  assert [r.rid for r in b1] == [0, 2, 3]         # oldest program, max_batch of it
+  b2 = s._take_batch()
+  assert [r.rid for r in b2] == [1]               # count-only: one per run
+  assert [r.rid for r in s.ready] == [4, 5]
+  plain = Server(programs(), workers=0, batching=False)
+  for i in range(3):
+    plain.submit(req(i, 'tc', 1))
+  assert len(plain._take_batch()) == 1
+
+
+def test_poisson_arrivals_seeded():
+  a = poisson_arrivals(1000, 500.0, seed=5)
+  assert np.all(np.diff(a) >= 0)
+  assert abs(a[-1] - 2.0) < 0.3
+  assert np.array_equal(a, poisson_arrivals(1000, 500.0, seed=5))
