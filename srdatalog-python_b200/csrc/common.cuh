@@ -68,7 +68,7 @@ struct TrieView {
   const uint32_t* hdir = nullptr;
   const uint32_t* hpool = nullptr;
   uint64_t n = 0;
-  uint32_t n_roots = 0;
+  const uint64_t* n_roots_d = nullptr;  // device-resident root count
   uint32_t dir_n = 0;
   int arity = 2;
 };

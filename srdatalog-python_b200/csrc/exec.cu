@@ -165,6 +165,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
   Table cur;
   cur.n = 1;
   std::vector<DevBuf> cur_cols;
+  DevBuf cur_count;
   for (size_t li = 0; li < levels.size(); li++) {
     LevelSpec& lv = levels[li];
     const bool last = li + 1 == levels.size();
@@ -195,7 +196,10 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
         pid = prof_begin("join_expand_keys");
         join_expand(L_, lv, cur, w, total, nullptr, ch.keys.as<uint64_t>(),
                     d_small_.as<uint64_t>() + 2, s);
-        ch.n = total ? read_scalar(2) : 0;
+        // a filter-free two-source product emits exactly its candidates
+        const bool exact = lv.kind == kCartesian && lv.nsrc == 2 && lv.src[0].out_slot >= 0 &&
+                           lv.src[1].out_slot >= 0 && lv.nfilt == 0;
+        ch.n = total == 0 ? 0 : exact ? total : read_scalar(2);
         prof_end(pid, 4.0 * total * std::max(1, lv.nsrc) + 8.0 * ch.n, (double)total);
         derived_ += ch.n;
         target->v[kNew].chunks.push_back(std::move(ch));
@@ -210,13 +214,18 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
         cols.emplace_back(std::max<uint64_t>(total, 1) * 4, L_.stream);
         next.col[c] = cols.back().as<uint32_t>();
       }
+      // The table's row count stays on the device; the next level uses the
+      // candidate total as capacity and reads the true count itself.
+      DevBuf count(8, L_.stream);
+      SRDL_CUDA(cudaMemsetAsync(count.as<void>(), 0, 8, L_.stream));
       pid = prof_begin("join_expand_table");
-      join_expand(L_, lv, cur, w, total, &next, nullptr, d_small_.as<uint64_t>() + 2, s);
-      next.n = total ? read_scalar(2) : 0;
-      prof_end(pid, 4.0 * total * std::max(1, lv.nsrc) + 4.0 * next.n * levels[li + 1].n_in_slots,
-               (double)total);
+      join_expand(L_, lv, cur, w, total, &next, nullptr, count.as<uint64_t>(), s);
+      prof_end(pid, 4.0 * total * std::max(1, lv.nsrc), (double)total);
+      next.n = total;
+      next.d_n = count.as<uint64_t>();
       cur = next;
       cur_cols = std::move(cols);
+      cur_count = std::move(count);
     }
     if (!last && cur.n == 0) {
       if (op.count) counts_[op.rule] += 0;

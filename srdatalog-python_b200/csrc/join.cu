@@ -37,7 +37,7 @@ __device__ __forceinline__ void src_list(const SrcSpec& s, const Table& in, uint
                                          uint32_t& b, uint32_t& len) {
   if (s.prefix_slot < 0) {
     b = 0;
-    len = s.t.n_roots;
+    len = (uint32_t)*s.t.n_roots_d;
   } else {
     uint32_t e;
     trie_range(s.t, in.col[s.prefix_slot][r], b, e);
@@ -60,8 +60,15 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
                                                                uint8_t* __restrict__ drv,
                                                                uint32_t* __restrict__ beg,
                                                                uint2* __restrict__ orange) {
+  // A table written by the previous level may fill only part of its
+  // capacity; its true size is on the device and the rest expands to nothing.
+  const uint64_t nrows = in.d_n ? min(in.n, *in.d_n) : in.n;
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < in.n;
        r += (uint64_t)gridDim.x * blockDim.x) {
+    if (r >= nrows) {
+      work[r] = 0;
+      continue;
+    }
     if (lv.kind == kColumnJoin) {
       uint32_t best = 0xffffffffu, bb = 0;
       int bd = 0;

@@ -133,7 +133,8 @@ struct LevelSpec {
 
 struct Table {
   uint32_t* col[kMaxSlots] = {};
-  uint64_t n = 0;
+  uint64_t n = 0;                 // rows (or row capacity when d_n is set)
+  const uint64_t* d_n = nullptr;  // device-resident row count <= n, or null
 };
 
 size_t join_work_scratch_bytes(uint64_t rows);

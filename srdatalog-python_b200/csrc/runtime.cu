@@ -323,7 +323,7 @@ void Database::load_rows(const std::string& name, const uint32_t* rows, uint64_t
   SRDL_REQUIRE(r.arity <= 2, kErrUnsupported,
                "relation " + name + ": only arity 1 and 2 relations can be materialised");
   r.staged.insert(r.staged.end(), rows, rows + n * r.arity);
-  r.pinned_words = 0;  // page-locked mirror is stale
+  r.pinned_valid = false;  // page-locked mirror is stale
   r.loaded = true;
 }
 
@@ -332,7 +332,7 @@ void Database::clear_inputs() {
     Relation& r = *kv.second;
     r.staged.clear();
     r.staged.shrink_to_fit();
-    r.pinned_words = 0;
+    r.pinned_valid = false;
     r.dstaged.reset();
     r.dstaged_n = 0;
     r.dstaged_max = 0;
@@ -437,12 +437,17 @@ void Database::upload_inputs() {
     if (r.arity == 2) {
       // Host rows are copied once into page-locked memory so that every run
       // uploads them with one asynchronous DMA.
-      if (r.pinned_words != r.staged.size() && n) {
-        if (r.pinned) SRDL_CUDA(cudaFreeHost(r.pinned));
-        r.pinned = nullptr;
-        SRDL_CUDA(cudaMallocHost(&r.pinned, r.staged.size() * 4));
+      // (The page-locked buffer is kept and only grows: cudaFreeHost would
+      // synchronise the whole device and stall other handles' streams.)
+      if (!r.pinned_valid && n) {
+        if (r.staged.size() > r.pinned_cap) {
+          if (r.pinned) SRDL_CUDA(cudaFreeHost(r.pinned));
+          r.pinned = nullptr;
+          r.pinned_cap = std::max(r.staged.size(), r.pinned_cap + r.pinned_cap / 2);
+          SRDL_CUDA(cudaMallocHost(&r.pinned, r.pinned_cap * 4));
+        }
         memcpy(r.pinned, r.staged.data(), r.staged.size() * 4);
-        r.pinned_words = r.staged.size();
+        r.pinned_valid = true;
       }
       // A row-major (c0, c1) pair read as a little-endian uint64 is
       // (c1 << 32) | c0, i.e. the key of permutation (1,0).
@@ -492,7 +497,9 @@ void Database::ensure_trie(Relation& r, Index& ix) {
   build_lo(L_, ix.keys.as<uint64_t>(), n, ix.lo.as<uint32_t>());
   DevBuf scratch(roots_scratch_bytes(n) + 1024, L_.stream);
   Scratch s{scratch.as<char>(), scratch.bytes(), 0};
-  build_roots(L_, ix.keys.as<uint64_t>(), n, ix.roots.as<uint32_t>(), d_small_.as<uint64_t>() + 1, s);
+  // the root count stays on the device: kernels read it, the host never waits for it
+  ix.nroots_d = DevBuf(8, L_.stream);
+  build_roots(L_, ix.keys.as<uint64_t>(), n, ix.roots.as<uint32_t>(), ix.nroots_d.as<uint64_t>(), s);
   ix.dir_n = 0;
   if ((uint64_t)dom_max_ + 2 <= kDenseDirMax) {
     ix.dir_n = dom_max_ + 2;
@@ -500,8 +507,6 @@ void Database::ensure_trie(Relation& r, Index& ix) {
     build_dir(L_, ix.keys.as<uint64_t>(), n, ix.dir.as<uint32_t>(), ix.dir_n);
   }
   prof_end(pid, 8.0 * n + 4.0 * n + 8.0 * n + 4.0 * ix.dir_n, (double)n);
-  ix.n_roots = (uint32_t)read_scalar(1);
-  if (pid != (size_t)-1) kev_[pid].bytes += 4.0 * ix.n_roots;
   ix.trie = true;
 }
 
@@ -553,7 +558,7 @@ TrieView Database::view(Relation& r, Index& ix) {
   t.hdir = ix.hdir.bytes() ? ix.hdir.as<uint32_t>() : nullptr;
   t.hpool = ix.hpool.bytes() ? ix.hpool.as<uint32_t>() : nullptr;
   t.n = ix.n;
-  t.n_roots = ix.n_roots;
+  t.n_roots_d = ix.nroots_d.as<uint64_t>();
   t.dir_n = ix.dir_n;
   t.arity = r.arity;
   return t;

@@ -46,7 +46,8 @@ struct Index {
   uint64_t n = 0;
   bool trie = false;
   DevBuf lo, roots, dir;
-  uint32_t n_roots = 0, dir_n = 0;
+  DevBuf nroots_d;  // device-resident count of `roots`
+  uint32_t dir_n = 0;
   bool hash_done = false;  // hashed child lists built (or found unnecessary)
   DevBuf hdir, hpool;
 };
@@ -77,7 +78,8 @@ struct Relation {
   RelVersion v[3];
   std::vector<uint32_t> staged;  // host rows loaded before run (row-major)
   uint32_t* pinned = nullptr;    // page-locked copy of `staged` used for the upload
-  size_t pinned_words = 0;
+  size_t pinned_cap = 0;         // words allocated; grows, freed only at close
+  bool pinned_valid = false;     // holds the current `staged`
   DevBuf dstaged;                // device rows loaded before run (row-major pairs)
   uint64_t dstaged_n = 0;
   uint32_t dstaged_max = 0;
