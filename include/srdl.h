@@ -78,6 +78,18 @@ int srdl_set_profiling(srdl_db* db, int enable);
 /* Kernels this process has launched through libsrdl so far. */
 uint64_t srdl_launch_count(void);
 
+/* For the count-only rule `rule`, also count bindings per group of the
+ * rule's first bound variable: group g holds values in [bounds[g],
+ * bounds[g+1]) (n_bounds = groups + 1, host array, non-decreasing;
+ * n_bounds = 0 removes the grouping).  Splits the count of a disjoint-union
+ * batch per instance.  The rule's last level must be a two-source column
+ * join without filters (status 7 otherwise).  No reference counterpart. */
+int srdl_set_count_groups(srdl_db* db, const char* rule, const uint32_t* bounds,
+                          uint64_t n_bounds);
+
+/* Per-group counts of the last run (n_groups = bounds - 1). */
+int srdl_group_counts(srdl_db* db, const char* rule, uint64_t* out, uint64_t n_groups);
+
 /* Drop every staged input (host and device rows) so the handle can be
  * reloaded with another input; the plan stays.  No reference counterpart. */
 int srdl_clear_inputs(srdl_db* db);

@@ -190,6 +190,17 @@ int srdl_load_device_rows(srdl_db* h, const char* rel, const uint32_t* d_rows, u
 
 uint64_t srdl_launch_count(void) { return srdl::launches_total(); }
 
+int srdl_set_count_groups(srdl_db* h, const char* rule, const uint32_t* bounds,
+                          uint64_t n_bounds) {
+  if (!h || !rule) return kErrArg;
+  SRDL_GUARD(0, h->db->set_count_groups(rule, bounds, n_bounds); return 0;)
+}
+
+int srdl_group_counts(srdl_db* h, const char* rule, uint64_t* out, uint64_t n_groups) {
+  if (!h || !rule || (n_groups && !out)) return kErrArg;
+  SRDL_GUARD(0, h->db->group_counts(rule, out, n_groups); return 0;)
+}
+
 int srdl_clear_inputs(srdl_db* h) {
   if (!h) return kErrArg;
   SRDL_GUARD(0, h->db->clear_inputs(); return 0;)

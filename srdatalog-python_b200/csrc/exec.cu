@@ -181,8 +181,33 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
     if (last) {
       if (op.count) {
         lv.emit = kEmitCount;
+        DevBuf gb, gc;
+        auto grp = group_bounds_.find(op.rule);
+        if (grp != group_bounds_.end()) {
+          SRDL_REQUIRE(lv.kind == kColumnJoin && lv.nsrc == 2 && lv.nfilt == 0, kErrUnsupported,
+                       "grouped counts need a two-source column join without filters as the "
+                       "last level of rule " + op.rule);
+          const uint64_t ng = grp->second.size() - 1;
+          gb = DevBuf(grp->second.size() * 4, L_.stream);
+          gc = DevBuf(ng * 8, L_.stream);
+          SRDL_CUDA(cudaMemcpyAsync(gb.as<void>(), grp->second.data(), grp->second.size() * 4,
+                                    cudaMemcpyHostToDevice, L_.stream));
+          SRDL_CUDA(cudaMemsetAsync(gc.as<void>(), 0, ng * 8, L_.stream));
+          lv.grp_bounds = gb.as<uint32_t>();
+          lv.n_groups = (uint32_t)ng;
+          lv.grp_counts = gc.as<unsigned long long>();
+        }
         pid = prof_begin("join_expand_count");
         join_expand(L_, lv, cur, w, total, nullptr, nullptr, d_small_.as<uint64_t>() + 2, s);
+        if (lv.grp_counts) {
+          std::vector<uint64_t> h(lv.n_groups);
+          SRDL_CUDA(cudaMemcpyAsync(h.data(), gc.as<void>(), h.size() * 8, cudaMemcpyDeviceToHost,
+                                    L_.stream));
+          SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+          auto& acc = group_counts_[op.rule];
+          acc.resize(h.size(), 0);
+          for (size_t g = 0; g < h.size(); g++) acc[g] += h[g];
+        }
         // per candidate: its value (4 B) and one probed word of each other list (4 B)
         prof_end(pid, 4.0 * total * std::max(1, lv.nsrc), (double)total);
         counts_[op.rule] += read_scalar(2);

@@ -250,6 +250,23 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
         }
       }
       const unsigned m = __ballot_sync(kAllLanes, ok);
+      if (MODE == kModeCount && lv.grp_bounds) {
+        // per-group counts (one request of a batch per group): warp-aggregated
+        int g = -1;
+        if (ok) {
+          const uint32_t key = lv.n_in_slots > 0 ? in.col[0][r] : v;
+          uint32_t lo = 0, hi = lv.n_groups + 1;  // last bound <= key
+          while (lo + 1 < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (lv.grp_bounds[mid] <= key) lo = mid;
+            else hi = mid;
+          }
+          if (key >= lv.grp_bounds[0] && lo < lv.n_groups) g = (int)lo;
+        }
+        const unsigned peers = __match_any_sync(kAllLanes, g);
+        if (g >= 0 && lane == __ffs(peers) - 1)
+          atomicAdd(&lv.grp_counts[g], (unsigned long long)__popc(peers));
+      }
       if (MODE == kModeCount || MODE == kModeTableCount) {
         running += __popc(m);
       } else if (MODE == kModeKeys) {

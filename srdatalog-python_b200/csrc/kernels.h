@@ -129,6 +129,11 @@ struct LevelSpec {
   int emit = kEmitTable;
   int key_slot[2] = {-1, -1};           // emit keys: slots of the target index columns
   int key_arity = 2;
+  // Count mode only: also add every counted binding to grp_counts[g] for the
+  // group g with grp_bounds[g] <= (value of slot 0) < grp_bounds[g+1].
+  const uint32_t* grp_bounds = nullptr;  // n_groups + 1 sorted entries
+  uint32_t n_groups = 0;
+  unsigned long long* grp_counts = nullptr;
 };
 
 struct Table {

@@ -310,6 +310,7 @@ void Database::reset_device_state() {
     kv.second->pending_delta = false;
   }
   counts_.clear();
+  group_counts_.clear();
   kstats_.clear();
   derived_ = 0;
   for (auto& s : step_stats_) s = StepStats{};
@@ -325,6 +326,37 @@ void Database::load_rows(const std::string& name, const uint32_t* rows, uint64_t
   r.staged.insert(r.staged.end(), rows, rows + n * r.arity);
   r.pinned_valid = false;  // page-locked mirror is stale
   r.loaded = true;
+}
+
+void Database::set_count_groups(const std::string& rule, const uint32_t* bounds,
+                                uint64_t n_bounds) {
+  if (n_bounds == 0) {
+    group_bounds_.erase(rule);
+    group_counts_.erase(rule);
+    return;
+  }
+  SRDL_REQUIRE(bounds && n_bounds >= 2 && n_bounds <= (1ull << 31), kErrArg,
+               "set_count_groups: need 2 or more bounds");
+  for (uint64_t j = 0; j + 1 < n_bounds; j++)
+    SRDL_REQUIRE(bounds[j] <= bounds[j + 1], kErrArg, "set_count_groups: bounds must be non-decreasing");
+  bool known = false;
+  for (auto& st : steps_)
+    for (auto& op : st.ops)
+      if (op.kind == Op::Execute && op.rule == rule) {
+        SRDL_REQUIRE(op.count, kErrArg, "set_count_groups: rule " + rule + " is not count-only");
+        known = true;
+      }
+  SRDL_REQUIRE(known, kErrArg, "set_count_groups: unknown rule " + rule);
+  group_bounds_[rule].assign(bounds, bounds + n_bounds);
+  group_counts_.erase(rule);
+}
+
+void Database::group_counts(const std::string& rule, uint64_t* out, uint64_t n_groups) const {
+  auto it = group_bounds_.find(rule);
+  SRDL_REQUIRE(it != group_bounds_.end(), kErrArg, "group_counts: no groups set for " + rule);
+  SRDL_REQUIRE(n_groups == it->second.size() - 1, kErrArg, "group_counts: wrong group count");
+  auto c = group_counts_.find(rule);
+  for (uint64_t g = 0; g < n_groups; g++) out[g] = c == group_counts_.end() ? 0 : c->second[g];
 }
 
 void Database::clear_inputs() {

@@ -141,6 +141,10 @@ class Database {
   void load_rows(const std::string& rel, const uint32_t* rows, uint64_t n);
   void load_device_rows(const std::string& rel, const uint32_t* d_rows, uint64_t n);
   void clear_inputs();
+  // Count-only rule `rule`: also count per group of its first variable's
+  // values, [bounds[g], bounds[g+1]) (n_bounds = groups + 1; 0 clears).
+  void set_count_groups(const std::string& rule, const uint32_t* bounds, uint64_t n_bounds);
+  void group_counts(const std::string& rule, uint64_t* out, uint64_t n_groups) const;
   // counts[j] = rows of FULL(rel) whose first declared column is in
   // [bounds[j], bounds[j+1]), for j < n_bounds - 1.
   void range_counts(const std::string& rel, const uint32_t* bounds, uint64_t n_bounds,
@@ -175,6 +179,8 @@ class Database {
   std::vector<std::string> inputs_;
   std::vector<Step> steps_;
   std::map<std::string, uint64_t> counts_;
+  std::map<std::string, std::vector<uint32_t>> group_bounds_;
+  std::map<std::string, std::vector<uint64_t>> group_counts_;
   std::vector<StepStats> step_stats_;
   uint32_t dom_max_ = 0;
   int bits_ = 1;

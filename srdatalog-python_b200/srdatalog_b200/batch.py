@@ -13,7 +13,9 @@ rows whose first column lies in its range.
 
 Requirements checked here: the plan's filters use no constants (a constant
 would have to be shifted per instance), and the union's values fit in
-uint32.  Count-only rules are counted for the union as a whole.
+uint32.  Count-only rules are counted per instance too: the count of every
+binding is also added to the group of its first variable's value
+(srdl_set_count_groups), and each instance is one group.
 '''
 
 from __future__ import annotations
@@ -28,6 +30,11 @@ from .plan import parse_filter
 
 class BatchError(ValueError):
   pass
+
+
+def count_rules(plan: dict) -> list:
+  return [op['rule'] for st in plan['steps'] for op in st['ops']
+          if op['op'] == 'execute_pipeline' and op.get('count')]
 
 
 def check_batchable(plan: dict) -> None:
@@ -89,7 +96,14 @@ class BatchRun:
     self.db.clear_inputs()
     for rel, rows in self.union.inputs.items():
       self.db.load_rows(rel, rows)
+    bounds = self.union.offsets.astype(np.uint32)
+    for rule in count_rules(plan):
+      self.db.set_count_groups(rule, bounds)
     self.db.run(max_iters)
+
+  def counts(self, rule: str) -> np.ndarray:
+    '''Per-instance counts of a count-only rule.'''
+    return self.db.group_counts(rule)
 
   def sizes(self, rel: str) -> np.ndarray:
     '''Per-instance row counts of FULL(rel), computed on the device.'''

@@ -38,6 +38,8 @@ SIGNATURES = {
   'srdl_set_profiling': (ctypes.c_int, [_vp, ctypes.c_int]),
   'srdl_launch_count': (_u64, []),
   'srdl_clear_inputs': (ctypes.c_int, [_vp]),
+  'srdl_set_count_groups': (ctypes.c_int, [_vp, _cp, _u32p, _u64]),
+  'srdl_group_counts': (ctypes.c_int, [_vp, _cp, ctypes.POINTER(_u64), _u64]),
   'srdl_range_counts': (ctypes.c_int, [_vp, _cp, _u32p, _u64, ctypes.POINTER(_u64)]),
   'srdl_run': (ctypes.c_int, [_vp, _u64]),
   'srdl_size': (_u64, [_vp, _cp]),
@@ -139,6 +141,19 @@ class Database:
 
   def set_profiling(self, on: bool = True) -> None:
     check(lib().srdl_set_profiling(self._h, 1 if on else 0), 'srdl_set_profiling')
+
+  def set_count_groups(self, rule: str, bounds) -> None:
+    b = np.ascontiguousarray(bounds, dtype=np.uint32)
+    self._groups = {**getattr(self, '_groups', {}), rule: b.shape[0] - 1}
+    check(lib().srdl_set_count_groups(self._h, rule.encode(), b.ctypes.data_as(_u32p), b.shape[0]),
+          f'srdl_set_count_groups({rule})')
+
+  def group_counts(self, rule: str) -> np.ndarray:
+    n = self._groups[rule]
+    out = np.zeros(n, np.uint64)
+    check(lib().srdl_group_counts(self._h, rule.encode(), out.ctypes.data_as(ctypes.POINTER(_u64)), n),
+          f'srdl_group_counts({rule})')
+    return out
 
   def clear_inputs(self) -> None:
     check(lib().srdl_clear_inputs(self._h), 'srdl_clear_inputs')

@@ -9,8 +9,8 @@ sizes against a device-memory budget and batches them continuously.
   is idle.  A worker takes the oldest admitted request and, with it, every
   admitted request of the same program (up to `max_batch`), and evaluates
   them as one disjoint-union run (srdatalog_b200.batch): their iterations share
-  launches.  Count-only programs (the triangle count) cannot be split per
-  request after a union run and are evaluated one request per run.
+  launches; count-only programs (the triangle count) get per-request counts
+  from grouped counting.  Only small requests are unioned (see Server).
 * Workers own their database handles, so each has its own CUDA stream and
   the runs of different workers overlap on the GPU; relations stay on the
   device until the request's result (its size or count) has been read.
@@ -87,12 +87,19 @@ class Server:
 
   def __init__(self, programs: dict, device: int = 0, workers: int = 4,
                budget_bytes: int = 120 << 30, max_batch: int = 256, batching: bool = True,
-               keep_rows: bool = False):
+               keep_rows: bool = False, batch_max_edges: int = 1 << 20,
+               batch_max_span: int = 1 << 23):
     self.programs = programs
     self.device = device
     self.budget = budget_bytes
     self.max_batch = max_batch if batching else 1
     self.keep_rows = keep_rows
+    # Only small requests are unioned: their runs are dominated by per-launch
+    # and per-iteration overhead, which a union shares.  A large request runs
+    # alone (other workers proceed in parallel), and a union's value span stays
+    # small enough for the dense per-value directory.
+    self.batch_max_edges = batch_max_edges
+    self.batch_max_span = batch_max_span
     self.cv = threading.Condition()
     self.pending: list[Request] = []   # arrived, waiting for admission (FIFO)
     self.ready: list[Request] = []     # admitted, not started
@@ -160,15 +167,15 @@ class Server:
   def _take_batch(self) -> list:
     first = self.ready[0]
     spec = self.programs[first.program]
-    if spec.count_only or self.max_batch == 1:
+    if self.max_batch == 1 or _edges(first) > self.batch_max_edges:
       batch = [first]
     else:
       batch, span = [], 0
       for r in self.ready:
-        if r.program != first.program:
+        if r.program != first.program or _edges(r) > self.batch_max_edges:
           continue
         s = _span(r)
-        if batch and (len(batch) >= self.max_batch or span + s > 0xFFFFFFFF):
+        if batch and (len(batch) >= self.max_batch or span + s > self.batch_max_span):
           break
         batch.append(r)
         span += s
@@ -213,6 +220,8 @@ class Server:
     if db is None:
       db = dbs[batch[0].program] = Database(spec.plan, device=self.device)
     db.clear_inputs()
+    if spec.count_only:
+      db.set_count_groups(spec.out, [])
     if len(batch) == 1:
       r = batch[0]
       for rel, rows in r.inputs.items():
@@ -225,15 +234,22 @@ class Server:
     union = make_union([r.inputs for r in batch])
     for rel, rows in union.inputs.items():
       db.load_rows(rel, rows)
+    bounds = union.offsets.astype(np.uint32)
+    if spec.count_only:
+      db.set_count_groups(spec.out, bounds)
     db.run()
-    sizes = db.range_counts(spec.out, union.offsets.astype(np.uint32))
-    all_rows = db.dump(spec.out) if self.keep_rows else None
+    sizes = db.group_counts(spec.out) if spec.count_only else db.range_counts(spec.out, bounds)
+    all_rows = db.dump(spec.out) if self.keep_rows and not spec.count_only else None
     if all_rows is not None:
       cuts = np.searchsorted(all_rows[:, 0], union.offsets.astype(np.int64), side='left')
     for j, r in enumerate(batch):
       r.result = int(sizes[j])
       if all_rows is not None:
         r.rows = (all_rows[cuts[j]:cuts[j + 1]].astype(np.uint64) - union.offsets[j]).astype(np.uint32)
+
+
+def _edges(r: Request) -> int:
+  return sum(int(np.asarray(a).shape[0]) for a in r.inputs.values())
 
 
 def _span(r: Request) -> int:

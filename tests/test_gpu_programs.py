@@ -171,3 +171,18 @@ def test_batched_union_matches_each_instance():
       plain.load_rows('ArcInput', inst['ArcInput'])
       plain.run()
       assert plain.size('Path') == want.shape[0]
+
+
+def test_batched_triangle_counts_per_instance():
+  '''Count-only rules over a disjoint union report each instance's count
+  through grouped counting (srdl_set_count_groups).'''
+  from srdatalog_b200.batch import BatchRun
+  insts = [{'KnowsInput': W.rmat_edges(s, d, seed=40 + j)}
+           for j, (s, d) in enumerate([(8, 3000), (10, 20000), (6, 500), (12, 60000), (9, 7000)] * 4)]
+  insts.append({'KnowsInput': np.array([(i, j) for i in range(30) for j in range(i + 1, 30)],
+                                       np.uint32)})
+  br = BatchRun(load_plan('triangle'), insts)
+  counts = br.counts('TriangleJoin')
+  want = [oracle.triangle_count(i['KnowsInput']) for i in insts]
+  assert [int(c) for c in counts] == want
+  assert br.db.count('TriangleJoin') == sum(want)

@@ -32,15 +32,15 @@ def test_oversized_request_runs_alone():
   assert [r.rid for r in s.pending] == [1]
 
 
-def test_batches_group_one_program_and_keep_counts_single():
+def test_batches_group_one_program():
   s = Server(programs(), workers=0, budget_bytes=1 << 40, max_batch=3)
   for i, p in enumerate(['tc', 'triangle', 'tc', 'tc', 'tc', 'triangle']):
     s.submit(req(i, p, 1))
   b1 = s._take_batch()
   assert [r.rid for r in b1] == [0, 2, 3]         # oldest program, max_batch of it
   b2 = s._take_batch()
-  assert [r.rid for r in b2] == [1]               # count-only: one per run
-  assert [r.rid for r in s.ready] == [4, 5]
+  assert [r.rid for r in b2] == [1, 5]            # count-only rules batch too (grouped counts)
+  assert [r.rid for r in s.ready] == [4]
   plain = Server(programs(), workers=0, batching=False)
   for i in range(3):
     plain.submit(req(i, 'tc', 1))
@@ -52,3 +52,14 @@ def test_poisson_arrivals_seeded():
   assert np.all(np.diff(a) >= 0)
   assert abs(a[-1] - 2.0) < 0.3
   assert np.array_equal(a, poisson_arrivals(1000, 500.0, seed=5))
+
+
+def test_large_requests_run_alone_and_span_is_capped():
+  s = Server(programs(), workers=0, budget_bytes=1 << 40, batch_max_edges=10, batch_max_span=20)
+  big = Request(0, 'tc', {'ArcInput': np.zeros((11, 2), np.uint32)}, footprint=1)
+  s.submit(big)
+  for i in range(1, 6):
+    s.submit(Request(i, 'tc', {'ArcInput': np.array([[0, 7]], np.uint32)}, footprint=1))
+  assert [r.rid for r in s._take_batch()] == [0]          # over the edge limit: alone
+  assert [r.rid for r in s._take_batch()] == [1, 2]       # spans 8 + 8 <= 20 < 24
+  assert [r.rid for r in s._take_batch()] == [3, 4]
