@@ -175,6 +175,22 @@ class ClockSampler:
             'samples': len(sm), 'reasons': sorted(reasons)}
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+  '''The largest x over all ranks (every rank gets it); x itself on one rank.'''
+  if dist is None:
+    return x
+  import torch
+  t = torch.tensor([x], dtype=torch.float64, device=device)
+  dist.all_reduce(t, op=dist.ReduceOp.MAX)
+  return float(t.item())
+
+
+def replica_throughput(units_per_step: float, steps: int, world: int, max_ms: float) -> float:
+  '''Whole-job rate of `world` independent replicas, each doing units_per_step
+  per step for `steps` steps, timed by the slowest rank (max_ms in total).'''
+  return units_per_step * steps * world / (max_ms / 1e3)
+
+
 def hbm_peak():
   try:
     with open(PEAKS_PATH) as f:
@@ -432,11 +448,8 @@ def main():
   if dist:
     dist.barrier()
   total_ms = sum(step_ms)
-  if dist:
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
-  value = per_step * args.steps * world / (total_ms / 1e3)
+  total_ms = max_over_ranks(total_ms, dist, dev)
+  value = replica_throughput(per_step, args.steps, world, total_ms)
   stats = db.stats()
   db.close()
   del d_edges
@@ -472,10 +485,7 @@ def main():
     e2e_ms.append(ev0.elapsed_time(ev1))
     assert got == units
   e2e_total = sum(e2e_ms)
-  if dist:
-    t = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_total = float(t.item())
+  e2e_total = max_over_ranks(e2e_total, dist, dev)
   db2.close()
   plain = None
   if batched and not args.no_cpu_baseline:
@@ -513,7 +523,7 @@ def main():
     'config': {'workload': wl['desc'], 'edges': int(n), 'tuples_per_step': int(units),
                'parallelism': f'replicas{world}', 'l2': 'flushed between steps (256 MB write)',
                'inputs': 'HBM-resident for value; pinned host rows for e2e'},
-    'e2e': {'value': per_step * args.steps * world / (e2e_total / 1e3), 'unit': unit_name,
+    'e2e': {'value': replica_throughput(per_step, args.steps, world, e2e_total), 'unit': unit_name,
             'ms_per_step': e2e_total / args.steps, 'h2d_bytes_per_step': int(n) * 8,
             'd2h_bytes_per_step': 8 + (8 * per_step if batched else 0),
             'step_ms': [round(x, 3) for x in e2e_ms]},
