@@ -69,7 +69,34 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
       work[r] = 0;
       continue;
     }
-    if (lv.kind == kColumnJoin) {
+    if (lv.kind == kColumnJoin && lv.nsrc == 2) {
+      // Leapfrog seek: clip both sorted lists to their common value range
+      // [max(first), min(last)]; only that part can intersect.  The shorter
+      // clipped list drives, the other's clipped range is probed.
+      uint32_t b0, n0, b1, n1;
+      src_list(lv.src[0], in, r, b0, n0);
+      src_list(lv.src[1], in, r, b1, n1);
+      const uint32_t* v0 = lv.src[0].prefix_slot < 0 ? lv.src[0].t.roots : lv.src[0].t.lo;
+      const uint32_t* v1 = lv.src[1].prefix_slot < 0 ? lv.src[1].t.roots : lv.src[1].t.lo;
+      uint32_t e0 = b0 + n0, e1 = b1 + n1;
+      if (n0 && n1) {
+        const uint32_t lo = max(v0[b0], v1[b1]), hi = min(v0[e0 - 1], v1[e1 - 1]);
+        if (lo > hi) {
+          e0 = b0;
+        } else {
+          b0 = lower_bound_u32(v0, b0, e0, lo);
+          e0 = hi == 0xffffffffu ? e0 : lower_bound_u32(v0, b0, e0, hi + 1);
+          b1 = lower_bound_u32(v1, b1, e1, lo);
+          e1 = hi == 0xffffffffu ? e1 : lower_bound_u32(v1, b1, e1, hi + 1);
+        }
+      }
+      const uint32_t l0 = e0 - b0, l1 = e1 - b1;
+      const int bd = l1 < l0 ? 1 : 0;
+      work[r] = (l0 && l1) ? (bd ? l1 : l0) : 0;
+      drv[r] = (uint8_t)bd;
+      beg[r] = bd ? b1 : b0;
+      orange[r] = bd ? make_uint2(b0, e0) : make_uint2(b1, e1);
+    } else if (lv.kind == kColumnJoin) {
       uint32_t best = 0xffffffffu, bb = 0;
       int bd = 0;
       bool empty = false;
