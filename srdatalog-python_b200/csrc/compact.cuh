@@ -237,6 +237,7 @@ void compact_diff(const Launch& L, DedupDiffSel<K> sel, uint64_t n, uint64_t* d_
   uint8_t* flags = s.take<uint8_t>(n);
   uint32_t* counts = s.take<uint32_t>(nb);
   uint64_t* offs = s.take<uint64_t>(nb + 1);
+  prefer_shared(dd_flag_kernel<K>);
   dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, counts);
   cp_scan_kernel<<<1, 1024, 0, L.stream>>>(counts, nb, offs, d_total);
   cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, offs);

@@ -17,19 +17,34 @@ struct Launch {
   uint32_t* d_err = nullptr;  // device error word (bounded-wait failures etc.)
 };
 
-// Bump allocator over a caller-provided scratch region (256-byte aligned).
+// Bump allocator over a caller-provided scratch region.  Every piece starts
+// on a 256-byte boundary of the address space (asynchronous 16-byte copies
+// need aligned sources), whatever the alignment of the region itself.
 struct Scratch {
   char* base = nullptr;
   size_t cap = 0, used = 0;
   template <typename T>
   T* take(size_t count) {
+    const size_t pad = (256 - ((uintptr_t)(base + used) & 255)) & 255;
     size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
-    SRDL_REQUIRE(used + bytes <= cap, kErrCapacity, "scratch region too small");
-    T* p = reinterpret_cast<T*>(base + used);
-    used += bytes;
+    SRDL_REQUIRE(used + pad + bytes <= cap, kErrCapacity, "scratch region too small");
+    T* p = reinterpret_cast<T*>(base + used + pad);
+    used += pad + bytes;
     return p;
   }
 };
+
+// Ask for the largest shared-memory carveout for a kernel (once per kernel):
+// the default split caps blocks of the shared-memory-heavy kernels per SM.
+template <typename K>
+inline void prefer_shared(K* kernel) {
+  static bool done = false;
+  if (!done) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
+    done = true;
+  }
+}
 
 // Process-wide count of kernels this library has launched (bench evidence).
 void count_launches(int k);

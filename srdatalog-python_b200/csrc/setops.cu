@@ -100,6 +100,7 @@ void merge_disjoint(const Launch& L, const uint64_t* a, uint64_t na, const uint6
   if (total == 0) return;
   const uint64_t blocks = (total + kMgTile - 1) / kMgTile;
   SRDL_REQUIRE(blocks < (1ull << 31), kErrCapacity, "merge: too many rows");
+  prefer_shared(merge_kernel);
   merge_kernel<<<(unsigned)blocks, kMgThreads, 0, L.stream>>>(a, na, b, nb, out);
   SRDL_CUDA(cudaGetLastError());
   count_launches(1);

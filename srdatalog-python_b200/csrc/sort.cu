@@ -11,9 +11,10 @@
 // 2^bits on all values.  A two-column key (hi, lo) is compressed to
 // (hi << bits) | lo -- 32 bits when 2*bits <= 32 -- and sorted with
 // ceil(2*bits / 8) stable counting passes.  Each pass is a histogram launch
-// (shared-memory counters per block), one single-block scan, and a scatter
-// launch in which every warp ranks its keys with __match_any_sync, the tile
-// is staged in shared memory in digit order and written out coalesced.  No
+// (shared-memory counters per block), a per-digit scan over the blocks, and a
+// scatter launch in which every warp ranks its keys with one ballot per digit
+// bit, the tile is staged in shared memory in digit order and written out
+// coalesced.  No
 // block ever waits on another.  The dedup (and optional "not in FULL" test)
 // runs as one order-preserving compaction over the sorted keys that also
 // expands them back to (hi << 32) | lo.
@@ -107,21 +108,67 @@ __global__ void __launch_bounds__(kRsThreads) rs_rowscan(uint32_t* c, int nb,
   if (threadIdx.x == 0) digit_tot[blockIdx.x] = tot;
 }
 
+// Asynchronous 16-byte global -> shared copy (cp.async, no registers held);
+// bytes past `src_bytes` (< 16 on a ragged tail) are zero-filled.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, uint32_t src_bytes) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Issue the copy of keys [tile, min(tile + kRsTile, end)) into `buf`.  Tile
+// starts are multiples of kRsTile keys from a 256-byte aligned buffer, so
+// every 16-byte piece is aligned; a piece that straddles `end` copies only
+// the valid bytes, and pieces past it copy nothing.
 template <typename K>
+__device__ __forceinline__ void rs_prefetch(K* buf, const K* in, uint64_t tile, uint64_t end) {
+  constexpr int kPieces = kRsTile * (int)sizeof(K) / 16;
+  const uint64_t valid_bytes = (end > tile ? end - tile : 0) * sizeof(K);
+  const char* src = reinterpret_cast<const char*>(in + tile);
+  char* dst = reinterpret_cast<char*>(buf);
+  for (int p = threadIdx.x; p < kPieces; p += kRsThreads) {
+    const uint64_t off = (uint64_t)p * 16;
+    const uint64_t left = off >= valid_bytes ? 0 : valid_bytes - off;
+    const uint32_t nb = left < 16 ? (uint32_t)left : 16u;
+    cp_async16(dst + off, nb ? src + off : src, nb);
+  }
+  cp_async_commit();
+}
+
+// One counting pass over this block's chunk, a tile of kRsTile keys at a
+// time, for digits of DB bits.  The next tile is copied into the other shared
+// buffer while the current one is ranked and written, so every block keeps a
+// tile of loads in flight.  Within a warp, the lanes holding the same digit
+// are found with DB ballots (one per digit bit), which is cheaper than a
+// match instruction; the lowest such lane adds the group's size to the warp's
+// counter for the digit and passes the old value on.  The staged
+// (digit-ordered) tile reuses the buffer the current keys were read from.
+template <typename K, int DB>
 __global__ void __launch_bounds__(kRsThreads) rs_scatter(const K* __restrict__ in,
                                                          K* __restrict__ out, uint64_t n,
-                                                         uint64_t chunk, int shift, int nbins,
+                                                         uint64_t chunk, int shift,
                                                          const uint32_t* __restrict__ offs,
                                                          const uint32_t* __restrict__ digit_tot) {
-  __shared__ uint32_t base[kRsBins];             // global output position per digit
-  __shared__ uint32_t wcnt[kRsWarps][kRsBins];   // per-warp digit counts -> warp offsets
-  __shared__ uint32_t tstart[kRsBins];           // digit start inside the staged tile
-  __shared__ uint32_t tot[kRsBins];
+  constexpr int nbins = 1 << DB;
+  constexpr uint32_t mask = nbins - 1;
+  __shared__ uint32_t base[kRsBins];             // next global output position per digit
+  __shared__ uint32_t gofs[kRsBins];             // base[d] minus the digit's start in the staged tile
+  __shared__ uint32_t wofs[kRsWarps][kRsBins];   // per-warp digit counts -> staged positions
   __shared__ uint32_t scan_sh[kRsThreads / 32 + 1];
-  __shared__ K stage[kRsTile];
+  __shared__ __align__(16) K buf[2][kRsTile];
 
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const uint32_t mask = nbins - 1;
+  const uint64_t begin = (uint64_t)blockIdx.x * chunk;
+  const uint64_t end = begin + chunk < n ? begin + chunk : n;
+  if (begin < end) rs_prefetch(buf[0], in, begin, end);
   {
     // digit base = keys with a smaller digit; plus this block's offset in the digit
     const int d = threadIdx.x;  // kRsThreads == kRsBins
@@ -130,69 +177,109 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter(const K* __restrict__ i
     const uint32_t dbase = block_excl_scan(t, scan_sh, &all);
     base[d] = d < nbins ? dbase + offs[(uint64_t)d * gridDim.x + blockIdx.x] : 0;
   }
-  const uint64_t begin = (uint64_t)blockIdx.x * chunk;
-  const uint64_t end = begin + chunk < n ? begin + chunk : n;
 
-  for (uint64_t tile = begin; tile < end; tile += kRsTile) {
-    for (int d = threadIdx.x; d < kRsWarps * kRsBins; d += kRsThreads) (&wcnt[0][0])[d] = 0;
-    __syncthreads();
-    K key[kRsPerWarp / 32];
-    uint32_t rank[kRsPerWarp / 32];
-    uint32_t dig[kRsPerWarp / 32];
-    // Warp `wid` owns keys [tile + wid*256, +256) in rounds of 32, so the
-    // (round, lane) order is the input order: ranks are stable.
+  const unsigned lt = lanemask_lt();
+  int cur = 0;
+  for (uint64_t tile = begin; tile < end; tile += kRsTile, cur ^= 1) {
 #pragma unroll
-    for (int r = 0; r < kRsPerWarp / 32; r++) {
-      const uint64_t i = tile + (uint64_t)wid * kRsPerWarp + r * 32 + lane;
-      const bool valid = i < end;
-      key[r] = valid ? in[i] : K(0);
-      const uint32_t d = valid ? ((uint32_t)(key[r] >> shift) & mask) : (uint32_t)kRsBins;
-      const unsigned peers = __match_any_sync(kAllLanes, d);
-      const int leader = __ffs(peers) - 1;
-      uint32_t old = 0;
-      if (lane == leader && valid) {
-        old = wcnt[wid][d];
-        wcnt[wid][d] = old + __popc(peers);
-      }
-      old = __shfl_sync(kAllLanes, old, leader);
-      rank[r] = old + __popc(peers & lanemask_lt());
-      dig[r] = d;
-      __syncwarp();
-    }
-    __syncthreads();
-    // Per digit: exclusive prefix over warps, and the tile total.
-    {
-      const int d = threadIdx.x;  // kRsThreads == kRsBins
-      uint32_t run = 0;
-#pragma unroll
-      for (int w = 0; w < kRsWarps; w++) {
-        uint32_t c = wcnt[w][d];
-        wcnt[w][d] = run;
-        run += c;
-      }
-      tot[d] = run;
-      uint32_t all;
-      tstart[d] = block_excl_scan(run, scan_sh, &all);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < kRsPerWarp / 32; r++) {
-      if (dig[r] < (uint32_t)kRsBins) {
-        const uint32_t d = dig[r];
-        stage[tstart[d] + wcnt[wid][d] + rank[r]] = key[r];
-      }
+    for (int w = 0; w < kRsWarps; w++) wofs[w][threadIdx.x] = 0;
+    const uint64_t next = tile + kRsTile;
+    if (next < end) {
+      rs_prefetch(buf[cur ^ 1], in, next, end);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
     const uint32_t cnt = (uint32_t)((end - tile) < kRsTile ? (end - tile) : kRsTile);
-    for (uint32_t j = threadIdx.x; j < cnt; j += kRsThreads) {
-      const K k = stage[j];
-      const uint32_t d = (uint32_t)(k >> shift) & mask;
-      out[base[d] + (j - tstart[d])] = k;
+    K key[kRsPerWarp / 32];
+    uint32_t rank[kRsPerWarp / 32];
+    // Warp `wid` owns keys [wid*256, +256) of the tile in rounds of 32, so the
+    // (round, lane) order is the input order.  Each round's counter update
+    // precedes the next round's (__syncwarp orders them): ranks are stable.
+#pragma unroll
+    for (int r = 0; r < kRsPerWarp / 32; r++) {
+      const uint32_t j = (uint32_t)wid * kRsPerWarp + r * 32 + lane;
+      const bool valid = j < cnt;
+      key[r] = buf[cur][j];
+      const uint32_t d = (uint32_t)(key[r] >> shift) & mask;
+      unsigned peers = __ballot_sync(kAllLanes, valid);
+#pragma unroll
+      for (int b = 0; b < DB; b++) {
+        const bool bit = (d >> b) & 1u;
+        const unsigned m = __ballot_sync(kAllLanes, bit);
+        peers &= bit ? m : ~m;
+      }
+      // invalid lanes (a ragged last tile) get an empty group and lane 0 as leader
+      peers = valid ? peers : 0u;
+      const int leader = valid ? __ffs(peers) - 1 : 0;
+      uint32_t old = 0;
+      if (valid && lane == leader) old = atomicAdd(&wofs[wid][d], (uint32_t)__popc(peers));
+      old = __shfl_sync(kAllLanes, old, leader);
+      rank[r] = valid ? old + __popc(peers & lt) : 0xffffffffu;
+      __syncwarp();
     }
     __syncthreads();
-    base[threadIdx.x] += tot[threadIdx.x];
+    // Per digit: staged start of each warp's run (tile start of the digit plus
+    // the earlier warps' counts), and the global offset of the digit's run.
+    {
+      const int d = threadIdx.x;  // kRsThreads == kRsBins
+      uint32_t c[kRsWarps], run = 0;
+#pragma unroll
+      for (int w = 0; w < kRsWarps; w++) {
+        c[w] = wofs[w][d];
+        run += c[w];
+      }
+      uint32_t all;
+      uint32_t start = block_excl_scan(run, scan_sh, &all);
+      gofs[d] = base[d] - start;
+      base[d] += run;
+#pragma unroll
+      for (int w = 0; w < kRsWarps; w++) {
+        wofs[w][d] = start;
+        start += c[w];
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kRsPerWarp / 32; r++) {
+      if (rank[r] != 0xffffffffu) {
+        const uint32_t d = (uint32_t)(key[r] >> shift) & mask;
+        buf[cur][wofs[wid][d] + rank[r]] = key[r];
+      }
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < cnt; j += kRsThreads) {
+      const K k = buf[cur][j];
+      out[gofs[(uint32_t)(k >> shift) & mask] + j] = k;
+    }
     __syncthreads();
   }
+}
+
+template <typename K>
+static void launch_scatter(const Launch& L, int nb, int w, const K* in, K* out, uint64_t n,
+                           uint64_t chunk, int shift, const uint32_t* offs,
+                           const uint32_t* digit_tot) {
+#define SRDL_SCATTER_CASE(DB)                                                          \
+  case DB:                                                                             \
+    prefer_shared(rs_scatter<K, DB>);                                                  \
+    rs_scatter<K, DB><<<nb, kRsThreads, 0, L.stream>>>(in, out, n, chunk, shift, offs, \
+                                                       digit_tot);                     \
+    break;
+  switch (w) {
+    SRDL_SCATTER_CASE(1)
+    SRDL_SCATTER_CASE(2)
+    SRDL_SCATTER_CASE(3)
+    SRDL_SCATTER_CASE(4)
+    SRDL_SCATTER_CASE(5)
+    SRDL_SCATTER_CASE(6)
+    SRDL_SCATTER_CASE(7)
+    SRDL_SCATTER_CASE(8)
+    default:
+      throw Error{kErrState, "radix sort: digit width out of range"};
+  }
+#undef SRDL_SCATTER_CASE
 }
 
 static inline bool use32(int bits) { return 2 * bits <= 32; }
@@ -232,7 +319,7 @@ static void sort_dedup_t(const Launch& L, const uint64_t* in, uint64_t n, int bi
     const int nbins = 1 << w;
     rs_hist<K><<<nb, kRsThreads, 0, L.stream>>>(a, n, chunk, shift, nbins, counts);
     rs_rowscan<<<nbins, kRsThreads, 0, L.stream>>>(counts, nb, digit_tot);
-    rs_scatter<K><<<nb, kRsThreads, 0, L.stream>>>(a, b, n, chunk, shift, nbins, counts, digit_tot);
+    launch_scatter<K>(L, nb, w, a, b, n, chunk, shift, counts, digit_tot);
     SRDL_CUDA(cudaGetLastError());
     count_launches(3);
     std::swap(a, b);
