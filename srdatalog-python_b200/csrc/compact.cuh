@@ -1,10 +1,15 @@
 // compact.cuh -- order-preserving stream compaction in three launches.
 //
-//   1. flag   : each block owns a contiguous chunk, evaluates the selector per
-//               element, stores a flag byte and the block's selected count;
+//   1. flag   : each block owns a contiguous chunk; every warp evaluates the
+//               selector on 32 consecutive elements at a time and stores the
+//               ballot as one flag word (bit l = element 32w + l); the block's
+//               selected count goes to blk_counts;
 //   2. scan   : one block turns the per-block counts into offsets + total;
-//   3. write  : each block re-reads its flags tile by tile, block-scans them
-//               and hands every selected element its output position.
+//   3. write  : each block walks its chunk a 2048-element tile at a time;
+//               warp w takes the tile's elements [256w, 256w + 256) in eight
+//               rounds of 32, so a round's output positions are the running
+//               count plus the popcount of the lower lanes of its flag word:
+//               loads and stores are coalesced.
 // No block waits on another, so nothing can spin.  Selectors provide
 //   __device__ void block_setup(uint64_t begin, uint64_t end);  (all threads)
 //   __device__ bool select(uint64_t i);
@@ -17,6 +22,7 @@
 namespace srdl {
 
 constexpr int kCpThreads = 256;
+constexpr int kCpWarps = kCpThreads / 32;
 constexpr int kCpItems = 8;
 constexpr int kCpTile = kCpThreads * kCpItems;
 
@@ -32,22 +38,31 @@ inline int cp_blocks(uint64_t n, uint64_t chunk) {
   uint64_t nb = (n + chunk - 1) / chunk;
   return nb ? (int)nb : 1;
 }
+inline uint64_t cp_words(uint64_t n) { return (n + 31) / 32; }
 inline size_t cp_scratch_bytes(uint64_t n) {
-  // flags + per-block counts and offsets (blocks <= 8 per SM; 256 SMs bound)
-  return ((n + 255) & ~uint64_t(255)) + (size_t)(256 * 8 + 1) * 12 + 3 * 256;
+  // flag words + per-block counts and offsets (blocks <= 8 per SM; 256 SMs
+  // bound) + the FULL range of every tile boundary (set difference), each
+  // piece padded to 256 bytes, plus alignment slack for the region itself
+  const uint64_t tiles = (n + kCpTile - 1) / kCpTile + 1;
+  return ((cp_words(n) * 4 + 255) & ~uint64_t(255)) + (size_t)(256 * 8 + 1) * 12 + 3 * 256 +
+         ((tiles * 8 + 255) & ~uint64_t(255)) + 256;
 }
 
 template <class Sel>
 __global__ void __launch_bounds__(kCpThreads) cp_flag_kernel(Sel sel, uint64_t n, uint64_t chunk,
-                                                             uint8_t* flags, uint32_t* blk_counts) {
+                                                             uint32_t* flags, uint32_t* blk_counts) {
   __shared__ uint32_t sh[kCpThreads / 32 + 1];
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = begin + chunk < n ? begin + chunk : n;
+  const int lane = threadIdx.x & 31;
   sel.block_setup(begin, end);
   uint32_t cnt = 0;
-  for (uint64_t i = begin + threadIdx.x; i < end; i += kCpThreads) {
-    bool f = sel.select(i);
-    flags[i] = f ? 1 : 0;
+  // chunk starts are multiples of 32, so each round of a warp is one flag word
+  for (uint64_t w0 = begin + (threadIdx.x & ~31u); w0 < end; w0 += kCpThreads) {
+    const uint64_t i = w0 + lane;
+    const bool f = i < end && sel.select(i);
+    const uint32_t m = __ballot_sync(kAllLanes, f);
+    if (lane == 0) flags[w0 / 32] = m;
     cnt += f;
   }
   uint32_t tot;
@@ -61,34 +76,38 @@ __global__ void cp_scan_kernel(const uint32_t* blk_counts, int nb, uint64_t* off
 
 template <class Sel>
 __global__ void __launch_bounds__(kCpThreads) cp_write_kernel(Sel sel, uint64_t n, uint64_t chunk,
-                                                              const uint8_t* flags,
+                                                              const uint32_t* __restrict__ flags,
                                                               const uint64_t* offs) {
-  __shared__ uint64_t sh[kCpThreads / 32 + 1];
+  __shared__ uint32_t wtot[2][kCpWarps];
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = begin + chunk < n ? begin + chunk : n;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned lt = lanemask_lt();
   uint64_t base = offs[blockIdx.x];
-  for (uint64_t tile = begin; tile < end; tile += kCpTile) {
-    const uint64_t i0 = tile + (uint64_t)threadIdx.x * kCpItems;
-    uint8_t f[kCpItems];
-    if (i0 + kCpItems <= end) {
-      uint2 v = *reinterpret_cast<const uint2*>(flags + i0);
+  int par = 0;
+  for (uint64_t tile = begin; tile < end; tile += kCpTile, par ^= 1) {
+    // lane r < 8 fetches the flag word of round r of this warp's 256 elements
+    const uint64_t w0 = tile + (uint64_t)wid * (kCpItems * 32);
+    const uint64_t wi = w0 + (uint64_t)lane * 32;
+    const uint32_t my_word = (lane < kCpItems && wi < end) ? flags[wi / 32] : 0u;
+    const uint32_t wcount = warp_sum((uint32_t)__popc(my_word));
+    if (lane == 0) wtot[par][wid] = wcount;
+    __syncthreads();
+    uint64_t pos = base;
+    uint32_t tile_total = 0;
 #pragma unroll
-      for (int j = 0; j < 4; j++) f[j] = (v.x >> (8 * j)) & 0xff;
-#pragma unroll
-      for (int j = 0; j < 4; j++) f[4 + j] = (v.y >> (8 * j)) & 0xff;
-    } else {
-#pragma unroll
-      for (int j = 0; j < kCpItems; j++) f[j] = (i0 + j < end) ? flags[i0 + j] : 0;
+    for (int w = 0; w < kCpWarps; w++) {
+      const uint32_t c = wtot[par][w];
+      pos += w < wid ? c : 0;
+      tile_total += c;
     }
-    uint64_t c = 0;
 #pragma unroll
-    for (int j = 0; j < kCpItems; j++) c += f[j];
-    uint64_t tot;
-    uint64_t pos = base + block_excl_scan(c, sh, &tot);
-#pragma unroll
-    for (int j = 0; j < kCpItems; j++)
-      if (f[j]) sel.emit(i0 + j, pos++);
-    base += tot;
+    for (int r = 0; r < kCpItems; r++) {
+      const uint32_t m = __shfl_sync(kAllLanes, my_word, r);
+      if ((m >> lane) & 1u) sel.emit(w0 + (uint64_t)r * 32 + lane, pos + __popc(m & lt));
+      pos += __popc(m);
+    }
+    base += tile_total;
   }
 }
 
@@ -101,7 +120,7 @@ void compact(const Launch& L, Sel sel, uint64_t n, uint64_t* d_total, Scratch& s
   }
   const uint64_t chunk = cp_chunk(n, L.num_sms);
   const int nb = cp_blocks(n, chunk);
-  uint8_t* flags = s.take<uint8_t>(n);
+  uint32_t* flags = s.take<uint32_t>(cp_words(n));
   uint32_t* counts = s.take<uint32_t>(nb);
   uint64_t* offs = s.take<uint64_t>(nb + 1);
   cp_flag_kernel<Sel><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, counts);
@@ -156,62 +175,76 @@ struct DedupDiffSel {
   __device__ void emit(uint64_t i, uint64_t pos) const { out[pos] = expand(a[i]); }
 };
 
+// FULL position of every tile boundary: fpos[t] = lower_bound(FULL, first key
+// of tile t) for t < tiles, fpos[tiles] = n_full.  One warp per boundary
+// (32-ary search), all boundaries in parallel.  Tile t's keys can only match
+// FULL[fpos[t], fpos[t+1] + 1): its last key is <= the next tile's first.
+template <typename K>
+__global__ void dd_bounds_kernel(DedupDiffSel<K> sel, uint64_t n, uint64_t tiles,
+                                 uint64_t* __restrict__ fpos) {
+  const uint64_t t = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / 32;
+  if (t > tiles) return;
+  uint64_t p = sel.n_full;
+  if (t < tiles) {
+    const uint64_t first = sel.expand(sel.a[t * kCpTile]);
+    p = warp_partition_point(0, sel.n_full, [&](uint64_t i) { return sel.full[i] < first; });
+  }
+  if ((threadIdx.x & 31) == 0) fpos[t] = p;
+}
+
 // Flag pass of DedupDiffSel with FULL: the block walks its chunk one tile at
-// a time; two warps locate the tile's slice of FULL (32-ary searches), the
-// block stages the slice in shared memory when it fits, and every key is then
-// probed by binary search in shared memory instead of global memory.
+// a time, stages the tile's slice of FULL in shared memory when it fits, and
+// every key is then probed by binary search in shared memory instead of
+// global memory.
 constexpr int kDdStage = 4096;  // FULL keys staged per tile (32 KB)
 
 template <typename K>
 __global__ void __launch_bounds__(kCpThreads) dd_flag_kernel(DedupDiffSel<K> sel, uint64_t n,
-                                                             uint64_t chunk, uint8_t* flags,
+                                                             uint64_t chunk,
+                                                             const uint64_t* __restrict__ fpos,
+                                                             uint32_t* flags,
                                                              uint32_t* blk_counts) {
   __shared__ uint64_t stage[kDdStage];
-  __shared__ uint64_t rng[2];
   __shared__ uint32_t sh[kCpThreads / 32 + 1];
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = begin + chunk < n ? begin + chunk : n;
-  const int wid = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   uint32_t cnt = 0;
   for (uint64_t tile = begin; tile < end; tile += kCpTile) {
     const uint64_t tend = tile + kCpTile < end ? tile + kCpTile : end;
-    if (wid == 0) {
-      const uint64_t first = sel.expand(sel.a[tile]);
-      const uint64_t f0 = warp_partition_point(0, sel.n_full,
-                                               [&](uint64_t i) { return sel.full[i] < first; });
-      if ((threadIdx.x & 31) == 0) rng[0] = f0;
-    } else if (wid == 1) {
-      const uint64_t last = sel.expand(sel.a[tend - 1]);
-      const uint64_t f1 = warp_partition_point(0, sel.n_full,
-                                               [&](uint64_t i) { return sel.full[i] <= last; });
-      if ((threadIdx.x & 31) == 0) rng[1] = f1;
-    }
-    __syncthreads();
-    const uint64_t f0 = rng[0], f1 = rng[1];
+    const uint64_t t = tile / kCpTile;
+    const uint64_t f0 = fpos[t];
+    uint64_t f1 = fpos[t + 1] + 1;
+    f1 = f1 < sel.n_full ? f1 : sel.n_full;
     const uint64_t len = f1 > f0 ? f1 - f0 : 0;
     const bool staged = len <= (uint64_t)kDdStage;
     if (staged)
       for (uint64_t j = threadIdx.x; j < len; j += kCpThreads) stage[j] = sel.full[f0 + j];
     __syncthreads();
-    for (uint64_t i = tile + threadIdx.x; i < tend; i += kCpThreads) {
-      const K c = sel.a[i];
-      bool keep = !(sel.dedup && i > 0 && sel.a[i - 1] == c);
-      if (keep && len) {
-        const uint64_t k = sel.expand(c);
-        if (staged) {
-          uint32_t lo = 0, hi = (uint32_t)len;
-          while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (stage[mid] < k) lo = mid + 1;
-            else hi = mid;
+    for (uint64_t w0 = tile + (threadIdx.x & ~31u); w0 < tend; w0 += kCpThreads) {
+      const uint64_t i = w0 + lane;
+      bool keep = false;
+      if (i < tend) {
+        const K c = sel.a[i];
+        keep = !(sel.dedup && i > 0 && sel.a[i - 1] == c);
+        if (keep && len) {
+          const uint64_t k = sel.expand(c);
+          if (staged) {
+            uint32_t lo = 0, hi = (uint32_t)len;
+            while (lo < hi) {
+              const uint32_t mid = (lo + hi) >> 1;
+              if (stage[mid] < k) lo = mid + 1;
+              else hi = mid;
+            }
+            keep = !(lo < len && stage[lo] == k);
+          } else {
+            const uint64_t p = lower_bound_u64(sel.full, f0, f1, k);
+            keep = !(p < f1 && sel.full[p] == k);
           }
-          keep = !(lo < len && stage[lo] == k);
-        } else {
-          const uint64_t p = lower_bound_u64(sel.full, f0, f1, k);
-          keep = !(p < f1 && sel.full[p] == k);
         }
       }
-      flags[i] = keep ? 1 : 0;
+      const uint32_t m = __ballot_sync(kAllLanes, keep);
+      if (lane == 0) flags[w0 / 32] = m;
       cnt += keep;
     }
     __syncthreads();
@@ -234,15 +267,19 @@ void compact_diff(const Launch& L, DedupDiffSel<K> sel, uint64_t n, uint64_t* d_
   }
   const uint64_t chunk = cp_chunk(n, L.num_sms);
   const int nb = cp_blocks(n, chunk);
-  uint8_t* flags = s.take<uint8_t>(n);
+  const uint64_t tiles = (n + kCpTile - 1) / kCpTile;
+  uint32_t* flags = s.take<uint32_t>(cp_words(n));
   uint32_t* counts = s.take<uint32_t>(nb);
   uint64_t* offs = s.take<uint64_t>(nb + 1);
+  uint64_t* fpos = s.take<uint64_t>(tiles + 1);
   prefer_shared(dd_flag_kernel<K>);
-  dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, counts);
+  const uint64_t bthreads = (tiles + 1) * 32;
+  dd_bounds_kernel<K><<<(unsigned)((bthreads + 255) / 256), 256, 0, L.stream>>>(sel, n, tiles, fpos);
+  dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, fpos, flags, counts);
   cp_scan_kernel<<<1, 1024, 0, L.stream>>>(counts, nb, offs, d_total);
   cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, offs);
   SRDL_CUDA(cudaGetLastError());
-  count_launches(3);
+  count_launches(4);
 }
 
 // Distinct first-column values of a sorted key array.

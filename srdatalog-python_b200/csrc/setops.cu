@@ -3,10 +3,11 @@
 // merge_disjoint replaces DSAI::merge (thrust::merge + set_union on root
 // keys, RT/gpu/device_sorted_array_index.ipp:709-847): FULL and DELTA are
 // disjoint sorted arrays, so FULL U DELTA is a plain merge whose output size
-// is known up front.  Each block owns one 2048-element output tile, finds
-// its two merge-path split points by binary search, stages both input
-// slices in shared memory with coalesced loads, merges 8 outputs per thread
-// and writes the tile back coalesced.
+// is known up front.  A first launch finds the merge-path split point of
+// every 2048-element output tile (one binary search per tile boundary); then
+// each block owns one output tile, stages both input slices in shared memory
+// with coalesced loads, merges 8 outputs per thread and writes the tile back
+// coalesced.
 //
 // set_difference replaces thrust::set_difference on the zipped columns
 // (.ipp:1104-1107) and the binary-probe variant (.ipp:933-1041): every
@@ -41,57 +42,75 @@ __device__ __forceinline__ uint64_t merge_path(const uint64_t* a, uint64_t na, c
   return lo;
 }
 
-// Same split found by one whole warp (warp_partition_point): the predicate
-// a[i] <= b[diag-1-i] is true on a prefix of [max(0, diag-nb), min(diag, na)).
-__device__ __forceinline__ uint64_t merge_path_warp(const uint64_t* a, uint64_t na,
-                                                    const uint64_t* b, uint64_t nb, uint64_t diag) {
-  const uint64_t lo = diag > nb ? diag - nb : 0;
-  const uint64_t hi = diag < na ? diag : na;
-  return warp_partition_point(lo, hi, [&](uint64_t i) { return a[i] <= b[diag - 1 - i]; });
+// Split search for every output tile, one thread per tile boundary.  The
+// splits are parked in the output itself: tile t's start split goes to
+// out[t*kMgTile] and its end split to out[t*kMgTile + 1] (the last tile's end
+// split is na and is not stored).  Only tile t's block reads or writes tile
+// t's slots, and it reads them before writing its outputs, so no scratch
+// buffer is needed.
+__global__ void merge_split_kernel(const uint64_t* __restrict__ a, uint64_t na,
+                                   const uint64_t* __restrict__ b, uint64_t nb, uint64_t tiles,
+                                   uint64_t* __restrict__ out) {
+  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (t >= tiles) return;
+  const uint64_t diag = t * kMgTile;
+  const uint64_t s = merge_path(a, na, b, nb, diag);
+  out[diag] = s;
+  if (t > 0) out[diag - kMgTile + 1] = s;
 }
+
+// Shared-memory index with one pad word per 16 keys: threads that walk the
+// tile 8 (or about 4) keys apart then hit different banks.
+__device__ __forceinline__ int mg_pad(int p) { return p + (p >> 4); }
+constexpr int kMgPadded = kMgTile + kMgTile / 16;
 
 __global__ void __launch_bounds__(kMgThreads) merge_kernel(const uint64_t* __restrict__ a,
                                                            uint64_t na,
                                                            const uint64_t* __restrict__ b,
                                                            uint64_t nb,
                                                            uint64_t* __restrict__ out) {
-  __shared__ uint64_t sin[kMgTile];
-  __shared__ uint64_t sout[kMgTile];
+  __shared__ uint64_t sin[kMgPadded];
+  __shared__ uint64_t sout[kMgPadded];
   __shared__ uint64_t split[2];
   const uint64_t total = na + nb;
   const uint64_t d0 = (uint64_t)blockIdx.x * kMgTile;
   const uint64_t d1 = d0 + kMgTile < total ? d0 + kMgTile : total;
-  if (threadIdx.x < 32) {
-    const uint64_t s0 = merge_path_warp(a, na, b, nb, d0);
-    if (threadIdx.x == 0) split[0] = s0;
-  } else if (threadIdx.x < 64) {
-    const uint64_t s1 = merge_path_warp(a, na, b, nb, d1);
-    if (threadIdx.x == 32) split[1] = s1;
-  }
+  const bool last = blockIdx.x + 1 == gridDim.x;
+  if (threadIdx.x == 0) split[0] = out[d0];
+  if (threadIdx.x == 1) split[1] = last ? na : out[d0 + 1];
   __syncthreads();
   const uint64_t i0 = split[0], i1 = split[1];
   const uint64_t j0 = d0 - i0, j1 = d1 - i1;
   const int la = (int)(i1 - i0), lb = (int)(j1 - j0), lt = la + lb;
-  for (int k = threadIdx.x; k < lt; k += kMgThreads) sin[k] = k < la ? a[i0 + k] : b[j0 + k - la];
+  for (int k = threadIdx.x; k < lt; k += kMgThreads)
+    sin[mg_pad(k)] = k < la ? a[i0 + k] : b[j0 + k - la];
   __syncthreads();
   const int ld = threadIdx.x * kMgItems;
   if (ld < lt) {
     int lo = ld > lb ? ld - lb : 0, hi = ld < la ? ld : la;
     while (lo < hi) {
       int mid = (lo + hi) >> 1;
-      if (sin[mid] <= sin[la + ld - 1 - mid]) lo = mid + 1;
+      if (sin[mg_pad(mid)] <= sin[mg_pad(la + ld - 1 - mid)]) lo = mid + 1;
       else hi = mid;
     }
     int i = lo, j = ld - lo;
+    uint64_t va = i < la ? sin[mg_pad(i)] : 0, vb = j < lb ? sin[mg_pad(la + j)] : 0;
 #pragma unroll
     for (int k = 0; k < kMgItems; k++) {
       if (ld + k >= lt) break;
-      const bool take_a = (j >= lb) || (i < la && sin[i] <= sin[la + j]);
-      sout[ld + k] = take_a ? sin[i++] : sin[la + j++];
+      const bool take_a = (j >= lb) || (i < la && va <= vb);
+      sout[mg_pad(ld + k)] = take_a ? va : vb;
+      if (take_a) {
+        i++;
+        va = i < la ? sin[mg_pad(i)] : 0;
+      } else {
+        j++;
+        vb = j < lb ? sin[mg_pad(la + j)] : 0;
+      }
     }
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < lt; k += kMgThreads) out[d0 + k] = sout[k];
+  for (int k = threadIdx.x; k < lt; k += kMgThreads) out[d0 + k] = sout[mg_pad(k)];
 }
 
 void merge_disjoint(const Launch& L, const uint64_t* a, uint64_t na, const uint64_t* b,
@@ -101,9 +120,11 @@ void merge_disjoint(const Launch& L, const uint64_t* a, uint64_t na, const uint6
   const uint64_t blocks = (total + kMgTile - 1) / kMgTile;
   SRDL_REQUIRE(blocks < (1ull << 31), kErrCapacity, "merge: too many rows");
   prefer_shared(merge_kernel);
+  merge_split_kernel<<<(unsigned)((blocks + 255) / 256), 256, 0, L.stream>>>(a, na, b, nb, blocks,
+                                                                             out);
   merge_kernel<<<(unsigned)blocks, kMgThreads, 0, L.stream>>>(a, na, b, nb, out);
   SRDL_CUDA(cudaGetLastError());
-  count_launches(1);
+  count_launches(2);
 }
 
 size_t diff_scratch_bytes(uint64_t n) { return cp_scratch_bytes(n); }
