@@ -126,3 +126,39 @@ def test_merge_disjoint(na, nb):
   rng.shuffle(u)
   a, b = np.sort(u[:na]), np.sort(u[na:na + nb])
   assert np.array_equal(gpu_merge(a, b), oracle.merge(a, b))
+
+
+def test_sort_unique_many_tiles():
+  '''20M keys of 2 x 21 bits: six 7-bit passes over ~10K tiles spread over
+  every block of the grid.'''
+  rng = np.random.default_rng(11)
+  k = keys_with_bits(rng, 20_000_000, 21, dup_frac=0.1)
+  assert np.array_equal(gpu_sort_unique(k, 21), oracle.sort_unique(k))
+
+
+@pytest.mark.parametrize('bits', [15, 17])
+def test_sort_unique_multi_portion(bits):
+  '''More than 2^29 keys (32-bit and 64-bit packed forms).  The input is a
+  scrambled multiset over the values 0..m-1 (each at least once), built on
+  the device; the output must be exactly enc(0..m-1) in order, where enc
+  splits a value into (hi, lo) halves of at most `bits` bits.'''
+  lib = native.lib()
+  n = (1 << 29) + 3 * 2048 + 77
+  m = n - 1000
+  i = torch.arange(n, dtype=torch.int64, device='cuda')
+  v = (i * 2654435761) % n
+  v = torch.where(v >= m, v - m, v)              # values m..n-1 fold onto 0..999
+  lo_bits = 30 - bits                           # values < 2^30 -> both halves < 2^bits
+  enc = lambda x: ((x >> lo_bits) << 32) | (x & ((1 << lo_bits) - 1))
+  keys = enc(v)
+  del v, i
+  out = torch.empty_like(keys)
+  d_n = torch.full((1,), -1, dtype=torch.int64, device='cuda')
+  sb = lib.srdl_sort_unique_scratch_bytes(n, bits)
+  scratch = torch.empty(sb, dtype=torch.uint8, device='cuda')
+  rc = lib.srdl_sort_unique_u64(keys.data_ptr(), n, bits, out.data_ptr(), d_n.data_ptr(),
+                                scratch.data_ptr(), sb, stream())
+  assert rc == 0, native.last_error()
+  torch.cuda.synchronize()
+  assert int(d_n.item()) == m
+  assert torch.equal(out[:m], enc(torch.arange(m, dtype=torch.int64, device='cuda')))
