@@ -384,9 +384,35 @@ void Database::op_merge(const Op& op) {
   r.v[kFull].idx[op.index] = std::move(m);
 }
 
+static const char* op_kind_name(Op::Kind k) {
+  switch (k) {
+    case Op::Execute: return "execute_pipeline";
+    case Op::Rebuild: return "rebuild_index";
+    case Op::Clear: return "clear_relation";
+    case Op::CheckSize: return "check_size";
+    case Op::ComputeDelta: return "compute_delta";
+    case Op::Merge: return "merge_index";
+    case Op::RebuildFrom: return "rebuild_index_from";
+    case Op::Reconstruct: return "reconstruct";
+  }
+  return "other";
+}
+
 void Database::exec_ops(const Step& st, uint64_t it) {
   for (size_t i = 0; i < st.ops.size(); i++) {
     const Op& op = st.ops[i];
+    const auto h0 = std::chrono::steady_clock::now();
+    struct OpTimer {
+      OpStats& s;
+      std::chrono::steady_clock::time_point t0;
+      ~OpTimer() {
+        const double ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        s.ms += ms;
+        s.max_ms = ms > s.max_ms ? ms : s.max_ms;
+        s.calls++;
+      }
+    } timer{opstats_[op_kind_name(op.kind)], h0};
     switch (op.kind) {
       case Op::Execute: exec_pipeline(op, st.recursive, it); break;
       case Op::Rebuild: op_rebuild(st, i, op); break;
@@ -408,7 +434,16 @@ void Database::run(uint64_t max_iters) {
   reset_device_state();
   const uint64_t launches0 = launches_total();
   auto t0 = std::chrono::steady_clock::now();
+  opstats_.clear();
+  reset_alloc_max();
+  const AllocStats a0 = alloc_stats();
   upload_inputs();
+  {
+    OpStats& u = opstats_["upload_inputs"];
+    u.ms = u.max_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    u.calls = 1;
+  }
   for (size_t si = 0; si < steps_.size(); si++) {
     const Step& st = steps_[si];
     auto s0 = std::chrono::steady_clock::now();
@@ -439,6 +474,15 @@ void Database::run(uint64_t max_iters) {
   }
   SRDL_CUDA(cudaStreamSynchronize(L_.stream));
   run_ms_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  const AllocStats a1 = alloc_stats();
+  alloc_ = {a1.ms - a0.ms, a1.max_ms, a1.calls - a0.calls};
+  {
+    cudaMemPool_t pool;
+    uint64_t reserved = 0;
+    if (cudaDeviceGetDefaultMemPool(&pool, device_) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess)
+      pool_reserved_gb_ = reserved / 1e9;
+  }
   launches_ = launches_total() - launches0;
   prof_collect();
 }
@@ -496,6 +540,15 @@ std::string Database::stats_json() const {
       << ",\"scopes\":" << kv.second.scopes << "}";
     kfirst = false;
   }
+  o << "},\"host_ops\":{";
+  bool ofirst = true;
+  for (auto& kv : opstats_) {
+    o << (ofirst ? "" : ",") << "\"" << kv.first << "\":{\"ms\":" << kv.second.ms
+      << ",\"max_ms\":" << kv.second.max_ms << ",\"calls\":" << kv.second.calls << "}";
+    ofirst = false;
+  }
+  o << "},\"alloc\":{\"ms\":" << alloc_.ms << ",\"max_ms\":" << alloc_.max_ms
+    << ",\"calls\":" << alloc_.calls << ",\"pool_reserved_gb\":" << pool_reserved_gb_;
   o << "},\"counts\":{";
   bool first = true;
   for (auto& kv : counts_) {

@@ -1,5 +1,8 @@
 // runtime.cu -- Database: plan parsing, input staging, relation indexes.
 #include <algorithm>
+#include <atomic>
+#include <mutex>
+#include <unordered_map>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
@@ -26,8 +29,143 @@ std::vector<int> identity_perm(int arity) {
 
 // ------------------------------------------------------------------ DevBuf
 
+// Host time spent inside device allocations (process-wide), for the stats.
+static std::atomic<uint64_t> g_alloc_ns{0}, g_alloc_max_ns{0}, g_alloc_calls{0};
+
+AllocStats alloc_stats() {
+  return {g_alloc_ns.load() * 1e-6, g_alloc_max_ns.load() * 1e-6, g_alloc_calls.load()};
+}
+void reset_alloc_max() { g_alloc_max_ns.store(0); }
+
+static size_t size_class(size_t b) {
+  if (b <= 4096) return 4096;
+  const int k = 63 - __builtin_clzll((unsigned long long)b);
+  const size_t base = size_t(1) << k;
+  if (b == base) return b;
+  if (b >= (size_t(1) << 20)) return base << 1;  // 1 MB and up: powers of two
+  const size_t q = base / 4;
+  return base + ((b - base + q - 1) / q) * q;
+}
+
+// Timed driver allocation; on an out-of-memory answer every arena gives its
+// cached blocks back, the device drains, and the allocation is tried once more.
+static void release_all_arenas();
+static void* driver_alloc(size_t bytes, cudaStream_t st) {
+  const auto t0 = std::chrono::steady_clock::now();
+  void* p = nullptr;
+  cudaError_t e = cudaMallocAsync(&p, bytes, st);
+  if (e == cudaErrorMemoryAllocation) {
+    (void)cudaGetLastError();
+    release_all_arenas();
+    SRDL_CUDA(cudaDeviceSynchronize());
+    e = cudaMallocAsync(&p, bytes, st);
+  }
+  SRDL_CUDA(e);
+  const uint64_t ns = (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                          std::chrono::steady_clock::now() - t0)
+                          .count();
+  g_alloc_ns += ns;
+  g_alloc_calls++;
+  uint64_t prev = g_alloc_max_ns.load();
+  while (ns > prev && !g_alloc_max_ns.compare_exchange_weak(prev, ns)) {
+  }
+  return p;
+}
+
+class StreamArena {
+ public:
+  explicit StreamArena(cudaStream_t s) : st_(s) {}
+  // Smallest cached block of class [cls, 2*cls], else a new one of class cls;
+  // *got = the class of the block handed out.
+  void* take(size_t cls, size_t* got) {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      auto it = free_.lower_bound(cls);
+      if (it != free_.end() && it->first <= 2 * cls) {
+        void* p = it->second;
+        *got = it->first;
+        cached_ -= it->first;
+        free_.erase(it);
+        return p;
+      }
+    }
+    *got = cls;
+    return driver_alloc(cls, st_);
+  }
+  void give(void* p, size_t cls) {
+    std::lock_guard<std::mutex> g(mu_);
+    if (closed_) {
+      cudaFreeAsync(p, st_);
+      return;
+    }
+    free_.emplace(cls, p);
+    cached_ += cls;
+  }
+  // Frees every cached block (stream-ordered); with `close`, later returns
+  // are freed at once instead of cached.
+  void release(bool close) {
+    std::lock_guard<std::mutex> g(mu_);
+    for (auto& kv : free_) cudaFreeAsync(kv.second, st_);
+    free_.clear();
+    cached_ = 0;
+    if (close) closed_ = true;
+  }
+  int refs = 0;
+
+ private:
+  cudaStream_t st_;
+  std::mutex mu_;
+  std::multimap<size_t, void*> free_;
+  size_t cached_ = 0;
+  bool closed_ = false;
+};
+
+static std::mutex g_arena_mu;
+static std::unordered_map<cudaStream_t, std::shared_ptr<StreamArena>>& arenas() {
+  static auto* m = new std::unordered_map<cudaStream_t, std::shared_ptr<StreamArena>>();
+  return *m;
+}
+
+static std::shared_ptr<StreamArena> arena_for(cudaStream_t s) {
+  std::lock_guard<std::mutex> g(g_arena_mu);
+  auto it = arenas().find(s);
+  return it == arenas().end() ? nullptr : it->second;
+}
+
+void arena_attach(cudaStream_t s) {
+  std::lock_guard<std::mutex> g(g_arena_mu);
+  auto& a = arenas()[s];
+  if (!a) a = std::make_shared<StreamArena>(s);
+  a->refs++;
+}
+
+void arena_detach(cudaStream_t s) {
+  std::shared_ptr<StreamArena> a;
+  {
+    std::lock_guard<std::mutex> g(g_arena_mu);
+    auto it = arenas().find(s);
+    if (it == arenas().end()) return;
+    if (--it->second->refs > 0) return;
+    a = it->second;
+    arenas().erase(it);
+  }
+  a->release(true);
+}
+
+static void release_all_arenas() {
+  std::vector<std::shared_ptr<StreamArena>> all;
+  {
+    std::lock_guard<std::mutex> g(g_arena_mu);
+    for (auto& kv : arenas()) all.push_back(kv.second);
+  }
+  for (auto& a : all) a->release(false);
+}
+
 DevBuf::DevBuf(size_t bytes, cudaStream_t st) : bytes_(bytes), st_(st) {
-  if (bytes) SRDL_CUDA(cudaMallocAsync(&p_, (bytes + 255) & ~size_t(255), st));
+  if (!bytes) return;
+  arena_ = arena_for(st);
+  if (arena_) p_ = arena_->take(size_class(bytes), &cls_);
+  else p_ = driver_alloc((bytes + 255) & ~size_t(255), st);
 }
 
 DevBuf& DevBuf::operator=(DevBuf&& o) noexcept {
@@ -36,6 +174,8 @@ DevBuf& DevBuf::operator=(DevBuf&& o) noexcept {
     p_ = o.p_;
     bytes_ = o.bytes_;
     st_ = o.st_;
+    arena_ = std::move(o.arena_);
+    cls_ = o.cls_;
     o.p_ = nullptr;
     o.bytes_ = 0;
   }
@@ -43,7 +183,11 @@ DevBuf& DevBuf::operator=(DevBuf&& o) noexcept {
 }
 
 void DevBuf::reset() {
-  if (p_) cudaFreeAsync(p_, st_);
+  if (p_) {
+    if (arena_) arena_->give(p_, cls_);
+    else cudaFreeAsync(p_, st_);
+  }
+  arena_.reset();
   p_ = nullptr;
   bytes_ = 0;
 }
@@ -78,6 +222,7 @@ Database::~Database() {
     for (auto& kv : rels_) kv.second->pending = Index{};
     for (auto& kv : rels_) kv.second->dstaged.reset();
     d_small_.reset();
+    arena_detach(L_.stream);
     cudaStreamSynchronize(L_.stream);
     if (h_small_) cudaFreeHost(h_small_);
     for (auto& kv : rels_)
@@ -215,6 +360,7 @@ void Database::init_device() {
   SRDL_CUDA(cudaDeviceGetDefaultMemPool(&pool, device_));
   uint64_t thr = ~0ull;
   SRDL_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  arena_attach(L_.stream);
   SRDL_CUDA(cudaMallocHost(&h_small_, kSmallSlots * sizeof(uint64_t)));
   d_small_ = DevBuf(kSmallSlots * sizeof(uint64_t), L_.stream);
   dev_ready_ = true;
@@ -237,6 +383,7 @@ void Database::set_stream(cudaStream_t s) {
   // Release everything allocated on the old stream before switching.
   SRDL_CUDA(cudaStreamSynchronize(L_.stream));
   reset_device_state();
+  arena_attach(s);
   for (auto& kv : rels_) {
     if (kv.second->dstaged_n) SRDL_CUDA(cudaStreamSynchronize(L_.stream));
   }
@@ -252,6 +399,8 @@ void Database::set_stream(cudaStream_t s) {
     r.dstaged = std::move(nb);
   }
   d_small_ = std::move(keep_small);
+  SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  arena_detach(L_.stream);
   SRDL_CUDA(cudaStreamSynchronize(L_.stream));
   if (own_stream_) SRDL_CUDA(cudaStreamDestroy(L_.stream));
   L_.stream = s;
