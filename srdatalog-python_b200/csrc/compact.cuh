@@ -41,11 +41,12 @@ inline int cp_blocks(uint64_t n, uint64_t chunk) {
 inline uint64_t cp_words(uint64_t n) { return (n + 31) / 32; }
 inline size_t cp_scratch_bytes(uint64_t n) {
   // flag words + per-block counts and offsets (blocks <= 8 per SM; 256 SMs
-  // bound) + the FULL range of every tile boundary (set difference), each
-  // piece padded to 256 bytes, plus alignment slack for the region itself
+  // bound) + the FULL and HEAD positions of every tile boundary (set
+  // difference), each piece padded to 256 bytes, plus alignment slack for the
+  // region itself
   const uint64_t tiles = (n + kCpTile - 1) / kCpTile + 1;
   return ((cp_words(n) * 4 + 255) & ~uint64_t(255)) + (size_t)(256 * 8 + 1) * 12 + 3 * 256 +
-         ((tiles * 8 + 255) & ~uint64_t(255)) + 256;
+         2 * ((tiles * 8 + 255) & ~uint64_t(255)) + 256;
 }
 
 template <class Sel>
@@ -131,8 +132,9 @@ void compact(const Launch& L, Sel sel, uint64_t n, uint64_t* d_total, Scratch& s
 }
 
 // Keeps a[i] when it differs from a[i-1] (optional) and is absent from the
-// sorted unique array full[0..n_full).  Keys are stored compressed as
-// (hi << bits) | lo and are expanded to (hi << 32) | lo on output.
+// sorted unique arrays full[0..n_full) and head[0..n_head) (a Device2Level
+// relation's two segments; head may be empty).  Keys are stored compressed
+// as (hi << bits) | lo and are expanded to (hi << 32) | lo on output.
 template <typename K>
 struct DedupDiffSel {
   const K* a;
@@ -141,6 +143,8 @@ struct DedupDiffSel {
   const uint64_t* full;
   uint64_t n_full;
   uint64_t* out;
+  const uint64_t* head = nullptr;
+  uint64_t n_head = 0;
 
   __device__ __forceinline__ uint64_t expand(K c) const {
     if (sizeof(K) == 8 && bits == 32) return (uint64_t)c;
@@ -179,17 +183,23 @@ struct DedupDiffSel {
 // of tile t) for t < tiles, fpos[tiles] = n_full.  One warp per boundary
 // (32-ary search), all boundaries in parallel.  Tile t's keys can only match
 // FULL[fpos[t], fpos[t+1] + 1): its last key is <= the next tile's first.
+// hpos (when a HEAD is given) holds the same positions in HEAD.
 template <typename K>
 __global__ void dd_bounds_kernel(DedupDiffSel<K> sel, uint64_t n, uint64_t tiles,
-                                 uint64_t* __restrict__ fpos) {
+                                 uint64_t* __restrict__ fpos, uint64_t* __restrict__ hpos) {
   const uint64_t t = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / 32;
   if (t > tiles) return;
-  uint64_t p = sel.n_full;
+  uint64_t p = sel.n_full, q = sel.n_head;
   if (t < tiles) {
     const uint64_t first = sel.expand(sel.a[t * kCpTile]);
     p = warp_partition_point(0, sel.n_full, [&](uint64_t i) { return sel.full[i] < first; });
+    if (hpos)
+      q = warp_partition_point(0, sel.n_head, [&](uint64_t i) { return sel.head[i] < first; });
   }
-  if ((threadIdx.x & 31) == 0) fpos[t] = p;
+  if ((threadIdx.x & 31) == 0) {
+    fpos[t] = p;
+    if (hpos) hpos[t] = q;
+  }
 }
 
 // Flag pass of DedupDiffSel with FULL: the block walks its chunk one tile at
@@ -202,6 +212,7 @@ template <typename K>
 __global__ void __launch_bounds__(kCpThreads) dd_flag_kernel(DedupDiffSel<K> sel, uint64_t n,
                                                              uint64_t chunk,
                                                              const uint64_t* __restrict__ fpos,
+                                                             const uint64_t* __restrict__ hpos,
                                                              uint32_t* flags,
                                                              uint32_t* blk_counts) {
   __shared__ uint64_t stage[kDdStage];
@@ -218,6 +229,12 @@ __global__ void __launch_bounds__(kCpThreads) dd_flag_kernel(DedupDiffSel<K> sel
     f1 = f1 < sel.n_full ? f1 : sel.n_full;
     const uint64_t len = f1 > f0 ? f1 - f0 : 0;
     const bool staged = len <= (uint64_t)kDdStage;
+    uint64_t h0 = 0, h1 = 0;
+    if (hpos) {
+      h0 = hpos[t];
+      h1 = hpos[t + 1] + 1;
+      h1 = h1 < sel.n_head ? h1 : sel.n_head;
+    }
     if (staged)
       for (uint64_t j = threadIdx.x; j < len; j += kCpThreads) stage[j] = sel.full[f0 + j];
     __syncthreads();
@@ -242,6 +259,11 @@ __global__ void __launch_bounds__(kCpThreads) dd_flag_kernel(DedupDiffSel<K> sel
             keep = !(p < f1 && sel.full[p] == k);
           }
         }
+        if (keep && h1 > h0) {
+          const uint64_t k = sel.expand(c);
+          const uint64_t p = lower_bound_u64(sel.head, h0, h1, k);
+          keep = !(p < h1 && sel.head[p] == k);
+        }
       }
       const uint32_t m = __ballot_sync(kAllLanes, keep);
       if (lane == 0) flags[w0 / 32] = m;
@@ -257,10 +279,15 @@ __global__ void __launch_bounds__(kCpThreads) dd_flag_kernel(DedupDiffSel<K> sel
 // compact() for DedupDiffSel with a FULL array: tiled, shared-memory probes.
 template <typename K>
 void compact_diff(const Launch& L, DedupDiffSel<K> sel, uint64_t n, uint64_t* d_total, Scratch& s) {
-  if (!sel.full || sel.n_full == 0) {
+  if (!sel.head || sel.n_head == 0) {
+    sel.head = nullptr;
+    sel.n_head = 0;
+  }
+  if ((!sel.full || sel.n_full == 0) && !sel.head) {
     compact(L, sel, n, d_total, s);
     return;
   }
+  if (!sel.full) sel.n_full = 0;
   if (n == 0) {
     SRDL_CUDA(cudaMemsetAsync(d_total, 0, sizeof(uint64_t), L.stream));
     return;
@@ -272,10 +299,12 @@ void compact_diff(const Launch& L, DedupDiffSel<K> sel, uint64_t n, uint64_t* d_
   uint32_t* counts = s.take<uint32_t>(nb);
   uint64_t* offs = s.take<uint64_t>(nb + 1);
   uint64_t* fpos = s.take<uint64_t>(tiles + 1);
+  uint64_t* hpos = sel.head ? s.take<uint64_t>(tiles + 1) : nullptr;
   prefer_shared(dd_flag_kernel<K>);
   const uint64_t bthreads = (tiles + 1) * 32;
-  dd_bounds_kernel<K><<<(unsigned)((bthreads + 255) / 256), 256, 0, L.stream>>>(sel, n, tiles, fpos);
-  dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, fpos, flags, counts);
+  dd_bounds_kernel<K><<<(unsigned)((bthreads + 255) / 256), 256, 0, L.stream>>>(sel, n, tiles, fpos,
+                                                                                hpos);
+  dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, fpos, hpos, flags, counts);
   cp_scan_kernel<<<1, 1024, 0, L.stream>>>(counts, nb, offs, d_total);
   cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, offs);
   SRDL_CUDA(cudaGetLastError());

@@ -304,8 +304,10 @@ void Database::op_rebuild(const Step& st, size_t pos, const Op& op) {
   }
   if (fuse) {
     const Index* full = nullptr;
-    if (r.v[kFull].has_index()) full = &ensure_index(r, kFull, op.index);
-    sort_into(r.pending, in ? in : nullptr, total, false, full);
+    if (r.v[kFull].has_index())
+      full = r.lsm ? &full_base(r, op.index) : &ensure_index(r, kFull, op.index);
+    const Index* head = r.lsm && op.index == r.canonical && r.head.n ? &r.head : nullptr;
+    sort_into(r.pending, in ? in : nullptr, total, false, full, head);
     r.pending_delta = true;
     rv.chunks.clear();
     rv.idx.clear();
@@ -341,7 +343,7 @@ void Database::op_compute_delta(const Op& op) {
     d.n = nw.n;
     return;
   }
-  Index& f = ensure_index(r, kFull, op.index);
+  Index& f = r.lsm ? full_base(r, op.index) : ensure_index(r, kFull, op.index);
   DevBuf scratch(diff_scratch_bytes(nw.n) + 1024, L_.stream);
   Scratch s{scratch.as<char>(), scratch.bytes(), 0};
   size_t pid = prof_begin("set_difference");
@@ -349,6 +351,7 @@ void Database::op_compute_delta(const Op& op) {
                  d_small_.as<uint64_t>(), s);
   d.n = read_scalar(0);
   prof_end(pid, 8.0 * (nw.n + f.n + d.n), (double)nw.n);
+  if (r.lsm) subtract_head(r, op.index, d);
 }
 
 void Database::op_merge(const Op& op) {
@@ -373,6 +376,34 @@ void Database::op_merge(const Op& op) {
     return;
   }
   if (dn == 0) return;
+  if (r.lsm) {
+    if (op.index != r.canonical) {
+      // Only the canonical permutation has a HEAD; this one is rebuilt from it.
+      r.v[kFull].idx.erase(op.index);
+      return;
+    }
+    // DELTA goes into HEAD (O(|HEAD| + |DELTA|)); HEAD is merged into FULL
+    // once it holds more than a tenth of FULL (device_2level_index.h:291-318).
+    Index& f = full_base(r, op.index);
+    const uint64_t fn = f.n;
+    for (auto it2 = r.v[kFull].idx.begin(); it2 != r.v[kFull].idx.end();)
+      it2 = it2->first == r.canonical ? std::next(it2) : r.v[kFull].idx.erase(it2);
+    Index& h = r.head;
+    Index m;
+    m.n = h.n + dn;
+    m.keys = DevBuf(m.n * 8, L_.stream);
+    size_t pid = prof_begin("merge");
+    if (h.n)
+      merge_disjoint(L_, h.keys.as<uint64_t>(), h.n, d->keys.as<uint64_t>(), dn,
+                     m.keys.as<uint64_t>());
+    else
+      SRDL_CUDA(cudaMemcpyAsync(m.keys.as<uint64_t>(), d->keys.as<uint64_t>(), dn * 8,
+                                cudaMemcpyDeviceToDevice, L_.stream));
+    prof_end(pid, 16.0 * m.n, (double)m.n);
+    h = std::move(m);
+    if (h.n * 10 > fn) compact_head(r);
+    return;
+  }
   Index& f = ensure_index(r, kFull, op.index);
   Index m;
   m.n = f.n + dn;
@@ -467,6 +498,9 @@ void Database::run(uint64_t max_iters) {
         exec_ops(st, it);
         step_stats_[si].iterations++;
       }
+      // Post-stratum reconstruct: every LSM relation ends as one FULL array.
+      for (auto& kv : rels_)
+        if (kv.second->head.n) compact_head(*kv.second);
     }
     SRDL_CUDA(cudaStreamSynchronize(L_.stream));
     step_stats_[si].ms =
@@ -489,6 +523,7 @@ void Database::run(uint64_t max_iters) {
 
 uint64_t Database::size(const std::string& name) {
   Relation& r = rel(name);
+  if (r.head.n) compact_head(r);
   auto& fv = r.v[kFull];
   auto it = fv.idx.find(r.canonical);
   if (it != fv.idx.end()) return it->second.n;

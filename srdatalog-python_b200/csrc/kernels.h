@@ -64,11 +64,12 @@ size_t sort_scratch_bytes(uint64_t n, int dom_bits);
 // swapped first when `swap` is set) and writes the distinct keys, in
 // ascending order, into `out`.  When `full` is given, keys present in the
 // sorted unique array full[0..n_full) are dropped as well (fused
-// DELTA = unique(NEW) - FULL).  The output count goes to *d_nout.
-// `out` needs room for n keys and may alias `in`.
+// DELTA = unique(NEW) - FULL); so are keys present in head[0..n_head) (the
+// HEAD segment of a Device2LevelIndex FULL).  The output count goes to
+// *d_nout.  `out` needs room for n keys and may alias `in`.
 void sort_dedup(const Launch& L, const uint64_t* in, uint64_t n, int dom_bits, bool swap,
                 const uint64_t* full, uint64_t n_full, uint64_t* out, uint64_t* d_nout,
-                Scratch& s);
+                Scratch& s, const uint64_t* head = nullptr, uint64_t n_head = 0);
 
 // ------------------------------------------------------------- set ops
 size_t diff_scratch_bytes(uint64_t n);

@@ -248,6 +248,7 @@ void Database::parse_plan(const std::string& plan_json) {
     rel->input_file = r.at("input_file").s();
     rel->print_size = r.at("print_size").flag();
     rel->index_type = r.at("index_type").s();
+    rel->lsm = rel->index_type.find("Device2LevelIndex") != std::string::npos;
     rel->canonical = r.at("canonical").ints();
     SRDL_REQUIRE((int)rel->canonical.size() == rel->arity, kErrPlan,
                  "plan: canonical index arity mismatch for " + rel->name);
@@ -457,6 +458,7 @@ void Database::reset_device_state() {
     for (auto& v : kv.second->v) v.clear();
     kv.second->pending = Index{};
     kv.second->pending_delta = false;
+    kv.second->head = Index{};
   }
   counts_.clear();
   group_counts_.clear();
@@ -566,7 +568,8 @@ void Database::load_device_rows(const std::string& name, const uint32_t* d_rows,
 
 // Sorted unique keys of `in` (packed in some order) into `out`, optionally
 // dropping keys present in `full`.
-void Database::sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full) {
+void Database::sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full,
+                         const Index* head) {
   out.keys = DevBuf(std::max<uint64_t>(n, 1) * 8, L_.stream);
   out.trie = false;
   if (n == 0) {
@@ -575,10 +578,12 @@ void Database::sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, 
   }
   DevBuf scratch(sort_scratch_bytes(n, bits_), L_.stream);
   Scratch s{scratch.as<char>(), scratch.bytes(), 0};
-  const bool diff = full && full->n;
+  const bool hd = head && head->n;
+  const bool diff = (full && full->n) || hd;
   size_t pid = prof_begin(diff ? "sort_dedup_diff" : "sort_dedup");
-  sort_dedup(L_, in, n, bits_, swap, diff ? full->keys.as<uint64_t>() : nullptr,
-             full ? full->n : 0, out.keys.as<uint64_t>(), d_small_.as<uint64_t>(), s);
+  sort_dedup(L_, in, n, bits_, swap, full && full->n ? full->keys.as<uint64_t>() : nullptr,
+             full ? full->n : 0, out.keys.as<uint64_t>(), d_small_.as<uint64_t>(), s,
+             hd ? head->keys.as<uint64_t>() : nullptr, hd ? head->n : 0);
   prof_end(pid, 0, (double)n);
   out.n = read_scalar(0);
   if (pid != (size_t)-1) {
@@ -650,8 +655,45 @@ void Database::upload_inputs() {
 
 // ------------------------------------------------------------------ indexes
 
+Index& Database::full_base(Relation& r, const std::vector<int>& perm) {
+  auto it = r.v[kFull].idx.find(perm);
+  if (it != r.v[kFull].idx.end()) return it->second;
+  return ensure_index(r, kFull, perm);
+}
+
+void Database::compact_head(Relation& r) {
+  if (r.head.n == 0) return;
+  Index h = std::move(r.head);
+  r.head = Index{};
+  Index& f = full_base(r, r.canonical);
+  Index m;
+  m.n = f.n + h.n;
+  m.keys = DevBuf(m.n * 8, L_.stream);
+  size_t pid = prof_begin("merge");
+  merge_disjoint(L_, f.keys.as<uint64_t>(), f.n, h.keys.as<uint64_t>(), h.n, m.keys.as<uint64_t>());
+  prof_end(pid, 16.0 * m.n, (double)m.n);
+  r.v[kFull].idx.clear();
+  r.v[kFull].idx[r.canonical] = std::move(m);
+}
+
+void Database::subtract_head(Relation& r, const std::vector<int>& perm, Index& d) {
+  if (r.head.n == 0 || d.n == 0 || perm != r.canonical) return;
+  Index& h = r.head;
+  Index out;
+  out.keys = DevBuf(d.n * 8, L_.stream);
+  DevBuf scratch(diff_scratch_bytes(d.n) + 1024, L_.stream);
+  Scratch s{scratch.as<char>(), scratch.bytes(), 0};
+  size_t pid = prof_begin("set_difference");
+  set_difference(L_, d.keys.as<uint64_t>(), d.n, h.keys.as<uint64_t>(), h.n,
+                 out.keys.as<uint64_t>(), d_small_.as<uint64_t>(), s);
+  out.n = read_scalar(0);
+  prof_end(pid, 8.0 * (d.n + h.n + out.n), (double)d.n);
+  d = std::move(out);
+}
+
 Index& Database::ensure_index(Relation& r, Ver v, const std::vector<int>& perm) {
   SRDL_REQUIRE((int)perm.size() == r.arity, kErrPlan, "index arity mismatch on " + r.name);
+  if (v == kFull && r.head.n) compact_head(r);
   RelVersion& rv = r.v[v];
   auto it = rv.idx.find(perm);
   if (it != rv.idx.end()) return it->second;

@@ -104,6 +104,15 @@ struct Relation {
   bool loaded = false;
   bool pending_delta = false;    // NEW was sorted straight into a delta
   Index pending;
+  // Device2LevelIndex policy (index_type): FULL in the canonical permutation
+  // is kept as a large sorted segment (v[kFull]) plus a small sorted HEAD that
+  // receives each iteration's DELTA; HEAD is merged into FULL when it passes a
+  // tenth of FULL, at the end of the stratum, or before any read that wants
+  // FULL as one array (every such read goes through ensure_index).  FULL's
+  // other permutations are dropped whenever HEAD changes and are rebuilt from
+  // the merged canonical array on demand.
+  bool lsm = false;
+  Index head;
 };
 
 // Plan-level descriptions (parsed once from JSON).
@@ -244,10 +253,17 @@ class Database {
   void upload_inputs();
   uint64_t read_scalar(int slot);
   Index& ensure_index(Relation& r, Ver v, const std::vector<int>& perm);
+  // FULL's large segment in `perm` without merging HEAD into it.
+  Index& full_base(Relation& r, const std::vector<int>& perm);
+  // Merges r's HEAD into canonical FULL (drops FULL's other permutations).
+  void compact_head(Relation& r);
+  // d <- d - HEAD when d is in the canonical permutation of an LSM relation.
+  void subtract_head(Relation& r, const std::vector<int>& perm, Index& d);
   void ensure_trie(Relation& r, Index& ix);
   TrieView view(Relation& r, Index& ix);
   void ensure_hash(Index& ix);
-  void sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full);
+  void sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full,
+                 const Index* head = nullptr);
   void exec_ops(const Step& st, uint64_t iteration);
   void exec_pipeline(const Op& op, bool recursive, uint64_t iteration);
   void op_rebuild(const Step& st, size_t pos, const Op& op);

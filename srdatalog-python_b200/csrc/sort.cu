@@ -293,7 +293,7 @@ size_t sort_scratch_bytes(uint64_t n, int bits) {
 template <typename K>
 static void sort_dedup_t(const Launch& L, const uint64_t* in, uint64_t n, int bits, bool swap,
                          const uint64_t* full, uint64_t n_full, uint64_t* out,
-                         uint64_t* d_nout, Scratch& s) {
+                         uint64_t* d_nout, Scratch& s, const uint64_t* head, uint64_t n_head) {
   SRDL_REQUIRE(n < (1ull << 32), kErrCapacity, "sort: more than 2^32-1 rows in one index");
   K* a = s.take<K>(n);
   K* b = s.take<K>(n);
@@ -325,19 +325,20 @@ static void sort_dedup_t(const Launch& L, const uint64_t* in, uint64_t n, int bi
     std::swap(a, b);
     shift += w;
   }
-  DedupDiffSel<K> sel{a, bits, true, full, n_full, out};
+  DedupDiffSel<K> sel{a, bits, true, full, n_full, out, head, n_head};
   compact_diff(L, sel, n, d_nout, s);
 }
 
 void sort_dedup(const Launch& L, const uint64_t* in, uint64_t n, int bits, bool swap,
                 const uint64_t* full, uint64_t n_full, uint64_t* out, uint64_t* d_nout,
-                Scratch& s) {
+                Scratch& s, const uint64_t* head, uint64_t n_head) {
   if (n == 0) {
     SRDL_CUDA(cudaMemsetAsync(d_nout, 0, sizeof(uint64_t), L.stream));
     return;
   }
-  if (use32(bits)) sort_dedup_t<uint32_t>(L, in, n, bits, swap, full, n_full, out, d_nout, s);
-  else sort_dedup_t<uint64_t>(L, in, n, bits, swap, full, n_full, out, d_nout, s);
+  if (use32(bits))
+    sort_dedup_t<uint32_t>(L, in, n, bits, swap, full, n_full, out, d_nout, s, head, n_head);
+  else sort_dedup_t<uint64_t>(L, in, n, bits, swap, full, n_full, out, d_nout, s, head, n_head);
 }
 
 }  // namespace srdl
