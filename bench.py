@@ -45,10 +45,10 @@ WORKLOADS = {
   'sg': dict(plan='sg', rel='Arc', out='Sg', kind='size',
              desc='same generation, windowed forest n=10,000 (parent in [i-1000,i-1]) '
                   '+ 10% cross edges, seed 2'),
-  'batched': dict(plan='tc', rel='ArcInput', out='Path', kind='batched',
+  'batched': dict(plan='tc_lsm', rel='ArcInput', out='Path', kind='batched',
                   desc='4,096 independent TC instances, directed Erdos-Renyi, n log-uniform in '
                        '[64, 1024], mean out-degree U[2,8], seed 1000+j; evaluated as one '
-                       'disjoint union'),
+                       'disjoint union; Path declared Device2LevelIndex'),
 }
 
 BATCH_COUNT = 4096
@@ -314,7 +314,7 @@ def run_served(args, rank, world):
   from srdatalog_b200.serve import ProgramSpec, Server, poisson_arrivals, replay
   if world > 1 and rank != 0:
     return
-  progs = {'tc': ProgramSpec(load_plan('tc'), 'Path'), 'sg': ProgramSpec(load_plan('sg'), 'Sg'),
+  progs = {'tc': ProgramSpec(load_plan('tc_lsm'), 'Path'), 'sg': ProgramSpec(load_plan('sg'), 'Sg'),
            'triangle': ProgramSpec(load_plan('triangle'), 'TriangleJoin', count_only=True)}
   pool = serve_pool()
   rate = args.rate

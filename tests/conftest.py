@@ -22,7 +22,7 @@ def load_plan(name: str) -> dict:
 
 @pytest.fixture(scope='session')
 def plans():
-  return {n: load_plan(n) for n in ('tc', 'sg', 'triangle', 'tc_left')}
+  return {n: load_plan(n) for n in ('tc', 'sg', 'triangle', 'tc_left', 'tc_lsm')}
 
 
 @pytest.fixture(scope='session')

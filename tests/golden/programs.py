@@ -57,6 +57,21 @@ def triangle_program() -> Program:
   ])
 
 
+def tc_lsm_program() -> Program:
+  '''TC with the Device2LevelIndex hint on Path (the index-policy hook of
+  the DSL, examples/sg.py:30): same MIR as tc, FULL kept as HEAD + FULL.'''
+  arc = Relation('ArcInput', 2, column_types=(int, int), input_file='Arc.csv')
+  edge = Relation('Edge', 2, column_types=(int, int))
+  path = Relation('Path', 2, column_types=(int, int), print_size=True,
+                  index_type='SRDatalog::GPU::Device2LevelIndex')
+  x, y, z = Var('x'), Var('y'), Var('z')
+  return Program(rules=[
+    (edge(x, y) <= arc(x, y)).named('EdgeLoad'),
+    (path(x, y) <= edge(x, y)).named('TCBase'),
+    (path(x, z) <= path(x, y) & edge(y, z)).named('TCRec'),
+  ])
+
+
 def tc_left_program() -> Program:
   '''Left-recursive TC variant (Path(x,z) <= Edge(x,y), Path(y,z)): a second
   join shape whose delta index is (0,1); no reference fixture pins it.'''
@@ -77,4 +92,5 @@ PROGRAMS = {
   'sg': (sg_program, 'SgPlan', 'integration/sg.mir.sexpr'),
   'triangle': (triangle_program, 'TrianglePlan', 'integration/lsqb_triangle_count.mir.sexpr'),
   'tc_left': (tc_left_program, 'TcLeftPlan', None),
+  'tc_lsm': (tc_lsm_program, 'TcPlan', 'tc.mir.sexpr'),
 }

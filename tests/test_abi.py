@@ -30,7 +30,7 @@ def test_library_exports_every_header_symbol():
   assert lib.srdl_version() == 1
 
 
-@pytest.mark.parametrize('name', ['tc', 'sg', 'triangle', 'tc_left'])
+@pytest.mark.parametrize('name', ['tc', 'sg', 'triangle', 'tc_left', 'tc_lsm'])
 def test_open_committed_plans(name):
   db = native.Database(load_plan(name))
   db.close()

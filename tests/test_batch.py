@@ -16,7 +16,7 @@ def test_union_offsets_and_relabel():
 
 
 def test_plans_with_variable_filters_batch():
-  for name in ('tc', 'sg', 'triangle', 'tc_left'):
+  for name in ('tc', 'sg', 'triangle', 'tc_left', 'tc_lsm'):
     check_batchable(load_plan(name))
 
 

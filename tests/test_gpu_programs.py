@@ -149,7 +149,8 @@ def test_triangle_large_ids_sparse_path():
   assert db2.count('TriangleJoin') == db.count('TriangleJoin')
 
 
-def test_batched_union_matches_each_instance():
+@pytest.mark.parametrize('plan_name', ['tc', 'tc_lsm'])
+def test_batched_union_matches_each_instance(plan_name):
   '''Independent TC instances evaluated as one disjoint union give each
   instance exactly its own closure (checked against the oracle per instance,
   and against the one-at-a-time loop through the same library).'''
@@ -157,7 +158,7 @@ def test_batched_union_matches_each_instance():
   insts = [{'ArcInput': W.er_instance(n, c, seed=500 + j)}
            for j, (n, c) in enumerate([(16, 2.0), (40, 3.5), (120, 1.5), (200, 2.5), (64, 8.0),
                                        (3, 1.0), (90, 2.2), (150, 4.0)] * 6)]
-  br = BatchRun(load_plan('tc'), insts)
+  br = BatchRun(load_plan(plan_name), insts)
   per = br.split_rows('Path')
   sizes = br.sizes('Path')
   plain = native.Database(load_plan('tc'))
