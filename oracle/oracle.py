@@ -294,3 +294,61 @@ def run_plan(plan: dict, inputs: dict, max_iters: int = 0):
       run_ops(ops, it)
   out = {n: sorted(db[(n, 'FULL')]) for n in rels}
   return out, counts
+
+
+def _by_first(rel: set) -> dict:
+  out: dict = {}
+  for a, b in rel:
+    out.setdefault(a, set()).add(b)
+  return out
+
+
+def andersen(inputs: dict) -> list:
+  '''PointsTo of examples/andersen.py:60-97 by naive iteration over Python
+  sets (rules Base, Assign, Load, Store), independent of any plan.'''
+  pts = set(map(tuple, np.asarray(inputs['AddressOf']).tolist()))
+  assign = list(map(tuple, np.asarray(inputs['Assign']).tolist()))
+  load = list(map(tuple, np.asarray(inputs['Load']).tolist()))
+  store = list(map(tuple, np.asarray(inputs['Store']).tolist()))
+  while True:
+    by = _by_first(pts)
+    new = set()
+    for y, z in assign:                       # PointsTo(y,x) <= PointsTo(z,x), Assign(y,z)
+      for x in by.get(z, ()):
+        new.add((y, x))
+    for y, x in load:                         # PointsTo(y,w) <= PointsTo(x,z), Load(y,x), PointsTo(z,w)
+      for z in by.get(x, ()):
+        for w in by.get(z, ()):
+          new.add((y, w))
+    for y, x in store:                        # PointsTo(z,w) <= PointsTo(y,z), Store(y,x), PointsTo(x,w)
+      for z in by.get(y, ()):
+        for w in by.get(x, ()):
+          new.add((z, w))
+    if new <= pts:
+      return sorted(pts)
+    pts |= new
+
+
+def cspa(inputs: dict) -> dict:
+  '''ValueFlow / ValueAlias / MemoryAlias of examples/cspa.py:75-108 by naive
+  iteration over Python sets, independent of any plan.'''
+  assign = set(map(tuple, np.asarray(inputs['AssignInput']).tolist()))
+  deref = set(map(tuple, np.asarray(inputs['DerefInput']).tolist()))
+  vf = set(assign)                                              # VF_Assign
+  vf |= {(x, x) for x, _ in assign} | {(x, x) for _, x in assign}   # VF_Refl1/2
+  ma = {(x, x) for _, x in assign} | {(x, x) for x, _ in assign}    # MA_Refl1/2
+  va: set = set()
+  while True:
+    vf_by, ma_by, va_by, de_by = _by_first(vf), _by_first(ma), _by_first(va), _by_first(deref)
+    n_vf = {(x, y) for x, z in vf for y in vf_by.get(z, ())}            # VF_Trans
+    n_vf |= {(x, y) for x, z in assign for y in ma_by.get(z, ())}       # VF_Assign_MA
+    n_va = {(x, y) for z, xs in vf_by.items() for x in xs for y in xs}  # VA_VF
+    n_va |= {(x, y) for z, xs in vf_by.items() for w in ma_by.get(z, ())
+             for x in xs for y in vf_by.get(w, ())}                      # VA_VF_MA_VF
+    n_ma = {(x, w) for y, xs in de_by.items() for z in va_by.get(y, ())
+            for x in xs for w in de_by.get(z, ())}                       # MA_Deref_VA
+    if n_vf <= vf and n_va <= va and n_ma <= ma:
+      return {'ValueFlow': sorted(vf), 'ValueAlias': sorted(va), 'MemoryAlias': sorted(ma)}
+    vf |= n_vf
+    va |= n_va
+    ma |= n_ma

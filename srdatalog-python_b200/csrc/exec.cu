@@ -425,6 +425,7 @@ static const char* op_kind_name(Op::Kind k) {
     case Op::Merge: return "merge_index";
     case Op::RebuildFrom: return "rebuild_index_from";
     case Op::Reconstruct: return "reconstruct";
+    case Op::Hook: return "inject_cpp_hook";
   }
   return "other";
 }
@@ -456,6 +457,7 @@ void Database::exec_ops(const Step& st, uint64_t it) {
       case Op::Merge: op_merge(op); break;
       case Op::RebuildFrom: ensure_index(rel(op.rel), op.ver, op.index); break;
       case Op::Reconstruct: break;
+      case Op::Hook: break;
     }
   }
 }

@@ -297,6 +297,8 @@ void Database::parse_plan(const std::string& plan_json) {
             SRDL_REQUIRE(rels_.count(s.rel), kErrPlan, "plan: unknown relation " + s.rel);
           op.pipeline.push_back(std::move(po));
         }
+      } else if (k == "inject_cpp_hook") {
+        op.kind = Op::Hook;
       } else {
         op.rel = oj.at("rel").s();
         SRDL_REQUIRE(rels_.count(op.rel), kErrPlan, "plan: unknown relation " + op.rel);

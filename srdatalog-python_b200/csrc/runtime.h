@@ -135,7 +135,9 @@ struct PipeOp {
 };
 
 struct Op {
-  enum Kind { Execute, Rebuild, Clear, CheckSize, ComputeDelta, Merge, RebuildFrom, Reconstruct } kind;
+  // Hook: an injected C++ hook of the reference (mir/types.py:358), kept in
+  // the plan and skipped (there is no C++ code generation here).
+  enum Kind { Execute, Rebuild, Clear, CheckSize, ComputeDelta, Merge, RebuildFrom, Reconstruct, Hook } kind;
   std::string rel, rule;
   Ver ver = kFull;
   std::vector<int> index, source_index;

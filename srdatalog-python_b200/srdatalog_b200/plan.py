@@ -25,6 +25,7 @@ filter, insert_into.
 from __future__ import annotations
 
 import json
+import warnings
 from typing import Any
 
 PLAN_VERSION = 1
@@ -100,17 +101,34 @@ def _instr(node: Any) -> dict:
   if kind == 'PostStratumReconstructInternCols':
     return {'op': 'post_stratum_reconstruct', 'rel': node.rel_name,
             'index': [int(c) for c in node.canonical_index]}
+  if kind == 'InjectCppHook':
+    # Raw C++ pasted into the generated step (mir/types.py:358).  There is no
+    # C++ code generation here, so the hook is kept in the plan for the record
+    # and skipped by the runtime; the reference's own hooks only print sizes.
+    warnings.warn(f'rule {node.rule_name}: injected C++ hook is not executed by this runtime',
+                  stacklevel=3)
+    return {'op': 'inject_cpp_hook', 'rule': node.rule_name, 'code': node.code}
   raise PlanError(f'MIR instruction {kind} is not supported by this runtime')
+
+
+def _instrs(nodes: Any) -> list:
+  '''Instructions in order; a ParallelGroup's independent ops (mir/types.py:351)
+  run one after the other, which is one of the orders they may run in.'''
+  out = []
+  for n in nodes:
+    if type(n).__name__ == 'ParallelGroup':
+      out += _instrs(n.ops)
+    else:
+      out.append(_instr(n))
+  return out
 
 
 def _step(plan: Any, recursive: bool) -> dict:
   kind = type(plan).__name__
-  if kind == 'FixpointPlan':
-    ops = [_instr(i) for i in plan.instructions]
-  elif kind == 'Block':
-    ops = [_instr(i) for i in plan.instructions]
+  if kind in ('FixpointPlan', 'Block'):
+    ops = _instrs(plan.instructions)
   else:
-    ops = [_instr(plan)]
+    ops = _instrs([plan])
   return {'recursive': bool(recursive), 'ops': ops}
 
 
@@ -195,6 +213,8 @@ def validate_plan(plan: dict) -> None:
   arity = {r['name']: r['arity'] for r in plan['relations']}
   for st in plan['steps']:
     for op in st['ops']:
+      if op['op'] == 'inject_cpp_hook':
+        continue
       if op['op'] != 'execute_pipeline':
         if op['rel'] not in arity:
           raise PlanError(f'unknown relation {op["rel"]}')

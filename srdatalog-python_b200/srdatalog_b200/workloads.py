@@ -148,3 +148,27 @@ def served_request_input(program: str, m: int, seed: int) -> dict:
 def write_csv(edges: np.ndarray, path: str, delimiter: str = '\t') -> None:
   '''Write an edge list as the reference's loader reads it (one row per line).'''
   np.savetxt(path, edges.astype(np.int64), fmt='%d', delimiter=delimiter)
+
+
+def _pairs(rng: np.random.Generator, n_vars: int, m: int) -> np.ndarray:
+  s = rng.integers(0, n_vars, m, dtype=np.uint32)
+  d = rng.integers(0, n_vars, m, dtype=np.uint32)
+  return _dedup_in_order(s, d)
+
+
+def andersen_inputs(n_vars: int, m: int, seed: int) -> dict:
+  '''Inputs of the Andersen program (examples/andersen.py): AddressOf,
+  Assign, Load and Store facts over `n_vars` variables, about m/4 each,
+  drawn uniformly and deduplicated.'''
+  rng = _rng(seed)
+  q = max(1, m // 4)
+  return {'AddressOf': _pairs(rng, n_vars, q), 'Assign': _pairs(rng, n_vars, q),
+          'Load': _pairs(rng, n_vars, q), 'Store': _pairs(rng, n_vars, q)}
+
+
+def cspa_inputs(n_vars: int, m: int, seed: int) -> dict:
+  '''Inputs of the CSPA program (examples/cspa.py): AssignInput (3/4 of m)
+  and DerefInput (1/4) over `n_vars` variables, uniform, deduplicated.'''
+  rng = _rng(seed)
+  return {'AssignInput': _pairs(rng, n_vars, max(1, 3 * m // 4)),
+          'DerefInput': _pairs(rng, n_vars, max(1, m // 4))}

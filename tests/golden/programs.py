@@ -86,6 +86,68 @@ def tc_left_program() -> Program:
   ])
 
 
+def _bin(name: str, input_file: str | None = None, print_size: bool = False) -> Relation:
+  kw = {'column_types': (int, int), 'print_size': print_size}
+  if input_file:
+    kw['input_file'] = input_file
+  return Relation(name, 2, **kw)
+
+
+def andersen_program() -> Program:
+  '''Andersen points-to analysis (examples/andersen.py): two non-linear
+  rules (Load, Store) with per-delta variable orders, a parallel group of
+  five pipelines per iteration, and an injected C++ hook on Store.'''
+  address_of = _bin('AddressOf', 'addressOf.csv')
+  assign = _bin('Assign', 'assign.csv')
+  load = _bin('Load', 'load.csv')
+  store = _bin('Store', 'store.csv')
+  points_to = _bin('PointsTo', print_size=True)
+  w, x, y, z = Var('w'), Var('x'), Var('y'), Var('z')
+  return Program(rules=[
+    (points_to(y, x) <= address_of(y, x)).named('Base').with_plan(var_order=['y', 'x']),
+    (points_to(y, x) <= points_to(z, x) & assign(y, z))
+    .named('Assign').with_plan(var_order=['z', 'x', 'y']),
+    (points_to(y, w) <= points_to(x, z) & load(y, x) & points_to(z, w))
+    .named('Load')
+    .with_plan(delta=0, var_order=['x', 'z', 'y', 'w'])
+    .with_plan(delta=2, var_order=['z', 'x', 'y', 'w']),
+    (points_to(z, w) <= points_to(y, z) & store(y, x) & points_to(x, w))
+    .named('Store')
+    .with_plan(delta=0, var_order=['y', 'x', 'z', 'w'])
+    .with_plan(delta=2, var_order=['x', 'y', 'w', 'z'])
+    .with_inject_cpp('// report PointsTo delta / full sizes'),
+  ])
+
+
+def cspa_program() -> Program:
+  '''Context-sensitive points-to (examples/cspa.py): five mutually recursive
+  binary relations, anonymous variables, three-atom joins.'''
+  assign_in = Relation('AssignInput', 2, input_file='Assign.csv')
+  deref_in = Relation('DerefInput', 2, input_file='Dereference.csv')
+  assign, deref = Relation('Assign', 2), Relation('Deref', 2)
+  vf = Relation('ValueFlow', 2, print_size=True)
+  va = Relation('ValueAlias', 2, print_size=True)
+  ma = Relation('MemoryAlias', 2, print_size=True)
+  w, x, y, z = Var('w'), Var('x'), Var('y'), Var('z')
+  return Program(rules=[
+    (assign(x, y) <= assign_in(x, y)).named('LoadAssign'),
+    (deref(x, y) <= deref_in(x, y)).named('LoadDeref'),
+    (vf(y, x) <= assign(y, x)).named('VF_Assign'),
+    (vf(x, x) <= assign(x, Var('_'))).named('VF_Refl1'),
+    (vf(x, x) <= assign(Var('_'), x)).named('VF_Refl2'),
+    (ma(x, x) <= assign(Var('_'), x)).named('MA_Refl1'),
+    (ma(x, x) <= assign(x, Var('_'))).named('MA_Refl2'),
+    (vf(x, y) <= vf(x, z) & vf(z, y)).named('VF_Trans').with_plan(var_order=['z', 'x', 'y']),
+    (vf(x, y) <= assign(x, z) & ma(z, y))
+    .named('VF_Assign_MA').with_plan(var_order=['z', 'x', 'y']),
+    (va(x, y) <= vf(z, x) & vf(z, y)).named('VA_VF').with_plan(var_order=['z', 'x', 'y']),
+    (va(x, y) <= vf(z, x) & ma(z, w) & vf(w, y))
+    .named('VA_VF_MA_VF').with_plan(var_order=['z', 'w', 'x', 'y']),
+    (ma(x, w) <= deref(y, x) & va(y, z) & deref(z, w))
+    .named('MA_Deref_VA').with_plan(var_order=['y', 'z', 'x', 'w']),
+  ])
+
+
 # name -> (builder, project name, reference MIR fixture or None)
 PROGRAMS = {
   'tc': (tc_program, 'TcPlan', 'tc.mir.sexpr'),
@@ -93,4 +155,6 @@ PROGRAMS = {
   'triangle': (triangle_program, 'TrianglePlan', 'integration/lsqb_triangle_count.mir.sexpr'),
   'tc_left': (tc_left_program, 'TcLeftPlan', None),
   'tc_lsm': (tc_lsm_program, 'TcPlan', 'tc.mir.sexpr'),
+  'andersen': (andersen_program, 'AndersenPlan', 'integration/andersen.mir.sexpr'),
+  'cspa': (cspa_program, 'CspaPlan', 'integration/cspa.mir.sexpr'),
 }

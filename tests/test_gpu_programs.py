@@ -232,3 +232,33 @@ def test_sg_two_level_vs_single_array(expected):
   a.run()
   assert a.size('Sg') == expected['sg_2k']['size']
   assert oracle.dump_hash(a.dump('Sg')) == expected['sg_2k']['sha256']
+
+
+@pytest.mark.parametrize('n,m,seed', [(50, 140, 0), (300, 700, 1), (1000, 1600, 2)])
+def test_andersen_vs_rules(n, m, seed):
+  '''Andersen points-to (non-linear Load/Store rules with per-delta orders, a
+  parallel group, an injected hook) against the naive rule restatement.'''
+  inp = W.andersen_inputs(n, m, seed)
+  db = native.Database(load_plan('andersen'))
+  for rel, rows in inp.items():
+    db.load_rows(rel, rows)
+  db.run()
+  want = np.array(oracle.andersen(inp), np.uint32).reshape(-1, 2)
+  assert db.size('PointsTo') == want.shape[0]
+  assert oracle.dump_hash(db.dump('PointsTo')) == oracle.dump_hash(want)
+
+
+@pytest.mark.parametrize('n,m,seed', [(40, 90, 0), (150, 260, 1), (300, 380, 2)])
+def test_cspa_vs_rules(n, m, seed):
+  '''CSPA (five mutually recursive relations, anonymous variables) against the
+  naive rule restatement.'''
+  inp = W.cspa_inputs(n, m, seed)
+  db = native.Database(load_plan('cspa'))
+  for rel, rows in inp.items():
+    db.load_rows(rel, rows)
+  db.run()
+  want = oracle.cspa(inp)
+  for rel in ('ValueFlow', 'ValueAlias', 'MemoryAlias'):
+    w = np.array(want[rel], np.uint32).reshape(-1, 2)
+    assert db.size(rel) == w.shape[0], rel
+    assert oracle.dump_hash(db.dump(rel)) == oracle.dump_hash(w), rel
