@@ -83,6 +83,19 @@ __device__ __forceinline__ uint64_t lower_bound_u64(const uint64_t* a, uint64_t 
   return lo;
 }
 
+// lower_bound in [lo, hi) for a key known to be >= a[lo - 1]'s key: gallop
+// forward from lo (1, 2, 4, ... steps), then binary-search the last gap.
+__device__ __forceinline__ uint64_t gallop_lower_bound_u64(const uint64_t* a, uint64_t lo,
+                                                           uint64_t hi, uint64_t key) {
+  uint64_t step = 1, prev = lo;
+  while (lo < hi && a[lo] < key) {
+    prev = lo + 1;
+    lo = lo + step < hi ? lo + step : hi;
+    step <<= 1;
+  }
+  return lower_bound_u64(a, prev, lo, key);
+}
+
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t lo,
                                                     uint32_t hi, uint32_t key) {
   while (lo < hi) {

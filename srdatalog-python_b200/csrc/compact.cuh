@@ -44,9 +44,11 @@ inline size_t cp_scratch_bytes(uint64_t n) {
   // bound) + the FULL and HEAD positions of every tile boundary (set
   // difference), each piece padded to 256 bytes, plus alignment slack for the
   // region itself
+  // (+ the merge-path cuts: FULL at most 16 times the keys on that path)
   const uint64_t tiles = (n + kCpTile - 1) / kCpTile + 1;
+  const uint64_t mtiles = (17 * n + kCpTile - 1) / kCpTile + 2;
   return ((cp_words(n) * 4 + 255) & ~uint64_t(255)) + (size_t)(256 * 8 + 1) * 12 + 3 * 256 +
-         2 * ((tiles * 8 + 255) & ~uint64_t(255)) + 256;
+         2 * ((tiles * 8 + 255) & ~uint64_t(255)) + 2 * ((mtiles * 8 + 255) & ~uint64_t(255)) + 256;
 }
 
 template <class Sel>
@@ -208,8 +210,9 @@ __global__ void dd_bounds_kernel(DedupDiffSel<K> sel, uint64_t n, uint64_t tiles
 // binary-searches the slice for its first key only and walks forward from
 // there for the other seven (both runs are sorted), so a key costs about one
 // comparison instead of a dozen.  The eight flag bits of four neighbouring
-// threads form one 32-key flag word.  Slices that do not fit, and the HEAD
-// segment, are probed by binary search in global memory within the tile's
+// threads form one 32-key flag word.  Slices that do not fit are searched in
+// global memory, each key galloping forward from the previous key's
+// position; the HEAD segment is probed by binary search within the tile's
 // range.
 constexpr int kDdStage = 4000;  // FULL keys staged per tile (31.25 KB: with 64-bit tile keys under 48 KB)
 
@@ -242,14 +245,43 @@ __global__ void __launch_bounds__(kCpThreads) dd_flag_kernel(DedupDiffSel<K> sel
       h1 = hpos[t + 1] + 1;
       h1 = h1 < sel.n_head ? h1 : sel.n_head;
     }
-    if (staged)
-      for (uint32_t j = threadIdx.x; j < len; j += kCpThreads) stage[j] = sel.full[f0 + j];
-    for (uint32_t j = threadIdx.x; j < tn; j += kCpThreads) skey[j + 1] = sel.a[tile + j];
-    if (threadIdx.x == 0) skey[0] = tile > 0 ? sel.a[tile - 1] : K(0);
+    // Staging: every thread issues all of its loads before its first shared
+    // store, so a tile costs one or two memory round trips, not one per load.
+    {
+      K kr[kCpItems];
+#pragma unroll
+      for (int q = 0; q < kCpItems; q++) {
+        const uint32_t j = threadIdx.x + q * kCpThreads;
+        kr[q] = j < tn ? sel.a[tile + j] : K(0);
+      }
+      const K prev = (threadIdx.x == 0 && tile > 0) ? sel.a[tile - 1] : K(0);
+      if (staged) {
+        for (uint32_t b0 = 0; b0 < len; b0 += kCpThreads * kCpItems) {
+          uint64_t fr[kCpItems];
+#pragma unroll
+          for (int q = 0; q < kCpItems; q++) {
+            const uint32_t j = b0 + threadIdx.x + q * kCpThreads;
+            fr[q] = j < len ? sel.full[f0 + j] : 0;
+          }
+#pragma unroll
+          for (int q = 0; q < kCpItems; q++) {
+            const uint32_t j = b0 + threadIdx.x + q * kCpThreads;
+            if (j < len) stage[j] = fr[q];
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kCpItems; q++) {
+        const uint32_t j = threadIdx.x + q * kCpThreads;
+        if (j < tn) skey[j + 1] = kr[q];
+      }
+      if (threadIdx.x == 0) skey[0] = prev;
+    }
     __syncthreads();
     uint32_t bits = 0;
     if (j0 < tn) {
       uint32_t p = 0;
+      uint64_t g = f0;  // unstaged slice: this thread's position in FULL
       if (staged && len) {
         const uint64_t k0 = sel.expand(skey[j0 + 1]);
         uint32_t lo = 0, hi = len;
@@ -272,7 +304,8 @@ __global__ void __launch_bounds__(kCpThreads) dd_flag_kernel(DedupDiffSel<K> sel
             while (p < len && stage[p] < k) p++;
             keep = !(p < len && stage[p] == k);
           } else {
-            const uint64_t g = lower_bound_u64(sel.full, f0, f1, k);
+            g = q == 0 ? lower_bound_u64(sel.full, f0, f1, k)
+                       : gallop_lower_bound_u64(sel.full, g, f1, k);
             keep = !(g < f1 && sel.full[g] == k);
           }
         }
@@ -297,7 +330,191 @@ __global__ void __launch_bounds__(kCpThreads) dd_flag_kernel(DedupDiffSel<K> sel
   if (threadIdx.x == 0) blk_counts[blockIdx.x] = tot;
 }
 
-// compact() for DedupDiffSel with a FULL array: tiled, shared-memory probes.
+// ---- merge-path flag pass (FULL streamed once) ------------------------------
+//
+// The keys a (sorted, possibly repeating) and FULL (sorted, unique) are
+// merged, FULL first on equal values, and the merged sequence is cut into
+// tiles of kCpTile elements (one thread per tile boundary finds the cut by
+// merge-path binary search, and the tile's start in HEAD).  Persistent blocks
+// walk the tiles; the next tile's two slices are copied into the second
+// shared buffer with cp.async while the current tile is merged, 8 merged
+// elements per thread.  An a-key is kept iff it differs from the last FULL
+// key taken at or before it (so it is not in FULL) and from the a-key before
+// it (dedup); HEAD, when present, is probed per kept key within the tile's
+// HEAD range.  Bits are OR-ed into the flag words (a tile's a-range does not
+// start on a word boundary).
+
+// Number of a-keys among the first `diag` merged elements.
+template <typename K>
+__device__ __forceinline__ uint64_t dm_path(const DedupDiffSel<K>& sel, uint64_t na,
+                                            uint64_t diag) {
+  uint64_t lo = diag > sel.n_full ? diag - sel.n_full : 0;
+  uint64_t hi = diag < na ? diag : na;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (sel.expand(sel.a[mid]) < sel.full[diag - 1 - mid]) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// split[t] = a-keys among the first t*kCpTile merged elements; hpos[t] = the
+// HEAD position of a[split[t]] (n_head past the last key).
+template <typename K>
+__global__ void dm_split_kernel(DedupDiffSel<K> sel, uint64_t na, uint64_t tiles,
+                                uint64_t* __restrict__ split, uint64_t* __restrict__ hpos) {
+  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (t > tiles) return;
+  const uint64_t total = na + sel.n_full;
+  const uint64_t diag = t * kCpTile < total ? t * kCpTile : total;
+  const uint64_t i = dm_path(sel, na, diag);
+  split[t] = i;
+  if (hpos)
+    hpos[t] = i < na ? lower_bound_u64(sel.head, 0, sel.n_head, sel.expand(sel.a[i])) : sel.n_head;
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_small(void* smem, const void* gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES)
+               : "memory");
+}
+
+// One merged tile's slices: la a-keys (K) at the start of the buffer, lf FULL
+// keys after them at an 8-byte boundary; returns nothing, commits one group.
+template <typename K>
+__device__ __forceinline__ void dm_fetch(const DedupDiffSel<K>& sel, unsigned char* buf,
+                                         uint64_t i0, uint32_t la, uint64_t j0, uint32_t lf) {
+  K* da = reinterpret_cast<K*>(buf);
+  uint64_t* df = reinterpret_cast<uint64_t*>(buf + ((la * sizeof(K) + 7) & ~size_t(7)));
+  for (uint32_t k = threadIdx.x; k < la; k += kCpThreads) cp_async_small<sizeof(K)>(da + k, sel.a + i0 + k);
+  for (uint32_t k = threadIdx.x; k < lf; k += kCpThreads) cp_async_small<8>(df + k, sel.full + j0 + k);
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kCpThreads) dm_mark_kernel(DedupDiffSel<K> sel, uint64_t na,
+                                                             uint64_t tiles,
+                                                             const uint64_t* __restrict__ split,
+                                                             const uint64_t* __restrict__ hpos,
+                                                             uint32_t* __restrict__ flags) {
+  __shared__ __align__(16) unsigned char buf[2][kCpTile * 8];
+  __shared__ uint32_t sbits[kCpTile / 32 + 2];
+  const uint64_t total = na + sel.n_full;
+  auto bounds = [&](uint64_t t, uint64_t& i0, uint64_t& i1, uint64_t& j0, uint64_t& j1) {
+    const uint64_t d0 = t * kCpTile;
+    const uint64_t d1 = d0 + kCpTile < total ? d0 + kCpTile : total;
+    i0 = split[t];
+    i1 = split[t + 1];
+    j0 = d0 - i0;
+    j1 = d1 - i1;
+  };
+  uint64_t t = blockIdx.x;
+  if (t >= tiles) return;
+  uint64_t i0, i1, j0, j1;
+  bounds(t, i0, i1, j0, j1);
+  dm_fetch(sel, buf[0], i0, (uint32_t)(i1 - i0), j0, (uint32_t)(j1 - j0));
+  int cur = 0;
+  for (;;) {
+    const uint64_t tn = t + gridDim.x;
+    uint64_t ni0 = 0, ni1 = 0, nj0 = 0, nj1 = 0;
+    if (tn < tiles) {
+      bounds(tn, ni0, ni1, nj0, nj1);
+      dm_fetch(sel, buf[cur ^ 1], ni0, (uint32_t)(ni1 - ni0), nj0, (uint32_t)(nj1 - nj0));
+    }
+    const uint32_t la = (uint32_t)(i1 - i0), lf = (uint32_t)(j1 - j0);
+    const uint64_t w0 = i0 / 32;
+    const uint32_t nwords = la ? (uint32_t)((i1 - 1) / 32 - w0 + 1) : 0;
+    for (uint32_t k = threadIdx.x; k < nwords; k += kCpThreads) sbits[k] = 0;
+    // values just before the tile (for the first element of thread 0's run)
+    const uint64_t edge_a = i0 > 0 ? sel.expand(sel.a[i0 - 1]) : 0;
+    const uint64_t edge_f = j0 > 0 ? sel.full[j0 - 1] : 0;
+    uint64_t h0 = 0, h1 = 0;
+    if (hpos) {
+      h0 = hpos[t];
+      h1 = hpos[t + 1] + 1;
+      h1 = h1 < sel.n_head ? h1 : sel.n_head;
+    }
+    if (tn < tiles) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    const K* sa = reinterpret_cast<const K*>(buf[cur]);
+    const uint64_t* sf =
+        reinterpret_cast<const uint64_t*>(buf[cur] + ((la * sizeof(K) + 7) & ~size_t(7)));
+    const uint32_t diag = threadIdx.x * kCpItems;
+    if (diag < la + lf && la) {
+      uint32_t lo = diag > lf ? diag - lf : 0, hi = diag < la ? diag : la;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (sel.expand(sa[mid]) < sf[diag - 1 - mid]) lo = mid + 1;
+        else hi = mid;
+      }
+      uint32_t ia = lo, jf = diag - lo;
+      bool has_f = jf > 0 || j0 > 0;
+      uint64_t last_f = jf > 0 ? sf[jf - 1] : edge_f;
+      bool has_p = ia > 0 || i0 > 0;
+      uint64_t prev = ia > 0 ? sel.expand(sa[ia - 1]) : edge_a;
+      // this thread's a-keys are consecutive: their bits fit two flag words
+      const uint64_t wbase = (i0 + ia) / 32;
+      uint64_t mask = 0;
+#pragma unroll
+      for (int q = 0; q < kCpItems; q++) {
+        if (ia + jf >= la + lf) break;
+        const uint64_t x = ia < la ? sel.expand(sa[ia]) : 0;
+        const bool take_a = jf >= lf || (ia < la && x < sf[jf]);
+        if (!take_a) {
+          last_f = sf[jf++];
+          has_f = true;
+          continue;
+        }
+        bool keep = !(has_f && last_f == x) && !(sel.dedup && has_p && prev == x);
+        if (keep && h1 > h0) {
+          const uint64_t g = lower_bound_u64(sel.head, h0, h1, x);
+          keep = !(g < h1 && sel.head[g] == x);
+        }
+        if (keep) mask |= 1ull << (i0 + ia - wbase * 32);
+        prev = x;
+        has_p = true;
+        ia++;
+      }
+      if ((uint32_t)mask) atomicOr(&sbits[wbase - w0], (uint32_t)mask);
+      if (mask >> 32) atomicOr(&sbits[wbase + 1 - w0], (uint32_t)(mask >> 32));
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < nwords; k += kCpThreads)
+      if (sbits[k]) atomicOr(&flags[w0 + k], sbits[k]);
+    __syncthreads();
+    if (tn >= tiles) break;
+    t = tn;
+    i0 = ni0;
+    i1 = ni1;
+    j0 = nj0;
+    j1 = nj1;
+    cur ^= 1;
+  }
+}
+
+// Per-block selected counts of a flag-word array (blocks own `chunk` keys).
+static __global__ void __launch_bounds__(kCpThreads) cp_count_kernel(const uint32_t* __restrict__ flags,
+                                                              uint64_t n, uint64_t chunk,
+                                                              uint32_t* blk_counts) {
+  __shared__ uint32_t sh[kCpThreads / 32 + 1];
+  const uint64_t begin = (uint64_t)blockIdx.x * chunk;
+  const uint64_t end = begin + chunk < n ? begin + chunk : n;
+  uint32_t c = 0;
+  for (uint64_t w = begin / 32 + threadIdx.x; w < (end + 31) / 32; w += kCpThreads)
+    c += __popc(flags[w]);
+  uint32_t tot;
+  block_excl_scan(c, sh, &tot);
+  if (threadIdx.x == 0) blk_counts[blockIdx.x] = tot;
+}
+
+// The merge-path pass streams all of FULL; past this ratio the per-tile
+// probes of dd_flag_kernel read less.
+constexpr uint64_t kDmMaxFullRatio = 16;
+
+// compact() for DedupDiffSel with a FULL array: merge path when FULL is not
+// much larger than the keys, tiled shared-memory probes otherwise.
 template <typename K>
 void compact_diff(const Launch& L, DedupDiffSel<K> sel, uint64_t n, uint64_t* d_total, Scratch& s) {
   if (!sel.head || sel.n_head == 0) {
@@ -319,6 +536,23 @@ void compact_diff(const Launch& L, DedupDiffSel<K> sel, uint64_t n, uint64_t* d_
   uint32_t* flags = s.take<uint32_t>(cp_words(n));
   uint32_t* counts = s.take<uint32_t>(nb);
   uint64_t* offs = s.take<uint64_t>(nb + 1);
+  if (sel.n_full <= kDmMaxFullRatio * n) {
+    const uint64_t mtiles = (n + sel.n_full + kCpTile - 1) / kCpTile;
+    SRDL_REQUIRE(mtiles < (1ull << 31), kErrCapacity, "set difference: too many rows");
+    uint64_t* split = s.take<uint64_t>(mtiles + 1);
+    uint64_t* mhpos = sel.head ? s.take<uint64_t>(mtiles + 1) : nullptr;
+    SRDL_CUDA(cudaMemsetAsync(flags, 0, cp_words(n) * 4, L.stream));
+    dm_split_kernel<K><<<(unsigned)((mtiles + 1 + 255) / 256), 256, 0, L.stream>>>(sel, n, mtiles,
+                                                                                  split, mhpos);
+    const unsigned mgrid = (unsigned)std::min<uint64_t>(mtiles, (uint64_t)L.num_sms * 4);
+    dm_mark_kernel<K><<<mgrid, kCpThreads, 0, L.stream>>>(sel, n, mtiles, split, mhpos, flags);
+    cp_count_kernel<<<nb, kCpThreads, 0, L.stream>>>(flags, n, chunk, counts);
+    cp_scan_kernel<<<1, 1024, 0, L.stream>>>(counts, nb, offs, d_total);
+    cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, offs);
+    SRDL_CUDA(cudaGetLastError());
+    count_launches(5);
+    return;
+  }
   uint64_t* fpos = s.take<uint64_t>(tiles + 1);
   uint64_t* hpos = sel.head ? s.take<uint64_t>(tiles + 1) : nullptr;
   prefer_shared(dd_flag_kernel<K>);

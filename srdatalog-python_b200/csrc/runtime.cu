@@ -588,6 +588,10 @@ void Database::sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, 
              hd ? head->keys.as<uint64_t>() : nullptr, hd ? head->n : 0);
   prof_end(pid, 0, (double)n);
   out.n = read_scalar(0);
+  if (trace_)
+    fprintf(stderr, "srdl: sort n=%llu full=%llu head=%llu out=%llu\n", (unsigned long long)n,
+            (unsigned long long)(full ? full->n : 0), (unsigned long long)(hd ? head->n : 0),
+            (unsigned long long)out.n);
   if (pid != (size_t)-1) {
     // Algorithmic bytes: each counting pass reads and writes the packed
     // keys once; packing reads the input; the dedup pass reads the sorted

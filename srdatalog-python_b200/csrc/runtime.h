@@ -6,6 +6,8 @@
 // The plan is interpreted; kernels are fixed.
 #pragma once
 
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <string>
@@ -231,6 +233,7 @@ class Database {
   double run_ms_ = 0;
   bool own_stream_ = true;
   bool profile_ = false;
+  bool trace_ = std::getenv("SRDL_TRACE") != nullptr;  // per-sort sizes on stderr
   struct KEvent {
     std::string name;
     cudaEvent_t a, b;
