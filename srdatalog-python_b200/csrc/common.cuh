@@ -67,6 +67,12 @@ struct TrieView {
   // has hash_cap(len) slots for a list of len children.
   const uint32_t* hdir = nullptr;
   const uint32_t* hpool = nullptr;
+  // Bitmaps of long child lists (dense directory only): bdir[v] = bitmap slot
+  // of v's children or kNoBitmap; bitmap s is bpool[s*bwords .. +bwords), bit
+  // c set iff (v, c) is a key.
+  const uint32_t* bdir = nullptr;
+  const uint32_t* bpool = nullptr;
+  uint32_t bwords = 0;
   uint64_t n = 0;
   const uint64_t* n_roots_d = nullptr;  // device-resident root count
   uint32_t dir_n = 0;
@@ -127,6 +133,7 @@ __device__ __forceinline__ void trie_range(const TrieView& t, uint32_t v, uint32
 }
 
 constexpr uint32_t kNoHash = 0xffffffffu;
+constexpr uint32_t kNoBitmap = 0xffffffffu;
 constexpr uint32_t kHashEmpty = 0xffffffffu;
 
 // log2 of the table size for a list of len children: load factor <= 1/2.

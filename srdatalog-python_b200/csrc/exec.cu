@@ -97,6 +97,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
     if (probed && !d.prefix.empty() && v == kFull) {
       ensure_trie(r, ix);
       ensure_hash(ix);
+      ensure_bitmaps(ix);
     }
     SrcSpec s;
     s.t = view(r, ix);

@@ -59,7 +59,8 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
                                                                uint64_t* __restrict__ work,
                                                                uint8_t* __restrict__ drv,
                                                                uint32_t* __restrict__ beg,
-                                                               uint2* __restrict__ orange) {
+                                                               uint2* __restrict__ orange,
+                                                               uint32_t* __restrict__ obm) {
   // A table written by the previous level may fill only part of its
   // capacity; its true size is on the device and the rest expands to nothing.
   const uint64_t nrows = in.d_n ? min(in.n, *in.d_n) : in.n;
@@ -96,6 +97,12 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
       drv[r] = (uint8_t)bd;
       beg[r] = bd ? b1 : b0;
       orange[r] = bd ? make_uint2(b0, e0) : make_uint2(b1, e1);
+      if (obm) {
+        // the probed (other) list's bitmap, if its parent value has one
+        const uint32_t* obd = bd ? lv.src[0].t.bdir : lv.src[1].t.bdir;
+        const int ops = bd ? lv.src[0].prefix_slot : lv.src[1].prefix_slot;
+        obm[r] = (obd && ops >= 0) ? obd[in.col[ops][r]] : kNoBitmap;
+      }
     } else if (lv.kind == kColumnJoin) {
       uint32_t best = 0xffffffffu, bb = 0;
       int bd = 0;
@@ -238,9 +245,10 @@ __device__ __forceinline__ uint32_t lower_bound_bf(const uint32_t* __restrict__ 
 template <int MODE>
 __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
     LevelSpec lv, Table in, const uint64_t* __restrict__ offs, const uint8_t* __restrict__ drv,
-    const uint32_t* __restrict__ beg, const uint2* __restrict__ orange, uint64_t total,
-    uint64_t chunk, Table out, uint64_t* __restrict__ out_keys,
-    unsigned long long* __restrict__ d_out_n, uint64_t* __restrict__ warp_counts) {
+    const uint32_t* __restrict__ beg, const uint2* __restrict__ orange,
+    const uint32_t* __restrict__ obm, uint64_t total, uint64_t chunk, Table out,
+    uint64_t* __restrict__ out_keys, unsigned long long* __restrict__ d_out_n,
+    uint64_t* __restrict__ warp_counts) {
   const int lane = threadIdx.x & 31;
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t c0 = gw * chunk;
@@ -251,24 +259,66 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
   const uint32_t* dir0 = lv.src[0].prefix_slot < 0 ? lv.src[0].t.dir : nullptr;
   const uint32_t* dir1 = lv.src[1].prefix_slot < 0 ? lv.src[1].t.dir : nullptr;
   const uint32_t dn0 = lv.src[0].t.dir_n, dn1 = lv.src[1].t.dir_n;
+  const uint32_t* bp0 = lv.src[0].t.bpool;
+  const uint32_t* bp1 = lv.src[1].t.bpool;
+  const uint32_t bw0 = lv.src[0].t.bwords, bw1 = lv.src[1].t.bwords;
   unsigned long long running = 0;
   if (MODE == kModeTableWrite) running = warp_counts[gw];
   if (c0 < c1) {
     uint64_t r0 = gallop_row(offs, 0, in.n, c0);
+    // The row of the warp's first candidate and its metadata, kept while the
+    // warp stays in it (r0 is warp-uniform): most candidates lie in rows
+    // longer than a warp round, whose lanes then need no row search and no
+    // per-lane metadata loads.
+    uint64_t crow = ~0ull, c_off = 0, c_end = 0;
+    int cd = 0;
+    uint32_t cbeg = 0, cslot = kNoBitmap;
+    uint2 crg = make_uint2(0, 0);
     for (uint64_t base = c0; base < c1; base += 32) {
       const uint64_t w = base + lane;
       bool ok = w < c1;
       uint64_t r = r0;
       uint32_t v = 0;
-      if (ok) {
+      if (r0 != crow) {
+        crow = r0;
+        c_off = offs[r0];
+        c_end = offs[r0 + 1];
+        cd = drv[r0];
+        cbeg = beg[r0];
+        crg = orange[r0];
+        cslot = obm ? obm[r0] : kNoBitmap;
+      }
+      if (base + 31 < c_end) {
+        if (ok) {
+          v = (cd == 0 ? vals0 : vals1)[cbeg + (uint32_t)(w - c_off)];
+          const uint32_t* odir = cd == 0 ? dir1 : dir0;
+          if (odir) {
+            const uint32_t odn = cd == 0 ? dn1 : dn0;
+            ok = v + 1u < odn && odir[v] < odir[v + 1];
+          } else if (cslot != kNoBitmap) {
+            const uint32_t* bm = cd == 0 ? bp1 : bp0;
+            const uint32_t bw = cd == 0 ? bw1 : bw0;
+            ok = (bm[(uint64_t)cslot * bw + (v >> 5)] >> (v & 31)) & 1u;
+          } else {
+            const uint32_t* ov = cd == 0 ? vals1 : vals0;
+            const uint32_t p = lower_bound_bf(ov, crg.x, crg.y, v);
+            ok = p < crg.y && ov[p] == v;
+          }
+        }
+      } else if (ok) {
         r = gallop_row(offs, r0, in.n, w);
         const uint32_t local = (uint32_t)(w - offs[r]);
         const int d = drv[r];
         v = (d == 0 ? vals0 : vals1)[beg[r] + local];
         const uint32_t* odir = d == 0 ? dir1 : dir0;
+        const uint32_t slot = obm ? obm[r] : kNoBitmap;
         if (odir) {
           const uint32_t odn = d == 0 ? dn1 : dn0;
           ok = v + 1u < odn && odir[v] < odir[v + 1];
+        } else if (slot != kNoBitmap) {
+          const uint32_t* bm = d == 0 ? bp1 : bp0;
+          const uint32_t bw = d == 0 ? bw1 : bw0;
+          ok = (bm[(uint64_t)slot * bw + (v >> 5)] >> (v & 31)) & 1u;
         } else {
           const uint2 rg = orange[r];
           const uint32_t* ov = d == 0 ? vals1 : vals0;
@@ -523,7 +573,7 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
 size_t join_work_scratch_bytes(uint64_t rows) {
   rows = rows ? rows : 1;
   return ((rows * 8 + 255) & ~size_t(255)) + ((rows + 1) * 8 + 255) + ((rows + 255) & ~size_t(255)) +
-         ((rows * 4 + 255) & ~size_t(255)) + ((rows * 8 + 255) & ~size_t(255)) +
+         2 * ((rows * 4 + 255) & ~size_t(255)) + ((rows * 8 + 255) & ~size_t(255)) +
          scan_scratch_bytes(rows) + 1024;
 }
 
@@ -546,9 +596,11 @@ JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scrat
   w.drv = s.take<uint8_t>(in.n ? in.n : 1);
   w.beg = s.take<uint32_t>(in.n ? in.n : 1);
   w.orange = s.take<uint2>(in.n ? in.n : 1);
+  if (lv.kind == kColumnJoin && lv.nsrc == 2 && (lv.src[0].t.bdir || lv.src[1].t.bdir))
+    w.obm = s.take<uint32_t>(in.n ? in.n : 1);
   if (in.n) {
     join_count_kernel<<<jgrid(in.n, L.num_sms), kJThreads, 0, L.stream>>>(lv, in, work, w.drv,
-                                                                          w.beg, w.orange);
+                                                                          w.beg, w.orange, w.obm);
     SRDL_CUDA(cudaGetLastError());
     count_launches(1);
   }
@@ -568,7 +620,7 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
   if (lv.kind == kColumnJoin && lv.nsrc == 2 && lv.nfilt == 0) {
 #define SRDL_CJ2(MODE, WC) \
   join_cj2_kernel<MODE><<<g, kJThreads, 0, L.stream>>>(lv, in, w.offs, w.drv, w.beg, w.orange, \
-                                                       total, chunk, out, out_keys, cnt, WC)
+                                                       w.obm, total, chunk, out, out_keys, cnt, WC)
     if (lv.emit == kEmitCount) {
       SRDL_CJ2(kModeCount, nullptr);
       count_launches(1);

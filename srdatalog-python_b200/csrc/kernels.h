@@ -93,6 +93,17 @@ void build_roots(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* ro
 // scan (dir_n entries, offs[dir_n-1] = total slots).  Build: hdir[v] = first
 // slot or kNoHash; every child of a hashed list is inserted into `pool`,
 // which the caller pre-fills with 0xff bytes.
+// Bitmaps of long child lists.  bitmap_plan: cnt[k] = values whose child
+// list has at least (1024 << k) entries, k < kBitmapLevels.  bitmap_build:
+// bdir[v] = a fresh slot for lists of at least min_len entries (kNoBitmap
+// otherwise); every key (v, c) of such a list sets bit c of v's bitmap
+// (pool zeroed by the caller); *d_slots receives the slot count.
+constexpr int kBitmapLevels = 7;
+void bitmap_plan(const Launch& L, const uint32_t* dir, uint32_t dir_n, unsigned long long* cnt);
+void bitmap_build(const Launch& L, const uint64_t* keys, uint64_t n, const uint32_t* dir,
+                  uint32_t dir_n, uint32_t min_len, uint32_t* bdir, uint32_t* pool, uint32_t bwords,
+                  unsigned int* d_slots);
+
 size_t child_hash_scratch_bytes(uint32_t dir_n);
 void child_hash_plan(const Launch& L, const uint32_t* dir, uint32_t dir_n, uint32_t min_len,
                      uint64_t* sizes, uint64_t* offs, Scratch& s);
@@ -168,6 +179,7 @@ struct JoinWork {
   uint8_t* drv = nullptr;    // column join: driver source per row
   uint32_t* beg = nullptr;   // column join: driver list begin per row
   uint2* orange = nullptr;   // two-source column join: the other list [x, y) per row
+  uint32_t* obm = nullptr;   // two-source column join: bitmap slot of the other list, or kNoBitmap
 };
 JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scratch& s);
 

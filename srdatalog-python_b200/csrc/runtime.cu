@@ -777,6 +777,51 @@ void Database::ensure_hash(Index& ix) {
   prof_end(pid, 8.0 * ix.n + 4.0 * slots + 16.0 * nv, (double)ix.n);
 }
 
+// Bitmaps for the longest child lists of an index probed by a column join:
+// a membership test becomes one load instead of a binary search of up to 16
+// dependent steps.  The threshold is the smallest length 1024 * 2^k whose
+// bitmaps (one bit per value of the domain each) fit in SRDL_BITMAP_MB
+// (default 256 MB; 0 disables); domains above 2^24 values get none.
+static uint64_t bitmap_budget() {
+  static const uint64_t v = [] {
+    const char* e = getenv("SRDL_BITMAP_MB");
+    return (e ? (uint64_t)strtoull(e, nullptr, 10) : 256ull) << 20;
+  }();
+  return v;
+}
+
+void Database::ensure_bitmaps(Index& ix) {
+  if (ix.bitmap_done) return;
+  ix.bitmap_done = true;
+  if (bitmap_budget() == 0 || !ix.dir_n || ix.n < 1024 || dom_max_ >= (1u << 24)) return;
+  const uint32_t bwords = (uint32_t)(((uint64_t)dom_max_ + 1 + 31) / 32);
+  size_t pid = prof_begin("trie_build");
+  DevBuf cnt(kBitmapLevels * 8 + 8, L_.stream);
+  bitmap_plan(L_, ix.dir.as<uint32_t>(), ix.dir_n, cnt.as<unsigned long long>());
+  unsigned long long c[kBitmapLevels];
+  SRDL_CUDA(cudaMemcpyAsync(c, cnt.as<void>(), sizeof(c), cudaMemcpyDeviceToHost, L_.stream));
+  SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  int level = -1;
+  for (int k = 0; k < kBitmapLevels; k++)
+    if (c[k] && c[k] * bwords * 4ull <= bitmap_budget()) {
+      level = k;
+      break;
+    }
+  if (level < 0) {
+    prof_end(pid, 0, 0);
+    return;
+  }
+  const uint64_t slots = c[level];
+  ix.bwords = bwords;
+  ix.bdir = DevBuf((size_t)(ix.dir_n - 1) * 4, L_.stream);
+  ix.bpool = DevBuf(slots * bwords * 4, L_.stream);
+  SRDL_CUDA(cudaMemsetAsync(ix.bpool.as<void>(), 0, slots * bwords * 4, L_.stream));
+  bitmap_build(L_, ix.keys.as<uint64_t>(), ix.n, ix.dir.as<uint32_t>(), ix.dir_n, 1024u << level,
+               ix.bdir.as<uint32_t>(), ix.bpool.as<uint32_t>(), bwords,
+               reinterpret_cast<unsigned int*>(cnt.as<unsigned long long>() + kBitmapLevels));
+  prof_end(pid, 8.0 * ix.n + 4.0 * slots * bwords + 8.0 * ix.dir_n, (double)ix.n);
+}
+
 TrieView Database::view(Relation& r, Index& ix) {
   ensure_trie(r, ix);
   TrieView t;
@@ -786,6 +831,9 @@ TrieView Database::view(Relation& r, Index& ix) {
   t.dir = ix.dir_n ? ix.dir.as<uint32_t>() : nullptr;
   t.hdir = ix.hdir.bytes() ? ix.hdir.as<uint32_t>() : nullptr;
   t.hpool = ix.hpool.bytes() ? ix.hpool.as<uint32_t>() : nullptr;
+  t.bdir = ix.bdir.bytes() ? ix.bdir.as<uint32_t>() : nullptr;
+  t.bpool = ix.bpool.bytes() ? ix.bpool.as<uint32_t>() : nullptr;
+  t.bwords = ix.bwords;
   t.n = ix.n;
   t.n_roots_d = ix.nroots_d.as<uint64_t>();
   t.dir_n = ix.dir_n;

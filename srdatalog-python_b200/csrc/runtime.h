@@ -70,6 +70,9 @@ struct Index {
   uint32_t dir_n = 0;
   bool hash_done = false;  // hashed child lists built (or found unnecessary)
   DevBuf hdir, hpool;
+  bool bitmap_done = false;  // bitmaps of long child lists built (or found unnecessary)
+  DevBuf bdir, bpool;
+  uint32_t bwords = 0;
 };
 
 struct Chunk {
@@ -267,6 +270,7 @@ class Database {
   void ensure_trie(Relation& r, Index& ix);
   TrieView view(Relation& r, Index& ix);
   void ensure_hash(Index& ix);
+  void ensure_bitmaps(Index& ix);
   void sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full,
                  const Index* head = nullptr);
   void exec_ops(const Step& st, uint64_t iteration);

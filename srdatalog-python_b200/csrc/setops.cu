@@ -252,6 +252,57 @@ void child_hash_build(const Launch& L, const uint64_t* keys, uint64_t n, const u
   count_launches(n ? 2 : 1);
 }
 
+// ---- bitmaps of long child lists ---------------------------------------
+
+__global__ void bitmap_plan_kernel(const uint32_t* __restrict__ dir, uint32_t nv,
+                                   unsigned long long* __restrict__ cnt) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+    const uint32_t len = dir[v + 1] - dir[v];
+#pragma unroll
+    for (int k = 0; k < kBitmapLevels; k++)
+      if (len >= (1024u << k)) atomicAdd(&cnt[k], 1ull);
+  }
+}
+
+__global__ void bitmap_assign_kernel(const uint32_t* __restrict__ dir, uint32_t nv,
+                                     uint32_t min_len, uint32_t* __restrict__ bdir,
+                                     unsigned int* __restrict__ d_slots) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+    bdir[v] = dir[v + 1] - dir[v] >= min_len ? atomicAdd(d_slots, 1u) : kNoBitmap;
+}
+
+__global__ void bitmap_fill_kernel(const uint64_t* __restrict__ keys, uint64_t n,
+                                   const uint32_t* __restrict__ bdir, uint32_t* __restrict__ pool,
+                                   uint32_t bwords) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    const uint32_t s = bdir[k >> 32], c = (uint32_t)k;
+    if (s != kNoBitmap) atomicOr(&pool[(uint64_t)s * bwords + (c >> 5)], 1u << (c & 31));
+  }
+}
+
+void bitmap_plan(const Launch& L, const uint32_t* dir, uint32_t dir_n, unsigned long long* cnt) {
+  const uint32_t nv = dir_n - 1;
+  SRDL_CUDA(cudaMemsetAsync(cnt, 0, kBitmapLevels * sizeof(unsigned long long), L.stream));
+  bitmap_plan_kernel<<<grid_for(nv, L.num_sms), 256, 0, L.stream>>>(dir, nv, cnt);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(1);
+}
+
+void bitmap_build(const Launch& L, const uint64_t* keys, uint64_t n, const uint32_t* dir,
+                  uint32_t dir_n, uint32_t min_len, uint32_t* bdir, uint32_t* pool, uint32_t bwords,
+                  unsigned int* d_slots) {
+  const uint32_t nv = dir_n - 1;
+  SRDL_CUDA(cudaMemsetAsync(d_slots, 0, sizeof(unsigned int), L.stream));
+  bitmap_assign_kernel<<<grid_for(nv, L.num_sms), 256, 0, L.stream>>>(dir, nv, min_len, bdir,
+                                                                       d_slots);
+  if (n)
+    bitmap_fill_kernel<<<grid_for(n, L.num_sms), 256, 0, L.stream>>>(keys, n, bdir, pool, bwords);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(n ? 2 : 1);
+}
+
 __global__ void bounds_kernel(const uint64_t* __restrict__ keys, uint64_t n,
                               const uint32_t* __restrict__ bounds, uint64_t nb,
                               uint64_t* __restrict__ pos) {
