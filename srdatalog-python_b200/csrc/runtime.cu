@@ -477,6 +477,11 @@ void Database::load_rows(const std::string& name, const uint32_t* rows, uint64_t
   SRDL_REQUIRE(r.arity <= 2, kErrUnsupported,
                "relation " + name + ": only arity 1 and 2 relations can be materialised");
   r.staged.insert(r.staged.end(), rows, rows + n * r.arity);
+  // The value bound is taken once here, not on every run (a run re-uploads
+  // the rows but never rescans them on the host).
+  uint32_t mx = r.staged_max;
+  for (uint64_t i = 0; i < n * r.arity; i++) mx = rows[i] > mx ? rows[i] : mx;
+  r.staged_max = mx;
   r.pinned_valid = false;  // page-locked mirror is stale
   r.loaded = true;
 }
@@ -517,6 +522,7 @@ void Database::clear_inputs() {
     Relation& r = *kv.second;
     r.staged.clear();
     r.staged.shrink_to_fit();
+    r.staged_max = 0;
     r.pinned_valid = false;
     r.dstaged.reset();
     r.dstaged_n = 0;
@@ -607,7 +613,7 @@ void Database::sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, 
 void Database::upload_inputs() {
   uint32_t mx = 0;
   for (auto& kv : rels_) {
-    for (uint32_t x : kv.second->staged) mx = std::max(mx, x);
+    if (!kv.second->staged.empty()) mx = std::max(mx, kv.second->staged_max);
     if (kv.second->dstaged_n) mx = std::max(mx, kv.second->dstaged_max);
   }
   dom_max_ = mx;

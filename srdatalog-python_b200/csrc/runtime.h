@@ -100,6 +100,7 @@ struct Relation {
   std::vector<int> canonical;
   RelVersion v[3];
   std::vector<uint32_t> staged;  // host rows loaded before run (row-major)
+  uint32_t staged_max = 0;       // largest value in `staged` (kept as rows are added)
   uint32_t* pinned = nullptr;    // page-locked copy of `staged` used for the upload
   size_t pinned_cap = 0;         // words allocated; grows, freed only at close
   bool pinned_valid = false;     // holds the current `staged`
