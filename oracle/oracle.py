@@ -257,6 +257,12 @@ def run_plan(plan: dict, inputs: dict, max_iters: int = 0):
       elif k == 'filter':
         ev = _filter_fn(p['code'])
         nb = [b for b in binds if ev(b)]
+      elif k == 'negation':
+        # keep a binding iff no tuple of the relation starts (in index order)
+        # with the prefix values
+        idx, pre = p['index'], p['prefix']
+        present = {tuple(t[idx[i]] for i in range(len(pre))) for t in db[(p['rel'], p['ver'])]}
+        nb = [b for b in binds if tuple(b[v] for v in pre) not in present]
       elif k == 'insert_into':
         if op['count']:
           counts[op['rule']] = counts.get(op['rule'], 0) + len(binds)
@@ -352,3 +358,31 @@ def cspa(inputs: dict) -> dict:
     vf |= n_vf
     va |= n_va
     ma |= n_ma
+
+
+def lsqb_q7(inputs: dict) -> dict:
+  '''Counts of examples/lsqb_q7_optional.py:106-131 in closed form: with T, C,
+  R, L the numbers of distinct tags, creators, replying comments and likers
+  of a message, Case1 = sum T*C*R*L, Case2 = sum over messages without likers
+  of T*C*R, Case3 = sum over messages without replies of T*C*L, Case4 = sum
+  over messages with neither of T*C.'''
+  def per_msg(rows, col):
+    a = np.unique(np.asarray(rows, np.int64), axis=0)
+    keys, cnt = np.unique(a[:, col], return_counts=True)
+    return dict(zip(keys.tolist(), cnt.tolist()))
+  t = per_msg(inputs['HasTag'], 0)
+  c = per_msg(inputs['HasCreator'], 0)
+  r = per_msg(inputs['ReplyOf'], 1)
+  lk = per_msg(inputs['Likes'], 1)
+  out = {'Case1Both': 0, 'Case2ReplyOnly': 0, 'Case3LikeOnly': 0, 'Case4Neither': 0}
+  for m, nt in t.items():
+    nc = c.get(m, 0)
+    nr, nl = r.get(m, 0), lk.get(m, 0)
+    out['Case1Both'] += nt * nc * nr * nl
+    if nl == 0:
+      out['Case2ReplyOnly'] += nt * nc * nr
+    if nr == 0:
+      out['Case3LikeOnly'] += nt * nc * nl
+    if nr == 0 and nl == 0:
+      out['Case4Neither'] += nt * nc
+  return out

@@ -108,6 +108,23 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
   std::vector<LevelSpec> levels;
   const PipeOp* insert = nullptr;
   for (const PipeOp& po : op.pipeline) {
+    if (po.kind == PipeOp::Negation) {
+      // anti-join: a filter term that probes the negated relation's index
+      SRDL_REQUIRE(!levels.empty(), kErrPlan, "rule " + op.rule + ": negation before any join");
+      LevelSpec& lv = levels.back();
+      SRDL_REQUIRE(lv.nfilt < kMaxFilt, kErrUnsupported, "too many filter terms");
+      const SourceDesc& d = po.sources[0];
+      Relation& nr = rel(d.rel);
+      SRDL_REQUIRE(nr.arity <= 2, kErrUnsupported, "negation over relation " + nr.name + " of arity > 2");
+      FiltSpec f;
+      f.negation = true;
+      f.a_slot = slot_of(d.prefix[0]);
+      f.b_slot = d.prefix.size() > 1 ? slot_of(d.prefix[1]) : -1;
+      SRDL_REQUIRE(f.b_slot < 0 || nr.arity == 2, kErrPlan, "negation prefix longer than " + nr.name);
+      f.neg = view(nr, ensure_index(nr, d.ver, d.index));
+      lv.filt[lv.nfilt++] = f;
+      continue;
+    }
     if (po.kind == PipeOp::Filter) {
       SRDL_REQUIRE(!levels.empty(), kErrPlan, "rule " + op.rule + ": filter before any join");
       LevelSpec& lv = levels.back();

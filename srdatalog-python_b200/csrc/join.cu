@@ -170,6 +170,7 @@ __device__ __forceinline__ uint64_t gallop_row(const uint64_t* offs, uint64_t lo
 }
 
 __device__ __forceinline__ bool filt_ok(const FiltSpec& f, uint32_t a, uint32_t b) {
+  if (f.negation) return f.b_slot < 0 ? !trie_has_root(f.neg, a) : !trie_child_contains(f.neg, a, b);
   switch (f.op) {
     case kNe: return a != b;
     case kEq: return a == b;
@@ -211,6 +212,10 @@ __device__ __forceinline__ bool level_filters(const LevelSpec& lv, const Table& 
         a = fs.a_slot == s0 ? v0 : fs.a_slot == s1 ? v1 : slot_value(in, fs.a_slot, r);
       if (fs.b_slot >= 0)
         b = fs.b_slot == s0 ? v0 : fs.b_slot == s1 ? v1 : slot_value(in, fs.b_slot, r);
+      if (fs.negation) {
+        ok &= filt_ok(fs, a, b);
+        continue;
+      }
       switch (fs.op) {
         case kNe: ok &= a != b; break;
         case kEq: ok &= a == b; break;

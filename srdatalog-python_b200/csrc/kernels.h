@@ -142,6 +142,10 @@ struct FiltSpec {
   int a_slot = -1, b_slot = -1;  // -1: use the constant
   uint32_t a_const = 0, b_const = 0;
   int op = kNe;
+  // Negation (MIR `negation`, mir/types.py:189): keep the binding iff the
+  // tuple (a) -- or (a, b) when b_slot >= 0 -- is not a key prefix of `neg`.
+  bool negation = false;
+  TrieView neg;
 };
 
 struct LevelSpec {

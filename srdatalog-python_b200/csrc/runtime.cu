@@ -281,6 +281,11 @@ void Database::parse_plan(const std::string& plan_json) {
             po.vars = pj.at("vars").strs();
             for (auto& s : pj.at("sources").a()) po.sources.push_back(parse_source(s));
             for (auto& v : pj.at("var_from_source").a()) po.var_from_source.push_back(v.strs());
+          } else if (pk == "negation") {
+            po.kind = PipeOp::Negation;
+            po.sources.push_back(parse_source(pj));
+            SRDL_REQUIRE(!po.sources[0].prefix.empty() && po.sources[0].prefix.size() <= 2,
+                         kErrUnsupported, "plan: negation needs one or two bound variables");
           } else if (pk == "filter") {
             po.kind = PipeOp::Filter;
             po.vars = pj.at("vars").strs();

@@ -130,7 +130,7 @@ struct SourceDesc {
 };
 
 struct PipeOp {
-  enum Kind { Scan, ColumnJoin, Cartesian, Filter, Insert } kind;
+  enum Kind { Scan, ColumnJoin, Cartesian, Filter, Insert, Negation } kind;
   std::vector<SourceDesc> sources;           // scan: one
   std::vector<std::string> vars;             // scan / cartesian / insert / filter vars
   std::string var;                           // column join var

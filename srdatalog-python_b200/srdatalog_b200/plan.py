@@ -18,8 +18,8 @@ Plan layout (version 1)::
 
 op kinds: execute_pipeline, rebuild_index, clear_relation, check_size,
 compute_delta_index, merge_index, rebuild_index_from_index,
-post_stratum_reconstruct.  Pipeline ops: scan, column_join, cartesian_join,
-filter, insert_into.
+post_stratum_reconstruct, inject_cpp_hook (kept, not executed).  Pipeline
+ops: scan, column_join, cartesian_join, filter, negation, insert_into.
 '''
 
 from __future__ import annotations
@@ -70,6 +70,13 @@ def _pipeline_op(node: Any) -> dict:
             'sources': [_source(s) for s in node.sources]}
   if kind == 'Filter':
     return {'op': 'filter', 'vars': list(node.vars), 'code': node.code}
+  if kind == 'Negation':
+    # anti-join on bound variables (mir/types.py:189); constant arguments
+    # would need a constant-bound probe, which this runtime does not have
+    if getattr(node, 'const_args', None):
+      raise PlanError(f'negation on {node.rel_name} with constant arguments is not supported')
+    return {'op': 'negation', 'rel': node.rel_name, 'ver': _ver(node.version),
+            'index': [int(c) for c in node.index], 'prefix': list(node.prefix_vars)}
   if kind == 'InsertInto':
     return {'op': 'insert_into', 'rel': node.rel_name, 'ver': _ver(node.version),
             'vars': list(node.vars), 'index': [int(c) for c in node.index]}
@@ -235,6 +242,14 @@ def validate_plan(plan: dict) -> None:
           bound += p['vars'] if k in ('scan', 'cartesian_join') else [p['var']]
         elif k == 'filter':
           parse_filter(p['code'], bound)
+        elif k == 'negation':
+          if p['rel'] not in arity:
+            raise PlanError(f'unknown relation {p["rel"]}')
+          if not 1 <= len(p['prefix']) <= min(2, arity[p['rel']]):
+            raise PlanError(f'negation on {p["rel"]}: needs 1..2 bound variables')
+          for v in p['prefix']:
+            if v not in bound:
+              raise PlanError(f'negation on {p["rel"]}: unbound var {v} in {op["rule"]}')
         elif k == 'insert_into':
           if p['rel'] not in arity or len(p['vars']) != arity[p['rel']]:
             raise PlanError(f'insert_into {p["rel"]}: arity mismatch')

@@ -172,3 +172,28 @@ def cspa_inputs(n_vars: int, m: int, seed: int) -> dict:
   rng = _rng(seed)
   return {'AssignInput': _pairs(rng, n_vars, max(1, 3 * m // 4)),
           'DerefInput': _pairs(rng, n_vars, max(1, m // 4))}
+
+
+def lsqb_q7_inputs(n_msgs: int, seed: int, tags: int = 64, persons: int = 5000,
+                   reply_frac: float = 0.5, like_frac: float = 0.5) -> dict:
+  '''Inputs of LSQB Q7 (examples/lsqb_q7_optional.py) over n_msgs messages:
+  every message gets 1-3 tags and 1 creator; a `reply_frac` share of the
+  messages gets 1-4 replying comments (comment ids above the messages) and a
+  `like_frac` share 1-6 likers; uniform draws, deduplicated.'''
+  rng = _rng(seed)
+  m = np.arange(n_msgs, dtype=np.uint32)
+
+  def fan(msgs, lo, hi, vals):
+    k = rng.integers(lo, hi + 1, msgs.shape[0])
+    mm = np.repeat(msgs, k)
+    return mm, rng.integers(0, vals, mm.shape[0], dtype=np.uint32)
+
+  tm, tv = fan(m, 1, 3, tags)
+  cm, cv = fan(m, 1, 1, persons)
+  rmsg = m[rng.random(n_msgs) < reply_frac]
+  rm, rc = fan(rmsg, 1, 4, 4 * n_msgs)
+  lmsg = m[rng.random(n_msgs) < like_frac]
+  lm, lp = fan(lmsg, 1, 6, persons)
+  return {'HasTag': _dedup_in_order(tm, tv), 'HasCreator': _dedup_in_order(cm, cv),
+          'ReplyOf': _dedup_in_order((rc + n_msgs).astype(np.uint32), rm),
+          'Likes': _dedup_in_order(lp, lm)}

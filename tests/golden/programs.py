@@ -148,6 +148,37 @@ def cspa_program() -> Program:
   ])
 
 
+def lsqb_q7_program() -> Program:
+  '''LSQB Q7 "optional" (examples/lsqb_q7_optional.py): messages with tags and
+  creators, counted by whether they have replies and likes; the two
+  "without" cases are negations of unary relations.'''
+  has_tag = Relation('HasTag', 2, input_file='Message_hasTag_Tag.csv')
+  has_creator = Relation('HasCreator', 2, input_file='Message_hasCreator_Person.csv')
+  reply_of = Relation('ReplyOf', 2, input_file='ReplyOf_Comment_Message.csv')
+  likes = Relation('Likes', 2, input_file='Person_likes_Message.csv')
+  has_reply = Relation('HasReply', 1, column_types=(int,))
+  has_liker = Relation('HasLiker', 1, column_types=(int,))
+  case1 = Relation('Case1', 5, print_size=True)
+  case2 = Relation('Case2', 4, print_size=True)
+  case3 = Relation('Case3', 4, print_size=True)
+  case4 = Relation('Case4', 3, print_size=True)
+  c, comment, liker, m, t = Var('c'), Var('comment'), Var('liker'), Var('m'), Var('t')
+  return Program(rules=[
+    (has_reply(m) <= reply_of(Var('_'), m)).named('MarkHasReply'),
+    (has_liker(m) <= likes(Var('_'), m)).named('MarkHasLiker'),
+    (case1(m, t, c, comment, liker)
+     <= has_tag(m, t) & has_creator(m, c) & reply_of(comment, m) & likes(liker, m))
+    .named('Case1Both').with_plan(var_order=['m', 'comment', 'liker', 't', 'c']).with_count(),
+    (case2(m, t, c, comment)
+     <= has_tag(m, t) & has_creator(m, c) & reply_of(comment, m) & ~has_liker(m))
+    .named('Case2ReplyOnly').with_plan(var_order=['m', 'comment', 't', 'c']).with_count(),
+    (case3(m, t, c, liker) <= has_tag(m, t) & has_creator(m, c) & likes(liker, m) & ~has_reply(m))
+    .named('Case3LikeOnly').with_plan(var_order=['m', 'liker', 't', 'c']).with_count(),
+    (case4(m, t, c) <= has_tag(m, t) & has_creator(m, c) & ~has_reply(m) & ~has_liker(m))
+    .named('Case4Neither').with_plan(var_order=['m', 't', 'c']).with_count(),
+  ])
+
+
 # name -> (builder, project name, reference MIR fixture or None)
 PROGRAMS = {
   'tc': (tc_program, 'TcPlan', 'tc.mir.sexpr'),
@@ -157,4 +188,5 @@ PROGRAMS = {
   'tc_lsm': (tc_lsm_program, 'TcPlan', 'tc.mir.sexpr'),
   'andersen': (andersen_program, 'AndersenPlan', 'integration/andersen.mir.sexpr'),
   'cspa': (cspa_program, 'CspaPlan', 'integration/cspa.mir.sexpr'),
+  'lsqb_q7': (lsqb_q7_program, 'LsqbQ7Plan', 'integration/lsqb_q7_optional.mir.sexpr'),
 }

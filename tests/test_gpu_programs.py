@@ -262,3 +262,18 @@ def test_cspa_vs_rules(n, m, seed):
     w = np.array(want[rel], np.uint32).reshape(-1, 2)
     assert db.size(rel) == w.shape[0], rel
     assert oracle.dump_hash(db.dump(rel)) == oracle.dump_hash(w), rel
+
+
+@pytest.mark.parametrize('n_msgs,seed', [(60, 0), (5000, 1), (400_000, 2)])
+def test_lsqb_q7_negation_counts(n_msgs, seed):
+  '''LSQB Q7: four-source column join, wide count-only heads and negations of
+  unary relations, against the closed-form counts.'''
+  inp = W.lsqb_q7_inputs(n_msgs, seed)
+  db = native.Database(load_plan('lsqb_q7'))
+  for rel, rows in inp.items():
+    db.load_rows(rel, rows)
+  db.run()
+  want = oracle.lsqb_q7(inp)
+  got = {rule: db.count(rule) for rule in want}
+  assert got == want
+  assert db.size('HasReply') == len(set(inp['ReplyOf'][:, 1].tolist()))

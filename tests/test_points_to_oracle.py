@@ -1,4 +1,5 @@
-'''The points-to programs (examples/andersen.py, examples/cspa.py): the plan
+'''Beyond TC/SG/triangle: the points-to programs (examples/andersen.py,
+examples/cspa.py) and LSQB Q7 with negation (examples/lsqb_q7_optional.py): the plan
 interpreter (oracle.run_plan, which walks the MIR op sequence) agrees with
 independent naive restatements of the programs' rules, so either can check
 the GPU path.'''
@@ -33,3 +34,11 @@ def test_points_to_plans_shape():
   assert sum(o['op'] == 'execute_pipeline' for o in rec['ops']) == 5   # the parallel group
   cs = load_plan('cspa')
   assert {r['name'] for r in cs['relations']} >= {'ValueFlow', 'ValueAlias', 'MemoryAlias'}
+
+
+@pytest.mark.parametrize('seed', [0, 1])
+def test_lsqb_q7_interpreter_vs_closed_form(seed):
+  '''Negation: the plan interpreter's counts of LSQB Q7 equal the closed form.'''
+  inp = W.lsqb_q7_inputs(60, seed, tags=8, persons=30)
+  _, counts = oracle.run_plan(load_plan('lsqb_q7'), inp)
+  assert counts == oracle.lsqb_q7(inp)
