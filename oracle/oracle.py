@@ -386,3 +386,18 @@ def lsqb_q7(inputs: dict) -> dict:
     if nr == 0 and nl == 0:
       out['Case4Neither'] += nt * nc
   return out
+
+
+def lsqb_q6(inputs: dict) -> int:
+  '''Count of examples/lsqb_q6_count.py:70-91 in closed form: Knows is the
+  symmetric closure of the input, N(p) its neighbours and I(p) the distinct
+  interests of p; the bindings (p1, p2, p3, t) with p1 != p3 number
+  sum over p2 of (|N(p2)| - 1) * sum over p3 in N(p2) of I(p3).'''
+  e = np.asarray(inputs['KnowsInput'], np.int64)
+  k = np.unique(np.concatenate([e, e[:, ::-1]]), axis=0)
+  hi = np.unique(np.asarray(inputs['HasInterestInput'], np.int64), axis=0)
+  n = int(max(k.max(initial=0), hi[:, 0].max(initial=0))) + 1
+  interests = np.bincount(hi[:, 0], minlength=n)
+  deg = np.bincount(k[:, 0], minlength=n)
+  s = np.bincount(k[:, 0], weights=interests[k[:, 1]], minlength=n)
+  return int(np.sum((deg - 1) * s))

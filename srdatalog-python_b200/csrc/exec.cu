@@ -341,6 +341,7 @@ void Database::op_rebuild(const Step& st, size_t pos, const Op& op) {
 void Database::op_compute_delta(const Op& op) {
   Relation& r = rel(op.rel);
   r.v[kDelta].clear();
+  r.delta_epoch++;
   if (r.pending_delta) {
     r.v[kDelta].idx[op.index] = std::move(r.pending);
     r.pending = Index{};
@@ -391,6 +392,9 @@ void Database::op_merge(const Op& op) {
       SRDL_CUDA(cudaMemcpyAsync(f.keys.as<uint64_t>(), d->keys.as<uint64_t>(), dn * 8,
                                 cudaMemcpyDeviceToDevice, L_.stream));
     f.n = dn;
+    f.epoch = r.delta_epoch;
+    r.base_epoch = r.full_epoch;
+    r.full_epoch = r.delta_epoch;
     return;
   }
   if (dn == 0) return;
@@ -407,6 +411,8 @@ void Database::op_merge(const Op& op) {
     for (auto it2 = r.v[kFull].idx.begin(); it2 != r.v[kFull].idx.end();)
       it2 = it2->first == r.canonical ? std::next(it2) : r.v[kFull].idx.erase(it2);
     Index& h = r.head;
+    r.base_epoch = r.full_epoch;
+    r.full_epoch = r.delta_epoch;
     Index m;
     m.n = h.n + dn;
     m.keys = DevBuf(m.n * 8, L_.stream);
@@ -422,14 +428,31 @@ void Database::op_merge(const Op& op) {
     if (h.n * 10 > fn) compact_head(r);
     return;
   }
-  Index& f = ensure_index(r, kFull, op.index);
+  // The same DELTA is merged into every permutation the plan lists.  The
+  // first one takes it on top of an up-to-date FULL; a later one merges it
+  // only when it was up to date just before this delta, and is otherwise
+  // rebuilt from a permutation that already holds it (never merged twice).
+  auto fit = r.v[kFull].idx.find(op.index);
+  Index* f = fit == r.v[kFull].idx.end() ? nullptr : &fit->second;
+  if (r.full_epoch < r.delta_epoch) {
+    if (!f || f->epoch != r.full_epoch) f = &ensure_index(r, kFull, op.index);
+    r.base_epoch = r.full_epoch;
+  } else {
+    if (f && f->epoch == r.delta_epoch) return;
+    if (!f || f->epoch != r.base_epoch) {
+      ensure_index(r, kFull, op.index);  // rebuilt from one that holds this delta
+      return;
+    }
+  }
   Index m;
-  m.n = f.n + dn;
+  m.n = f->n + dn;
   m.keys = DevBuf(m.n * 8, L_.stream);
   size_t pid = prof_begin("merge");
-  merge_disjoint(L_, f.keys.as<uint64_t>(), f.n, d->keys.as<uint64_t>(), dn, m.keys.as<uint64_t>());
+  merge_disjoint(L_, f->keys.as<uint64_t>(), f->n, d->keys.as<uint64_t>(), dn,
+                 m.keys.as<uint64_t>());
   prof_end(pid, 16.0 * m.n, (double)m.n);
-  r.v[kFull].idx.clear();
+  m.epoch = r.delta_epoch;
+  r.full_epoch = r.delta_epoch;
   r.v[kFull].idx[op.index] = std::move(m);
 }
 

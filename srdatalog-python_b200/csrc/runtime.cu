@@ -466,6 +466,7 @@ void Database::reset_device_state() {
     kv.second->pending = Index{};
     kv.second->pending_delta = false;
     kv.second->head = Index{};
+    kv.second->delta_epoch = kv.second->full_epoch = kv.second->base_epoch = 0;
   }
   counts_.clear();
   group_counts_.clear();
@@ -689,6 +690,7 @@ void Database::compact_head(Relation& r) {
   size_t pid = prof_begin("merge");
   merge_disjoint(L_, f.keys.as<uint64_t>(), f.n, h.keys.as<uint64_t>(), h.n, m.keys.as<uint64_t>());
   prof_end(pid, 16.0 * m.n, (double)m.n);
+  m.epoch = r.full_epoch;
   r.v[kFull].idx.clear();
   r.v[kFull].idx[r.canonical] = std::move(m);
 }
@@ -713,13 +715,22 @@ Index& Database::ensure_index(Relation& r, Ver v, const std::vector<int>& perm) 
   if (v == kFull && r.head.n) compact_head(r);
   RelVersion& rv = r.v[v];
   auto it = rv.idx.find(perm);
-  if (it != rv.idx.end()) return it->second;
+  if (it != rv.idx.end()) {
+    if (v != kFull || it->second.epoch >= r.full_epoch) return it->second;
+    rv.idx.erase(it);  // a FULL permutation that missed the latest delta
+  }
   Index& ix = rv.idx[perm];
-  // Build from any existing permutation of the same version.
+  // Build from an existing permutation of the same version (for FULL, one
+  // that holds every merged delta).
+  const Index* src = nullptr;
   for (auto& kv : rv.idx) {
     if (&kv.second == &ix) continue;
+    if (!src || (v == kFull && kv.second.epoch > src->epoch)) src = &kv.second;
+  }
+  if (src) {
     SRDL_REQUIRE(r.arity == 2, kErrUnsupported, "secondary index on non-binary relation " + r.name);
-    sort_into(ix, kv.second.keys.as<uint64_t>(), kv.second.n, true, nullptr);
+    sort_into(ix, src->keys.as<uint64_t>(), src->n, true, nullptr);
+    ix.epoch = src->epoch;
     return ix;
   }
   ix.n = 0;

@@ -65,6 +65,7 @@ struct Index {
   DevBuf keys;
   uint64_t n = 0;
   bool trie = false;
+  uint64_t epoch = 0;  // FULL: the last delta (Relation::delta_epoch) merged into this permutation
   DevBuf lo, roots, dir;
   DevBuf nroots_d;  // device-resident count of `roots`
   uint32_t dir_n = 0;
@@ -119,6 +120,11 @@ struct Relation {
   // the merged canonical array on demand.
   bool lsm = false;
   Index head;
+  // Every compute_delta_index makes a new DELTA (delta_epoch).  full_epoch is
+  // the last one any permutation of FULL has absorbed, base_epoch the one
+  // before it: a permutation at base_epoch still lacks the latest delta and is
+  // merged with it; one older than that is rebuilt from an up-to-date one.
+  uint64_t delta_epoch = 0, full_epoch = 0, base_epoch = 0;
 };
 
 // Plan-level descriptions (parsed once from JSON).

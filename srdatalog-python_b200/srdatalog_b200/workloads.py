@@ -197,3 +197,14 @@ def lsqb_q7_inputs(n_msgs: int, seed: int, tags: int = 64, persons: int = 5000,
   return {'HasTag': _dedup_in_order(tm, tv), 'HasCreator': _dedup_in_order(cm, cv),
           'ReplyOf': _dedup_in_order((rc + n_msgs).astype(np.uint32), rm),
           'Likes': _dedup_in_order(lp, lm)}
+
+
+def lsqb_q6_inputs(n_persons: int, m_knows: int, seed: int, tags: int = 200) -> dict:
+  '''Inputs of LSQB Q6 (examples/lsqb_q6_count.py): uniform Knows pairs
+  (no self-loops, deduplicated) and 0-4 interests per person.'''
+  rng = _rng(seed)
+  knows = uniform_edges(n_persons, m_knows, seed)
+  k = rng.integers(0, 5, n_persons)
+  p = np.repeat(np.arange(n_persons, dtype=np.uint32), k)
+  t = rng.integers(0, tags, p.shape[0], dtype=np.uint32)
+  return {'KnowsInput': knows, 'HasInterestInput': _dedup_in_order(p, t)}

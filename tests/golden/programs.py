@@ -179,6 +179,26 @@ def lsqb_q7_program() -> Program:
   ])
 
 
+def lsqb_q6_program() -> Program:
+  '''LSQB Q6 2-hop count (examples/lsqb_q6_count.py): Knows loaded in both
+  directions by two rules, a count-only arity-4 head with a filter.'''
+  knows_in = Relation('KnowsInput', 2, input_file='Person_knows_Person.csv')
+  interest_in = Relation('HasInterestInput', 2, input_file='Person_hasInterest_Tag.csv')
+  knows = Relation('Knows', 2)
+  has_interest = Relation('HasInterest', 2)
+  path = Relation('Path', 4)
+  p, p1, p2, p3, t, x, y = (Var(n) for n in ('p', 'p1', 'p2', 'p3', 't', 'x', 'y'))
+  return Program(rules=[
+    (knows(x, y) <= knows_in(x, y)).named('KnowsLoad'),
+    (knows(y, x) <= knows_in(x, y)).named('KnowsLoadRev'),
+    (has_interest(p, t) <= interest_in(p, t)).named('InterestLoad'),
+    (path(p1, p2, p3, t)
+     <= knows(p1, p2) & knows(p2, p3) & has_interest(p3, t)
+     & Filter(('p1', 'p3'), 'return p1 != p3;'))
+    .named('TwoHopPath').with_plan(var_order=['p2', 'p3', 'p1', 't']).with_count(),
+  ])
+
+
 # name -> (builder, project name, reference MIR fixture or None)
 PROGRAMS = {
   'tc': (tc_program, 'TcPlan', 'tc.mir.sexpr'),
@@ -189,4 +209,5 @@ PROGRAMS = {
   'andersen': (andersen_program, 'AndersenPlan', 'integration/andersen.mir.sexpr'),
   'cspa': (cspa_program, 'CspaPlan', 'integration/cspa.mir.sexpr'),
   'lsqb_q7': (lsqb_q7_program, 'LsqbQ7Plan', 'integration/lsqb_q7_optional.mir.sexpr'),
+  'lsqb_q6': (lsqb_q6_program, 'LsqbQ6Plan', 'integration/lsqb_q6_count.mir.sexpr'),
 }

@@ -277,3 +277,15 @@ def test_lsqb_q7_negation_counts(n_msgs, seed):
   got = {rule: db.count(rule) for rule in want}
   assert got == want
   assert db.size('HasReply') == len(set(inp['ReplyOf'][:, 1].tolist()))
+
+
+@pytest.mark.parametrize('n,m,seed', [(40, 90, 0), (20_000, 200_000, 1), (300_000, 2_400_000, 2)])
+def test_lsqb_q6_two_hop_counts(n, m, seed):
+  '''LSQB Q6: Knows loaded by two rules (both directions), a filtered
+  count-only 2-hop, against the closed form.'''
+  inp = W.lsqb_q6_inputs(n, m, seed)
+  db = native.Database(load_plan('lsqb_q6'))
+  for rel, rows in inp.items():
+    db.load_rows(rel, rows)
+  db.run()
+  assert db.count('TwoHopPath') == oracle.lsqb_q6(inp)

@@ -42,3 +42,10 @@ def test_lsqb_q7_interpreter_vs_closed_form(seed):
   inp = W.lsqb_q7_inputs(60, seed, tags=8, persons=30)
   _, counts = oracle.run_plan(load_plan('lsqb_q7'), inp)
   assert counts == oracle.lsqb_q7(inp)
+
+
+@pytest.mark.parametrize('seed', [0, 1])
+def test_lsqb_q6_interpreter_vs_closed_form(seed):
+  inp = W.lsqb_q6_inputs(40, 90, seed, tags=6)
+  _, counts = oracle.run_plan(load_plan('lsqb_q6'), inp)
+  assert counts['TwoHopPath'] == oracle.lsqb_q6(inp)
