@@ -45,10 +45,10 @@ WORKLOADS = {
   'sg': dict(plan='sg', rel='Arc', out='Sg', kind='size',
              desc='same generation, windowed forest n=10,000 (parent in [i-1000,i-1]) '
                   '+ 10% cross edges, seed 2'),
-  'batched': dict(plan='tc_lsm', rel='ArcInput', out='Path', kind='batched',
+  'batched': dict(plan='tc', rel='ArcInput', out='Path', kind='batched', tune=True,
                   desc='4,096 independent TC instances, directed Erdos-Renyi, n log-uniform in '
                        '[64, 1024], mean out-degree U[2,8], seed 1000+j; evaluated as one '
-                       'disjoint union; Path declared Device2LevelIndex'),
+                       'disjoint union; index policy and options picked by the autotuner'),
 }
 
 BATCH_COUNT = 4096
@@ -399,11 +399,19 @@ def main():
   plan = load_plan(wl['plan'])
   edges = make_edges(args.workload)
   n = edges.shape[0]
+  tuned = None
+  if wl.get('tune'):
+    # untimed: the autotuner times candidate settings on this very input
+    from srdatalog_b200.autotune import autotune
+    tuned = autotune(plan, {wl['rel']: edges}, device=local, reps=2)
+    plan = tuned.apply(plan)
   stream = torch.cuda.current_stream(dev)
 
   # ---------------- kernel-resident path (value)
   d_edges = torch.from_numpy(edges.view(np.int32).reshape(-1)).to(dev)
   db = Database(plan, device=local)
+  if tuned:
+    tuned.configure(db)
   db.set_stream(stream.cuda_stream)
   db.load_device_rows(wl['rel'], d_edges.data_ptr(), n)
   db.set_profiling(True)
@@ -464,6 +472,8 @@ def main():
                         'step_ms': [round(x, 3) for x in step_ms]}), flush=True)
     return
   db2 = Database(plan, device=local)
+  if tuned:
+    tuned.configure(db2)
   db2.set_stream(stream.cuda_stream)
   db2.load_rows(wl['rel'], edges)
   for _ in range(args.warmup):
@@ -538,6 +548,8 @@ def main():
   }
   if batched:
     line['config'].update(instances=per_step, tuples_per_s=units * args.steps * world / (total_ms / 1e3))
+  if tuned:
+    line['config']['autotuned'] = dict(tuned.to_json(), trials=len(tuned.trials))
     if plain:
       line['plain_loop'] = plain
       line['speedup_vs_plain_loop'] = value / plain['queries_per_s']

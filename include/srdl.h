@@ -75,6 +75,19 @@ int srdl_set_stream(srdl_db* db, void* stream);
  * device time and algorithmic bytes in srdl_stats_json ("kernels"). */
 int srdl_set_profiling(srdl_db* db, int enable);
 
+/* Per-handle tuning options (the autotuner's knobs; results never change):
+ *   "bitmap_mb"        budget for bitmaps of long child lists (MB, 0 = none;
+ *                      default SRDL_BITMAP_MB or 256)
+ *   "hash_min"         hash child lists longer than this (0 = never; default
+ *                      SRDL_HASH_MIN or 0)
+ *   "lsm_compact_pct"  Device2LevelIndex: merge HEAD into FULL once HEAD
+ *                      exceeds this percentage of FULL (default 10, the
+ *                      reference's kCompactRatio, device_2level_index.h:300)
+ * Unknown names return 1 (argument error); negative values are rejected.
+ * No reference counterpart: the reference fixes these at code-generation
+ * time. */
+int srdl_set_option(srdl_db* db, const char* name, int64_t value);
+
 /* Kernels this process has launched through libsrdl so far. */
 uint64_t srdl_launch_count(void);
 

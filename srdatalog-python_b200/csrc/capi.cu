@@ -190,6 +190,11 @@ int srdl_load_device_rows(srdl_db* h, const char* rel, const uint32_t* d_rows, u
 
 uint64_t srdl_launch_count(void) { return srdl::launches_total(); }
 
+int srdl_set_option(srdl_db* h, const char* name, int64_t value) {
+  if (!h || !name) return kErrArg;
+  SRDL_GUARD(0, h->db->set_option(name, value); return 0;)
+}
+
 int srdl_set_count_groups(srdl_db* h, const char* rule, const uint32_t* bounds,
                           uint64_t n_bounds) {
   if (!h || !rule) return kErrArg;

@@ -405,7 +405,8 @@ void Database::op_merge(const Op& op) {
       return;
     }
     // DELTA goes into HEAD (O(|HEAD| + |DELTA|)); HEAD is merged into FULL
-    // once it holds more than a tenth of FULL (device_2level_index.h:291-318).
+    // once it holds more than lsm_compact_pct percent of FULL (default 10,
+    // device_2level_index.h:291-318).
     Index& f = full_base(r, op.index);
     const uint64_t fn = f.n;
     for (auto it2 = r.v[kFull].idx.begin(); it2 != r.v[kFull].idx.end();)
@@ -425,7 +426,7 @@ void Database::op_merge(const Op& op) {
                                 cudaMemcpyDeviceToDevice, L_.stream));
     prof_end(pid, 16.0 * m.n, (double)m.n);
     h = std::move(m);
-    if (h.n * 10 > fn) compact_head(r);
+    if (h.n * 100 > fn * (uint64_t)opt_lsm_pct_) compact_head(r);
     return;
   }
   // The same DELTA is merged into every permutation the plan lists.  The

@@ -773,17 +773,26 @@ static uint32_t hash_min_len() {
   return v;
 }
 
+void Database::set_option(const std::string& name, int64_t value) {
+  SRDL_REQUIRE(value >= 0, kErrArg, "set_option: negative value for " + name);
+  if (name == "bitmap_mb") opt_bitmap_mb_ = value;
+  else if (name == "hash_min") opt_hash_min_ = value;
+  else if (name == "lsm_compact_pct") opt_lsm_pct_ = value;
+  else throw Error{kErrArg, "set_option: unknown option " + name};
+}
+
 void Database::ensure_hash(Index& ix) {
   if (ix.hash_done) return;
   ix.hash_done = true;
-  if (hash_min_len() == 0 || !ix.dir_n || ix.n == 0 || dom_max_ == 0xffffffffu) return;
+  const uint32_t min_len = opt_hash_min_ >= 0 ? (uint32_t)opt_hash_min_ : hash_min_len();
+  if (min_len == 0 || !ix.dir_n || ix.n == 0 || dom_max_ == 0xffffffffu) return;
   size_t pid = prof_begin("child_hash_build");
   DevBuf scratch(child_hash_scratch_bytes(ix.dir_n), L_.stream);
   Scratch s{scratch.as<char>(), scratch.bytes(), 0};
   const uint32_t nv = ix.dir_n - 1;
   uint64_t* sizes = s.take<uint64_t>(nv);
   uint64_t* offs = s.take<uint64_t>(nv + 1);
-  child_hash_plan(L_, ix.dir.as<uint32_t>(), ix.dir_n, hash_min_len(), sizes, offs, s);
+  child_hash_plan(L_, ix.dir.as<uint32_t>(), ix.dir_n, min_len, sizes, offs, s);
   SRDL_CUDA(cudaMemcpyAsync(h_small_ + 5, offs + nv, 8, cudaMemcpyDeviceToHost, L_.stream));
   SRDL_CUDA(cudaStreamSynchronize(L_.stream));
   const uint64_t slots = h_small_[5];
@@ -815,7 +824,8 @@ static uint64_t bitmap_budget() {
 void Database::ensure_bitmaps(Index& ix) {
   if (ix.bitmap_done) return;
   ix.bitmap_done = true;
-  if (bitmap_budget() == 0 || !ix.dir_n || ix.n < 1024 || dom_max_ >= (1u << 24)) return;
+  const uint64_t budget = opt_bitmap_mb_ >= 0 ? (uint64_t)opt_bitmap_mb_ << 20 : bitmap_budget();
+  if (budget == 0 || !ix.dir_n || ix.n < 1024 || dom_max_ >= (1u << 24)) return;
   const uint32_t bwords = (uint32_t)(((uint64_t)dom_max_ + 1 + 31) / 32);
   size_t pid = prof_begin("trie_build");
   DevBuf cnt(kBitmapLevels * 8 + 8, L_.stream);
@@ -825,7 +835,7 @@ void Database::ensure_bitmaps(Index& ix) {
   SRDL_CUDA(cudaStreamSynchronize(L_.stream));
   int level = -1;
   for (int k = 0; k < kBitmapLevels; k++)
-    if (c[k] && c[k] * bwords * 4ull <= bitmap_budget()) {
+    if (c[k] && c[k] * bwords * 4ull <= budget) {
       level = k;
       break;
     }

@@ -206,6 +206,7 @@ class Database {
                     uint64_t* counts);
   void set_stream(cudaStream_t s);
   void set_profiling(bool on) { profile_ = on; }
+  void set_option(const std::string& name, int64_t value);
   void load_csv(const std::string& rel, const std::string& path);
   void load_all(const std::string& dir);
   void run(uint64_t max_iters);
@@ -244,6 +245,9 @@ class Database {
   bool own_stream_ = true;
   bool profile_ = false;
   bool trace_ = std::getenv("SRDL_TRACE") != nullptr;  // per-sort sizes on stderr
+  int64_t opt_bitmap_mb_ = -1;      // -1: SRDL_BITMAP_MB or the default
+  int64_t opt_hash_min_ = -1;       // -1: SRDL_HASH_MIN or off
+  int64_t opt_lsm_pct_ = 10;        // HEAD -> FULL merge threshold (% of FULL)
   struct KEvent {
     std::string name;
     cudaEvent_t a, b;

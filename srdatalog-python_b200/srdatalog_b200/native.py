@@ -53,6 +53,7 @@ SIGNATURES = {
   'srdl_merge_u64': (ctypes.c_int, [_vp, _u64, _vp, _u64, _vp, _vp]),
   'srdl_sort_unique_u64_noalloc': (ctypes.c_int, [_vp, _u64, ctypes.c_int, _vp, _vp, _vp]),
   'srdl_sort_unique_noalloc_max_keys': (_u64, []),
+  'srdl_set_option': (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64]),
 }
 
 _LIB = None
@@ -141,6 +142,10 @@ class Database:
 
   def set_profiling(self, on: bool = True) -> None:
     check(lib().srdl_set_profiling(self._h, 1 if on else 0), 'srdl_set_profiling')
+
+  def set_option(self, name: str, value: int) -> None:
+    '''Tuning option (srdl_set_option): bitmap_mb, hash_min, lsm_compact_pct.'''
+    check(lib().srdl_set_option(self._h, name.encode(), int(value)), 'srdl_set_option')
 
   def set_count_groups(self, rule: str, bounds) -> None:
     b = np.ascontiguousarray(bounds, dtype=np.uint32)

@@ -289,3 +289,19 @@ def test_lsqb_q6_two_hop_counts(n, m, seed):
     db.load_rows(rel, rows)
   db.run()
   assert db.count('TwoHopPath') == oracle.lsqb_q6(inp)
+
+
+def test_autotune_on_device():
+  '''The tuner's runs on the GPU agree on the result, and the tuned setting
+  reproduces it.'''
+  from srdatalog_b200.autotune import autotune
+  e = W.uniform_edges(1500, 5000, 3)
+  plan = load_plan('tc')
+  res = autotune(plan, {'ArcInput': e}, reps=1, space={'bitmap_mb': [0, 256], 'lsm_compact_pct': [10]})
+  db = native.Database(res.apply(plan))
+  res.configure(db)
+  db.load_rows('ArcInput', e)
+  db.run()
+  keys, _, _ = oracle.tc(e)
+  assert db.size('Path') == keys.shape[0]
+  assert len(res.trials) >= 2
