@@ -401,3 +401,20 @@ def lsqb_q6(inputs: dict) -> int:
   deg = np.bincount(k[:, 0], minlength=n)
   s = np.bincount(k[:, 0], weights=interests[k[:, 1]], minlength=n)
   return int(np.sum((deg - 1) * s))
+
+
+def reach_avoid(edges: np.ndarray, blocked: np.ndarray) -> dict:
+  '''Reach = transitive closure of Edge minus Blocked edges; Cut = Blocked
+  pairs not in Reach (the reach_avoid test program), by Python sets.'''
+  blk = set(map(tuple, np.asarray(blocked).tolist()))
+  ok = [tuple(e) for e in np.asarray(edges).tolist() if tuple(e) not in blk]
+  succ: dict = {}
+  for a, b in ok:
+    succ.setdefault(a, set()).add(b)
+  reach = set(ok)
+  frontier = set(ok)
+  while frontier:
+    new = {(x, z) for x, y in frontier for z in succ.get(y, ())} - reach
+    reach |= new
+    frontier = new
+  return {'Reach': sorted(reach), 'Cut': sorted(p for p in blk if p not in reach)}

@@ -199,6 +199,23 @@ def lsqb_q6_program() -> Program:
   ])
 
 
+def reach_avoid_program() -> Program:
+  '''Reachability that avoids blocked edges, and the blocked pairs that are
+  not reachable: negation of a binary relation on two bound variables, once
+  inside a recursive stratum's join and once in a later stratum.  No
+  reference fixture pins it (stratified negation exercised here only).'''
+  edge = Relation('Edge', 2, column_types=(int, int), input_file='Edge.csv')
+  blocked = Relation('Blocked', 2, column_types=(int, int), input_file='Blocked.csv')
+  reach = Relation('Reach', 2, column_types=(int, int), print_size=True)
+  cut = Relation('Cut', 2, column_types=(int, int), print_size=True)
+  x, y, z = Var('x'), Var('y'), Var('z')
+  return Program(rules=[
+    (reach(x, y) <= edge(x, y) & ~blocked(x, y)).named('ReachBase'),
+    (reach(x, z) <= reach(x, y) & edge(y, z) & ~blocked(y, z)).named('ReachStep'),
+    (cut(x, y) <= blocked(x, y) & ~reach(x, y)).named('CutPairs'),
+  ])
+
+
 # name -> (builder, project name, reference MIR fixture or None)
 PROGRAMS = {
   'tc': (tc_program, 'TcPlan', 'tc.mir.sexpr'),
@@ -210,4 +227,5 @@ PROGRAMS = {
   'cspa': (cspa_program, 'CspaPlan', 'integration/cspa.mir.sexpr'),
   'lsqb_q7': (lsqb_q7_program, 'LsqbQ7Plan', 'integration/lsqb_q7_optional.mir.sexpr'),
   'lsqb_q6': (lsqb_q6_program, 'LsqbQ6Plan', 'integration/lsqb_q6_count.mir.sexpr'),
+  'reach_avoid': (reach_avoid_program, 'ReachAvoidPlan', None),
 }

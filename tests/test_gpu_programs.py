@@ -305,3 +305,20 @@ def test_autotune_on_device():
   keys, _, _ = oracle.tc(e)
   assert db.size('Path') == keys.shape[0]
   assert len(res.trials) >= 2
+
+
+@pytest.mark.parametrize('n,m,seed', [(30, 70, 0), (400, 1500, 1), (20_000, 24_000, 2)])
+def test_reach_avoid_negation(n, m, seed):
+  '''Negation of a binary relation on two bound variables, inside the
+  recursive step and in a later stratum over the recursive result.'''
+  e = W.uniform_edges(n, m, seed)
+  blocked = np.concatenate([e[::3], W.uniform_edges(n, m // 4, seed + 10)])
+  db = native.Database(load_plan('reach_avoid'))
+  db.load_rows('Edge', e)
+  db.load_rows('Blocked', blocked)
+  db.run()
+  want = oracle.reach_avoid(e, blocked)
+  for rel in ('Reach', 'Cut'):
+    w = np.array(want[rel], np.uint32).reshape(-1, 2)
+    assert db.size(rel) == w.shape[0], rel
+    assert oracle.dump_hash(db.dump(rel)) == oracle.dump_hash(w), rel

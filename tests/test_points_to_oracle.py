@@ -4,6 +4,7 @@ interpreter (oracle.run_plan, which walks the MIR op sequence) agrees with
 independent naive restatements of the programs' rules, so either can check
 the GPU path.'''
 
+import numpy as np
 import oracle
 import pytest
 from conftest import load_plan
@@ -49,3 +50,28 @@ def test_lsqb_q6_interpreter_vs_closed_form(seed):
   inp = W.lsqb_q6_inputs(40, 90, seed, tags=6)
   _, counts = oracle.run_plan(load_plan('lsqb_q6'), inp)
   assert counts['TwoHopPath'] == oracle.lsqb_q6(inp)
+
+
+@pytest.mark.parametrize('seed', [0, 1, 2])
+def test_reach_avoid_interpreter_vs_sets(seed):
+  '''Negation on two bound variables (inside a recursive join and in a later
+  stratum): interpreter == set restatement.'''
+  e = W.uniform_edges(30, 70, seed)
+  blocked = np.ascontiguousarray(e[::3])
+  extra = W.uniform_edges(30, 20, seed + 10)
+  blocked = np.concatenate([blocked, extra])
+  got, _ = oracle.run_plan(load_plan('reach_avoid'), {'Edge': e, 'Blocked': blocked})
+  want = oracle.reach_avoid(e, blocked)
+  assert sorted(got['Reach']) == want['Reach']
+  assert sorted(got['Cut']) == want['Cut']
+
+
+def test_set_option_rejects_unknown_names():
+  from srdatalog_b200 import native
+  db = native.Database(load_plan('tc'))
+  with pytest.raises(Exception):
+    db.set_option('no_such_option', 1)
+  with pytest.raises(Exception):
+    db.set_option('bitmap_mb', -1)
+  db.set_option('bitmap_mb', 0)
+  db.close()
