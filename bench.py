@@ -11,8 +11,12 @@ value : tuples/s with the input already in HBM (srdl_load_device_rows),
         CUDA events on the database stream, L2 flushed between steps.
 e2e   : same metric through the C ABI from pinned host rows (srdl_load_rows
         + srdl_run, which uploads them), result read back to the host.
-Multi-GPU (torchrun): independent replicas, one per GPU; value = total
-tuples over the max per-rank time.
+Multi-GPU (torchrun): one program sharded over the GPUs when its plan
+allows it (srdatalog_b200.shard: the triangle count splits its last join
+level's work items, TC partitions Path by source; inputs replicated, one
+final all-reduce of the result), value = the job's tuples over the max
+per-rank time (strong scaling); plans that would need a per-iteration
+exchange (SG) run as independent replicas (weak scaling).
 --impl reference: the CPU restatement of the reference's evaluation on
 the host cores, on a bounded sample of the same workload.
 '''
@@ -183,6 +187,16 @@ def max_over_ranks(x: float, dist, device) -> float:
   t = torch.tensor([x], dtype=torch.float64, device=device)
   dist.all_reduce(t, op=dist.ReduceOp.MAX)
   return float(t.item())
+
+
+def sum_over_ranks(x: int, dist, device) -> int:
+  '''The sum of an integer over all ranks (every rank gets it); x itself on one rank.'''
+  if dist is None:
+    return x
+  import torch
+  t = torch.tensor([x], dtype=torch.int64, device=device)
+  dist.all_reduce(t, op=dist.ReduceOp.SUM)
+  return int(t.item())
 
 
 def replica_throughput(units_per_step: float, steps: int, world: int, max_ms: float) -> float:
@@ -395,6 +409,7 @@ def main():
   torch.cuda.set_device(dev)
 
   from srdatalog_b200 import Database, native
+  from srdatalog_b200.shard import shard_plan
   wl = WORKLOADS[args.workload]
   plan = load_plan(wl['plan'])
   edges = make_edges(args.workload)
@@ -405,20 +420,38 @@ def main():
     from srdatalog_b200.autotune import autotune
     tuned = autotune(plan, {wl['rel']: edges}, device=local, reps=2)
     plan = tuned.apply(plan)
+  # N > 1: shard the one program over the ranks when its plan allows it
+  spec = shard_plan(plan) if world > 1 else None
+  sharded = bool(spec and spec.useful)
+  if sharded:
+    plan = spec.plan
   stream = torch.cuda.current_stream(dev)
+
+  def open_db():
+    d = Database(plan, device=local)
+    if tuned:
+      tuned.configure(d)
+    if sharded:
+      d.set_option('shard_world', world)
+      d.set_option('shard_rank', rank)
+    d.set_stream(stream.cuda_stream)
+    return d
+
+  def job_units(d) -> int:
+    # the job's result: a sharded relation's or count's parts add up
+    u = result_units(d, wl)
+    return sum_over_ranks(u, dist, dev) if sharded else u
 
   # ---------------- kernel-resident path (value)
   d_edges = torch.from_numpy(edges.view(np.int32).reshape(-1)).to(dev)
-  db = Database(plan, device=local)
-  if tuned:
-    tuned.configure(db)
-  db.set_stream(stream.cuda_stream)
+  db = open_db()
   db.load_device_rows(wl['rel'], d_edges.data_ptr(), n)
   db.set_profiling(True)
   flush = torch.empty(64 << 20, dtype=torch.int32, device=dev)  # 256 MB > 126 MB L2
   for _ in range(args.warmup):
     db.run()
-  units = result_units(db, wl)
+    job_units(db)
+  units = job_units(db)
   batched = wl['kind'] == 'batched'
   if batched:  # one step answers every instance: the metric counts queries
     insts, union = make_batch()
@@ -442,6 +475,7 @@ def main():
     l0 = native.lib().srdl_launch_count()
     ev0.record(stream)
     db.run()
+    got = job_units(db) if sharded else units  # sharded: the final all-reduce is timed
     ev1.record(stream)
     ev1.synchronize()
     launches += native.lib().srdl_launch_count() - l0
@@ -450,14 +484,16 @@ def main():
       agg = kernels.setdefault(k, {'ms': 0.0, 'bytes': 0.0, 'units': 0.0, 'scopes': 0})
       for f in agg:
         agg[f] += s[f]
-    assert result_units(db, wl) == units
+    assert got == units and (sharded or result_units(db, wl) == units)
   torch.cuda.synchronize(dev)
   clocks = sampler.stop()
   if dist:
     dist.barrier()
   total_ms = sum(step_ms)
   total_ms = max_over_ranks(total_ms, dist, dev)
-  value = replica_throughput(per_step, args.steps, world, total_ms)
+  # sharded: per_step is already the whole job's; replicas: one per rank
+  copies = 1 if sharded else world
+  value = replica_throughput(per_step, args.steps, copies, total_ms)
   stats = db.stats()
   db.close()
   del d_edges
@@ -471,13 +507,11 @@ def main():
                         'ms_per_step': total_ms / args.steps, 'quick': True,
                         'step_ms': [round(x, 3) for x in step_ms]}), flush=True)
     return
-  db2 = Database(plan, device=local)
-  if tuned:
-    tuned.configure(db2)
-  db2.set_stream(stream.cuda_stream)
+  db2 = open_db()
   db2.load_rows(wl['rel'], edges)
   for _ in range(args.warmup):
     db2.run()
+    job_units(db2)
   e2e_ms = []
   if dist:
     dist.barrier()
@@ -487,9 +521,13 @@ def main():
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     db2.run()
-    got = result_units(db2, wl)  # result read back to the host
+    got = job_units(db2)  # result read back to the host (summed over shards)
     if batched:  # every instance's size read back
       per_inst = db2.range_counts(wl['out'], bounds)
+      if sharded:
+        t = torch.from_numpy(per_inst.astype(np.int64)).to(dev)
+        dist.all_reduce(t)
+        per_inst = t.cpu().numpy()
     ev1.record(stream)
     ev1.synchronize()
     e2e_ms.append(ev0.elapsed_time(ev1))
@@ -528,12 +566,14 @@ def main():
   line = {
     'metric': metric_name, 'value': value, 'unit': unit_name, 'n_gpus': world,
     'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
-    'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'u32',
+    'higher_is_better': True, 'scaling': 'strong' if sharded else 'weak', 'vs_baseline': None,
+    'dtype': 'u32',
     'data': 'synthetic',
     'config': {'workload': wl['desc'], 'edges': int(n), 'tuples_per_step': int(units),
-               'parallelism': f'replicas{world}', 'l2': 'flushed between steps (256 MB write)',
+               'parallelism': f'shards{world}' if sharded else f'replicas{world}',
+               'l2': 'flushed between steps (256 MB write)',
                'inputs': 'HBM-resident for value; pinned host rows for e2e'},
-    'e2e': {'value': replica_throughput(per_step, args.steps, world, e2e_total), 'unit': unit_name,
+    'e2e': {'value': replica_throughput(per_step, args.steps, copies, e2e_total), 'unit': unit_name,
             'ms_per_step': e2e_total / args.steps, 'h2d_bytes_per_step': int(n) * 8,
             'd2h_bytes_per_step': 8 + (8 * per_step if batched else 0),
             'step_ms': [round(x, 3) for x in e2e_ms]},
@@ -547,7 +587,14 @@ def main():
     'clocks': clocks,
   }
   if batched:
-    line['config'].update(instances=per_step, tuples_per_s=units * args.steps * world / (total_ms / 1e3))
+    line['config'].update(instances=per_step,
+                          tuples_per_s=units * args.steps * copies / (total_ms / 1e3))
+  if sharded:
+    line['config']['sharding'] = {'partitioned': spec.partitioned,
+                                  'rules': {r: m for r, m in spec.modes.items() if m},
+                                  'inputs': 'replicated on every rank'}
+  elif world > 1 and spec is not None:
+    line['config']['sharding'] = {'replicas': spec.fallback or 'nothing to split'}
   if tuned:
     line['config']['autotuned'] = dict(tuned.to_json(), trials=len(tuned.trials))
     if plain:

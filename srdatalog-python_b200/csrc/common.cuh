@@ -147,6 +147,13 @@ __host__ __device__ __forceinline__ uint32_t hash_slot(uint32_t x, int k) {
   return (uint32_t)(((uint64_t)x * 0x9E3779B97F4A7C15ull) >> (64 - k));
 }
 
+// Owner of key value v among `world` shards: a multiplicative hash scaled to
+// [0, world), so consecutive ids spread evenly.  The Python host layer
+// (shard.owner) computes the same function.
+__host__ __device__ __forceinline__ uint32_t shard_owner(uint32_t v, uint32_t world) {
+  return (uint32_t)(((uint64_t)(v * 0x9E3779B1u) * world) >> 32);
+}
+
 __device__ __forceinline__ bool trie_has_root(const TrieView& t, uint32_t v) {
   uint32_t b, e;
   trie_range(t, v, b, e);

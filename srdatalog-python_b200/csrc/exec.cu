@@ -71,6 +71,8 @@ std::vector<FilterTerm> parse_filter(const std::string& code) {
 
 }  // namespace
 
+constexpr uint64_t kSegsPerShard = 256;
+
 void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
   std::map<std::string, int> slot;
   int nslots = 0;
@@ -173,6 +175,28 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
     levels.push_back(lv);
   }
   SRDL_REQUIRE(insert && !levels.empty(), kErrPlan, "rule " + op.rule + ": no insert_into");
+  const bool sharded = shard_world_ > 1 && op.shard != Op::NoShard;
+  // Work sharding splits the last-but-one level of rules with three or more
+  // levels (its items -- e.g. the triangle's (a, b) edges -- carry bounded
+  // work each, so interleaved segments balance; the first level's root keys
+  // can carry a hub's whole subtree) and otherwise the last level.
+  const size_t work_split = levels.size() >= 3 ? levels.size() - 2 : levels.size() - 1;
+  if (sharded && op.shard == Op::Key) {
+    // keep the bindings whose key value this shard owns, at the level binding it
+    const int ks = slot_of(op.shard_var);
+    for (size_t li = 0; li < levels.size(); li++) {
+      const int bound_after = li + 1 < levels.size() ? levels[li + 1].n_in_slots : nslots;
+      if (ks < levels[li].n_in_slots || ks >= bound_after) continue;
+      LevelSpec& lv = levels[li];
+      SRDL_REQUIRE(lv.nfilt < kMaxFilt, kErrUnsupported, "too many filter terms");
+      FiltSpec f;
+      f.a_slot = ks;
+      f.b_const = (uint32_t)shard_rank_;
+      f.shard_world = (uint32_t)shard_world_;
+      lv.filt[lv.nfilt++] = f;
+      break;
+    }
+  }
 
   Relation* target = &rel(insert->rel);
   if (!op.count)
@@ -195,7 +219,17 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
     SRDL_CUDA(cudaMemcpyAsync(h_small_ + 3, w.offs + cur.n, 8, cudaMemcpyDeviceToHost, L_.stream));
     SRDL_CUDA(cudaMemsetAsync(d_small_.as<uint64_t>() + 2, 0, 8, L_.stream));
     SRDL_CUDA(cudaStreamSynchronize(L_.stream));
-    const uint64_t total = h_small_[3];
+    uint64_t total = h_small_[3];
+    if (sharded && op.shard == Op::Work && li == work_split) {
+      // Deal this level's work items out in segments, kSegsPerShard per
+      // shard, interleaved so every shard gets a share of each key range
+      // (skewed keys cluster); later levels see only this shard's rows.
+      const uint64_t per = total / ((uint64_t)shard_world_ * kSegsPerShard);
+      lv.seg = std::max<uint64_t>(32, (per + 31) & ~uint64_t(31));
+      lv.seg_world = (uint32_t)shard_world_;
+      lv.seg_rank = (uint32_t)shard_rank_;
+      total = seg_owned(total, lv.seg, shard_world_, shard_rank_);
+    }
     if (last) {
       if (op.count) {
         lv.emit = kEmitCount;
@@ -506,6 +540,7 @@ void Database::exec_ops(const Step& st, uint64_t it) {
 
 void Database::run(uint64_t max_iters) {
   init_device();
+  SRDL_REQUIRE(shard_rank_ < shard_world_, kErrArg, "shard_rank must be below shard_world");
   reset_device_state();
   const uint64_t launches0 = launches_total();
   auto t0 = std::chrono::steady_clock::now();

@@ -170,6 +170,7 @@ __device__ __forceinline__ uint64_t gallop_row(const uint64_t* offs, uint64_t lo
 }
 
 __device__ __forceinline__ bool filt_ok(const FiltSpec& f, uint32_t a, uint32_t b) {
+  if (f.shard_world) return shard_owner(a, f.shard_world) == f.b_const;
   if (f.negation) return f.b_slot < 0 ? !trie_has_root(f.neg, a) : !trie_child_contains(f.neg, a, b);
   switch (f.op) {
     case kNe: return a != b;
@@ -180,6 +181,39 @@ __device__ __forceinline__ bool filt_ok(const FiltSpec& f, uint32_t a, uint32_t 
     default: return a >= b;
   }
 }
+
+// A shard's work items are the segments seg_rank, seg_rank + seg_world, ...
+// of `seg` items each (lv.seg = 0: all items, unsegmented).  The expand
+// kernels walk this shard's items as a dense "virtual" range [0, total) in
+// warp rounds of 32; SegWalk maps a round's first virtual item to its actual
+// item (a round never straddles segments: seg and every warp's start are
+// multiples of 32).
+// Instantiated with SEG = false for unsharded levels, which keep the plain
+// index arithmetic (and register count) of the hot kernels.
+template <bool SEG>
+struct SegWalk {
+  uint64_t seg, stride, rank_off, idx, off;
+  __device__ __forceinline__ SegWalk(const LevelSpec& lv, uint64_t v0) {
+    if (SEG) {
+      seg = lv.seg;
+      idx = v0 / seg;
+      off = v0 - idx * seg;
+      stride = seg * lv.seg_world;
+      rank_off = seg * lv.seg_rank;
+    } else {
+      seg = idx = stride = rank_off = 0;
+      off = v0;
+    }
+  }
+  __device__ __forceinline__ uint64_t at() const { return SEG ? idx * stride + rank_off + off : off; }
+  __device__ __forceinline__ void next() {
+    off += 32;
+    if (SEG && off == seg) {
+      off = 0;
+      idx++;
+    }
+  }
+};
 
 enum ExpandMode : int { kModeCount = 0, kModeKeys = 1, kModeTableCount = 2, kModeTableWrite = 3 };
 
@@ -212,7 +246,7 @@ __device__ __forceinline__ bool level_filters(const LevelSpec& lv, const Table& 
         a = fs.a_slot == s0 ? v0 : fs.a_slot == s1 ? v1 : slot_value(in, fs.a_slot, r);
       if (fs.b_slot >= 0)
         b = fs.b_slot == s0 ? v0 : fs.b_slot == s1 ? v1 : slot_value(in, fs.b_slot, r);
-      if (fs.negation) {
+      if (fs.negation || fs.shard_world) {
         ok &= filt_ok(fs, a, b);
         continue;
       }
@@ -247,7 +281,7 @@ __device__ __forceinline__ uint32_t lower_bound_bf(const uint32_t* __restrict__ 
 // range, so a candidate costs one coalesced load of its value plus a
 // branch-free binary search in the other list (or a directory check when
 // the other list is all roots of a dense index).
-template <int MODE>
+template <int MODE, bool SEG>
 __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
     LevelSpec lv, Table in, const uint64_t* __restrict__ offs, const uint8_t* __restrict__ drv,
     const uint32_t* __restrict__ beg, const uint2* __restrict__ orange,
@@ -270,7 +304,8 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
   unsigned long long running = 0;
   if (MODE == kModeTableWrite) running = warp_counts[gw];
   if (c0 < c1) {
-    uint64_t r0 = gallop_row(offs, 0, in.n, c0);
+    SegWalk<SEG> sw(lv, c0);
+    uint64_t r0 = gallop_row(offs, 0, in.n, sw.at());
     // The row of the warp's first candidate and its metadata, kept while the
     // warp stays in it (r0 is warp-uniform): most candidates lie in rows
     // longer than a warp round, whose lanes then need no row search and no
@@ -279,9 +314,10 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
     int cd = 0;
     uint32_t cbeg = 0, cslot = kNoBitmap;
     uint2 crg = make_uint2(0, 0);
-    for (uint64_t base = c0; base < c1; base += 32) {
-      const uint64_t w = base + lane;
-      bool ok = w < c1;
+    for (uint64_t base = c0; base < c1; base += 32, sw.next()) {
+      const uint64_t abase = sw.at();
+      const uint64_t w = abase + lane;
+      bool ok = base + lane < c1;
       uint64_t r = r0;
       uint32_t v = 0;
       if (r0 != crow) {
@@ -293,7 +329,7 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
         crg = orange[r0];
         cslot = obm ? obm[r0] : kNoBitmap;
       }
-      if (base + 31 < c_end) {
+      if (abase + 31 < c_end) {
         if (ok) {
           v = (cd == 0 ? vals0 : vals1)[cbeg + (uint32_t)(w - c_off)];
           const uint32_t* odir = cd == 0 ? dir1 : dir0;
@@ -385,7 +421,7 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
   }
 }
 
-template <int MODE>
+template <int MODE, bool SEG>
 __global__ void __launch_bounds__(kJThreads) join_expand_kernel(
     LevelSpec lv, Table in, const uint64_t* __restrict__ offs, const uint8_t* __restrict__ drv,
     const uint32_t* __restrict__ beg, uint64_t total, uint64_t chunk, Table out,
@@ -398,10 +434,11 @@ __global__ void __launch_bounds__(kJThreads) join_expand_kernel(
   unsigned long long running = 0;
   if (MODE == kModeTableWrite) running = warp_counts[gw];
   if (c0 < c1) {
-    uint64_t r0 = gallop_row(offs, 0, in.n, c0);
-    for (uint64_t base = c0; base < c1; base += 32) {
-      const uint64_t w = base + lane;
-      bool ok = w < c1;
+    SegWalk<SEG> sw(lv, c0);
+    uint64_t r0 = gallop_row(offs, 0, in.n, sw.at());
+    for (uint64_t base = c0; base < c1; base += 32, sw.next()) {
+      const uint64_t w = sw.at() + lane;
+      bool ok = base + lane < c1;
       uint64_t r = r0;
       uint32_t nv[kMaxSrc + 1];  // values of the slots this level binds
 #pragma unroll
@@ -483,7 +520,7 @@ __global__ void __launch_bounds__(kJThreads) join_expand_kernel(
 // Two-source cartesian product (both sources bind one variable): per row the
 // count pass stored list 0's begin and list 1's [begin, length); candidate
 // `local` pairs element local / len1 of list 0 with local % len1 of list 1.
-template <int MODE>
+template <int MODE, bool SEG>
 __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
     LevelSpec lv, Table in, const uint64_t* __restrict__ offs, const uint32_t* __restrict__ beg,
     const uint2* __restrict__ orange, uint64_t total, uint64_t chunk, Table out,
@@ -498,11 +535,14 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
   const int s0 = lv.src[0].out_slot, s1 = lv.src[1].out_slot;
   unsigned long long running = 0;
   if (MODE == kModeTableWrite) running = warp_counts[gw];
+  // without filters every candidate is written at its own index
+  if (MODE == kModeKeys && lv.nfilt == 0 && gw == 0 && lane == 0) *d_out_n = total;
   if (c0 < c1) {
-    uint64_t r0 = gallop_row(offs, 0, in.n, c0);
-    for (uint64_t base = c0; base < c1; base += 32) {
-      const uint64_t w = base + lane;
-      bool ok = w < c1;
+    SegWalk<SEG> sw(lv, c0);
+    uint64_t r0 = gallop_row(offs, 0, in.n, sw.at());
+    for (uint64_t base = c0; base < c1; base += 32, sw.next()) {
+      const uint64_t w = sw.at() + lane;
+      bool ok = base + lane < c1;
       uint64_t r = r0;
       uint32_t v0 = 0, v1 = 0;
       if (ok) {
@@ -530,7 +570,7 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
                               : k1 == s0       ? v0
                               : k1 == s1       ? v1
                                                : slot_value(in, k1, r);
-          out_keys[w] = (hi << 32) | lo;
+          out_keys[base + lane] = (hi << 32) | lo;
         }
         r0 = __shfl_sync(kAllLanes, r, 31);
         continue;
@@ -623,9 +663,11 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
   const uint64_t chunk = ((total + warps - 1) / warps + 31) & ~uint64_t(31);
   Table out = out_table ? *out_table : Table{};
   if (lv.kind == kColumnJoin && lv.nsrc == 2 && lv.nfilt == 0) {
-#define SRDL_CJ2(MODE, WC) \
-  join_cj2_kernel<MODE><<<g, kJThreads, 0, L.stream>>>(lv, in, w.offs, w.drv, w.beg, w.orange, \
-                                                       w.obm, total, chunk, out, out_keys, cnt, WC)
+#define SRDL_CJ2(MODE, WC)                                                                   \
+  (lv.seg ? join_cj2_kernel<MODE, true><<<g, kJThreads, 0, L.stream>>>(                       \
+                lv, in, w.offs, w.drv, w.beg, w.orange, w.obm, total, chunk, out, out_keys, cnt, WC) \
+          : join_cj2_kernel<MODE, false><<<g, kJThreads, 0, L.stream>>>(                      \
+                lv, in, w.offs, w.drv, w.beg, w.orange, w.obm, total, chunk, out, out_keys, cnt, WC))
     if (lv.emit == kEmitCount) {
       SRDL_CJ2(kModeCount, nullptr);
       count_launches(1);
@@ -647,15 +689,15 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
     return;
   }
   if (lv.kind == kCartesian && lv.nsrc == 2 && lv.src[0].out_slot >= 0 && lv.src[1].out_slot >= 0) {
-#define SRDL_CART2(MODE, WC) \
-  join_cart2_kernel<MODE><<<g, kJThreads, 0, L.stream>>>(lv, in, w.offs, w.beg, w.orange, total, \
-                                                         chunk, out, out_keys, cnt, WC)
+#define SRDL_CART2(MODE, WC)                                                                 \
+  (lv.seg ? join_cart2_kernel<MODE, true><<<g, kJThreads, 0, L.stream>>>(                     \
+                lv, in, w.offs, w.beg, w.orange, total, chunk, out, out_keys, cnt, WC)          \
+          : join_cart2_kernel<MODE, false><<<g, kJThreads, 0, L.stream>>>(                    \
+                lv, in, w.offs, w.beg, w.orange, total, chunk, out, out_keys, cnt, WC))
     if (lv.emit == kEmitCount) {
       SRDL_CART2(kModeCount, nullptr);
       count_launches(1);
     } else if (lv.emit == kEmitKeys) {
-      if (lv.nfilt == 0)  // every candidate is written at its own index
-        SRDL_CUDA(cudaMemcpyAsync(d_out_n, w.offs + in.n, 8, cudaMemcpyDeviceToDevice, L.stream));
       SRDL_CART2(kModeKeys, nullptr);
       count_launches(1);
     } else {
@@ -672,26 +714,28 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
     SRDL_CUDA(cudaGetLastError());
     return;
   }
+#define SRDL_EXP(MODE, WC)                                                                    \
+  (lv.seg ? join_expand_kernel<MODE, true><<<g, kJThreads, 0, L.stream>>>(                       \
+                lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, WC)              \
+          : join_expand_kernel<MODE, false><<<g, kJThreads, 0, L.stream>>>(                      \
+                lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, WC))
   if (lv.emit == kEmitCount) {
-    join_expand_kernel<kModeCount><<<g, kJThreads, 0, L.stream>>>(
-        lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, nullptr);
+    SRDL_EXP(kModeCount, nullptr);
     count_launches(1);
   } else if (lv.emit == kEmitKeys) {
-    join_expand_kernel<kModeKeys><<<g, kJThreads, 0, L.stream>>>(
-        lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, nullptr);
+    SRDL_EXP(kModeKeys, nullptr);
     count_launches(1);
   } else {
     uint64_t* wc = s.take<uint64_t>(warps + 1);
     uint64_t* wo = s.take<uint64_t>(warps + 1);
-    join_expand_kernel<kModeTableCount><<<g, kJThreads, 0, L.stream>>>(
-        lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, wc);
+    SRDL_EXP(kModeTableCount, wc);
     SRDL_CUDA(cudaGetLastError());
     exclusive_scan_u64(L, wc, warps, wo, s);
     SRDL_CUDA(cudaMemcpyAsync(d_out_n, wo + warps, 8, cudaMemcpyDeviceToDevice, L.stream));
-    join_expand_kernel<kModeTableWrite><<<g, kJThreads, 0, L.stream>>>(
-        lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, wo);
+    SRDL_EXP(kModeTableWrite, wo);
     count_launches(2);
   }
+#undef SRDL_EXP
   SRDL_CUDA(cudaGetLastError());
 }
 

@@ -146,6 +146,9 @@ struct FiltSpec {
   // tuple (a) -- or (a, b) when b_slot >= 0 -- is not a key prefix of `neg`.
   bool negation = false;
   TrieView neg;
+  // Shard filter: keep the binding iff shard_owner(a, shard_world) == b_const
+  // (0: not a shard filter).
+  uint32_t shard_world = 0;
 };
 
 struct LevelSpec {
@@ -165,6 +168,10 @@ struct LevelSpec {
   const uint32_t* grp_bounds = nullptr;  // n_groups + 1 sorted entries
   uint32_t n_groups = 0;
   unsigned long long* grp_counts = nullptr;
+  // Sharded work: expand only segments seg_rank, seg_rank + seg_world, ...
+  // of `seg` work items each (seg a multiple of 32; 0: every item).
+  uint64_t seg = 0;
+  uint32_t seg_world = 1, seg_rank = 0;
 };
 
 struct Table {
@@ -187,14 +194,24 @@ struct JoinWork {
 };
 JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scratch& s);
 
-// Pass 2: expands `total` work items; surviving bindings are appended to
-// `out_table` (emit table, in input order: the table stays sorted), to
-// `out_keys` (emit keys, any order) or counted (emit count) via *d_out_n,
-// which the caller zeroes.  Output capacity = total.
+// Pass 2: expands `total` work items (all of the count pass's items, or
+// with lv.seg set this shard's segments of them, total = seg_owned(...));
+// surviving bindings are appended to `out_table` (emit table, in input
+// order: the table stays sorted), to `out_keys` (emit keys, any order) or
+// counted (emit count) via *d_out_n, which the caller zeroes.  Output
+// capacity = total.
 size_t join_expand_scratch_bytes(int num_sms);
 void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const JoinWork& w,
                  uint64_t total, Table* out_table, uint64_t* out_keys, uint64_t* d_out_n,
                  Scratch& s);
+
+// Work items of shard `rank` among `world` when `total` items are dealt out
+// in segments of `seg` (segment i goes to shard i mod world).
+inline uint64_t seg_owned(uint64_t total, uint64_t seg, uint64_t world, uint64_t rank) {
+  const uint64_t round = seg * world, full = total / round, rem = total - full * round;
+  const uint64_t lo = rank * seg;
+  return full * seg + (rem > lo ? (rem - lo < seg ? rem - lo : seg) : 0);
+}
 
 
 }  // namespace srdl

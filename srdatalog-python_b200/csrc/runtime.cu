@@ -265,6 +265,17 @@ void Database::parse_plan(const std::string& plan_json) {
         op.kind = Op::Execute;
         op.rule = oj.at("rule").s();
         op.count = oj.at("count").flag();
+        if (oj.has("shard")) {
+          const std::string sh = oj.at("shard").s();
+          if (sh == "work") {
+            op.shard = Op::Work;
+          } else if (sh == "key") {
+            op.shard = Op::Key;
+            op.shard_var = oj.at("shard_var").s();
+          } else {
+            SRDL_REQUIRE(sh.empty(), kErrPlan, "rule " + op.rule + ": unknown shard mode " + sh);
+          }
+        }
         for (auto& pj : oj.at("pipeline").a()) {
           PipeOp po;
           const std::string pk = pj.at("op").s();
@@ -778,6 +789,10 @@ void Database::set_option(const std::string& name, int64_t value) {
   if (name == "bitmap_mb") opt_bitmap_mb_ = value;
   else if (name == "hash_min") opt_hash_min_ = value;
   else if (name == "lsm_compact_pct") opt_lsm_pct_ = value;
+  else if (name == "shard_world") {
+    SRDL_REQUIRE(value >= 1 && value <= 65536, kErrArg, "set_option: shard_world out of [1, 65536]");
+    shard_world_ = value;
+  } else if (name == "shard_rank") shard_rank_ = value;
   else throw Error{kErrArg, "set_option: unknown option " + name};
 }
 

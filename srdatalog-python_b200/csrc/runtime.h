@@ -155,6 +155,13 @@ struct Op {
   std::vector<int> index, source_index;
   bool count = false;
   std::vector<PipeOp> pipeline;
+  // Sharding of a rule when the database is one of several shards:
+  //   Work: the last level's work items are split evenly; this shard expands
+  //         its contiguous window (count-only rules over replicated inputs);
+  //   Key : only bindings whose `shard_var` value this shard owns
+  //         (shard_owner) are kept, filtered where the variable is bound.
+  enum Shard { NoShard, Work, Key } shard = NoShard;
+  std::string shard_var;
 };
 
 struct Step {
@@ -248,6 +255,7 @@ class Database {
   int64_t opt_bitmap_mb_ = -1;      // -1: SRDL_BITMAP_MB or the default
   int64_t opt_hash_min_ = -1;       // -1: SRDL_HASH_MIN or off
   int64_t opt_lsm_pct_ = 10;        // HEAD -> FULL merge threshold (% of FULL)
+  int64_t shard_rank_ = 0, shard_world_ = 1;  // this database's shard among shard_world_
   struct KEvent {
     std::string name;
     cudaEvent_t a, b;
