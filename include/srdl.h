@@ -83,9 +83,19 @@ int srdl_set_profiling(srdl_db* db, int enable);
  *   "lsm_compact_pct"  Device2LevelIndex: merge HEAD into FULL once HEAD
  *                      exceeds this percentage of FULL (default 10, the
  *                      reference's kCompactRatio, device_2level_index.h:300)
+ *   "shard_world",     evaluate as shard "shard_rank" of "shard_world"
+ *   "shard_rank"       (default 0 of 1): rules the plan marks
+ *                      "shard": "key" keep only bindings whose "shard_var"
+ *                      value v has owner(v) = ((v * 0x9E3779B1) mod 2^32)
+ *                      * world >> 32 equal to the rank; rules marked
+ *                      "shard": "work" expand only this shard's interleaved
+ *                      segments of one join level's work items.  The marks
+ *                      come from srdatalog_b200.shard.shard_plan; results
+ *                      of the shards add up to the unsharded result.
+ *                      srdl_run fails with status 1 if rank >= world.
  * Unknown names return 1 (argument error); negative values are rejected.
  * No reference counterpart: the reference fixes these at code-generation
- * time. */
+ * time and evaluates on one GPU. */
 int srdl_set_option(srdl_db* db, const char* name, int64_t value);
 
 /* Kernels this process has launched through libsrdl so far. */
