@@ -118,6 +118,29 @@ def test_set_difference(na, nb):
   assert np.array_equal(gpu_diff(a, b), oracle.set_difference(a, b))
 
 
+def test_set_difference_many_tiles():
+  '''40M - 24M keys built on the device: ~31K merged tiles whose output
+  offsets chain through the look-back of every block of the grid; checked
+  against torch.isin on the device.'''
+  lib = native.lib()
+  g = torch.Generator(device='cuda').manual_seed(5)
+  a = torch.unique(torch.randint(0, 1 << 40, (40_000_000,), device='cuda', generator=g))
+  extra = torch.randint(0, 1 << 40, (8_000_000,), device='cuda', generator=g)
+  b = torch.unique(torch.cat([a[::3], extra]))
+  out = torch.empty_like(a)
+  d_n = torch.full((1,), -1, dtype=torch.int64, device='cuda')
+  sb = lib.srdl_set_difference_scratch_bytes(a.numel())
+  scratch = torch.empty(sb, dtype=torch.uint8, device='cuda')
+  rc = lib.srdl_set_difference_u64(a.data_ptr(), a.numel(), b.data_ptr(), b.numel(), out.data_ptr(),
+                                   d_n.data_ptr(), scratch.data_ptr(), sb, stream())
+  assert rc == 0, native.last_error()
+  torch.cuda.synchronize()
+  want = a[~torch.isin(a, b)]
+  n = int(d_n.item())
+  assert n == want.numel()
+  assert torch.equal(out[:n], want)
+
+
 @pytest.mark.parametrize('na,nb', [(0, 0), (0, 10), (10, 0), (1, 1), (2047, 1), (3_000_000, 1000),
                                    (123_457, 98_765)])
 def test_merge_disjoint(na, nb):
