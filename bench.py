@@ -399,13 +399,19 @@ def main():
 
   import torch
   dist = None
+  # SRDL_BENCH_BACKEND=gloo runs the collectives on the host (several ranks
+  # can then share one GPU to exercise the N > 1 path; their kernels never
+  # wait on one another); timings are only meaningful with nccl.
+  backend = os.environ.get('SRDL_BENCH_BACKEND', 'nccl')
+  local = local % max(1, torch.cuda.device_count())
   if world > 1:
     import datetime
 
     import torch.distributed as dist
     torch.cuda.set_device(local)
-    dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
   dev = torch.device('cuda', local)
+  coll = dev if backend == 'nccl' else torch.device('cpu')  # where collective tensors live
   torch.cuda.set_device(dev)
 
   from srdatalog_b200 import Database, native
@@ -440,7 +446,7 @@ def main():
   def job_units(d) -> int:
     # the job's result: a sharded relation's or count's parts add up
     u = result_units(d, wl)
-    return sum_over_ranks(u, dist, dev) if sharded else u
+    return sum_over_ranks(u, dist, coll) if sharded else u
 
   # ---------------- kernel-resident path (value)
   d_edges = torch.from_numpy(edges.view(np.int32).reshape(-1)).to(dev)
@@ -490,7 +496,7 @@ def main():
   if dist:
     dist.barrier()
   total_ms = sum(step_ms)
-  total_ms = max_over_ranks(total_ms, dist, dev)
+  total_ms = max_over_ranks(total_ms, dist, coll)
   # sharded: per_step is already the whole job's; replicas: one per rank
   copies = 1 if sharded else world
   value = replica_throughput(per_step, args.steps, copies, total_ms)
@@ -525,7 +531,7 @@ def main():
     if batched:  # every instance's size read back
       per_inst = db2.range_counts(wl['out'], bounds)
       if sharded:
-        t = torch.from_numpy(per_inst.astype(np.int64)).to(dev)
+        t = torch.from_numpy(per_inst.astype(np.int64)).to(coll)
         dist.all_reduce(t)
         per_inst = t.cpu().numpy()
     ev1.record(stream)
@@ -533,7 +539,7 @@ def main():
     e2e_ms.append(ev0.elapsed_time(ev1))
     assert got == units
   e2e_total = sum(e2e_ms)
-  e2e_total = max_over_ranks(e2e_total, dist, dev)
+  e2e_total = max_over_ranks(e2e_total, dist, coll)
   db2.close()
   plain = None
   if batched and not args.no_cpu_baseline:
