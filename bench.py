@@ -11,12 +11,13 @@ value : tuples/s with the input already in HBM (srdl_load_device_rows),
         CUDA events on the database stream, L2 flushed between steps.
 e2e   : same metric through the C ABI from pinned host rows (srdl_load_rows
         + srdl_run, which uploads them), result read back to the host.
-Multi-GPU (torchrun): one program sharded over the GPUs when its plan
-allows it (srdatalog_b200.shard: the triangle count splits its last join
-level's work items, TC partitions Path by source; inputs replicated, one
-final all-reduce of the result), value = the job's tuples over the max
-per-rank time (strong scaling); plans that would need a per-iteration
-exchange (SG) run as independent replicas (weak scaling).
+Multi-GPU (torchrun): one program sharded over the GPUs
+(srdatalog_b200.shard: the triangle count splits a join level's work
+items, TC partitions Path by source, SG partitions Sg and sends each
+iteration's derived tuples to their owners with one all-to-all; inputs
+replicated, one final all-reduce of the result), value = the job's tuples
+over the max per-rank time (strong scaling); plans the analysis cannot
+shard run as independent replicas (weak scaling).
 --impl reference: the CPU restatement of the reference's evaluation on
 the host cores, on a bounded sample of the same workload.
 '''
@@ -415,7 +416,7 @@ def main():
   torch.cuda.set_device(dev)
 
   from srdatalog_b200 import Database, native
-  from srdatalog_b200.shard import shard_plan
+  from srdatalog_b200.shard import TorchExchange, shard_plan
   wl = WORKLOADS[args.workload]
   plan = load_plan(wl['plan'])
   edges = make_edges(args.workload)
@@ -431,6 +432,9 @@ def main():
   sharded = bool(spec and spec.useful)
   if sharded:
     plan = spec.plan
+  # plans whose recursive rules derive other shards' tuples send them there
+  # every iteration (all_to_all over the process group)
+  xch = TorchExchange() if sharded and spec.exchanged else None
   stream = torch.cuda.current_stream(dev)
 
   def open_db():
@@ -440,6 +444,8 @@ def main():
     if sharded:
       d.set_option('shard_world', world)
       d.set_option('shard_rank', rank)
+      if xch:
+        d.set_exchange(xch.callback(rank))
     d.set_stream(stream.cuda_stream)
     return d
 

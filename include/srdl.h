@@ -98,6 +98,32 @@ int srdl_set_profiling(srdl_db* db, int enable);
  * time and evaluates on one GPU. */
 int srdl_set_option(srdl_db* db, const char* name, int64_t value);
 
+/* Exchange of derived tuples between shards (plans marked by
+ * srdatalog_b200.shard.shard_plan carry "exchange" ops where a recursive
+ * rule derives tuples keyed by another shard's values).  With shard_world
+ * > 1, an exchange op partitions the relation's NEW tuples by the owner of
+ * their first declared column and calls fn three ways:
+ *   phase 0  counts[0..world) in: keys this shard sends to each shard;
+ *            out: keys it receives from each shard;
+ *   phase 1  d_send: the keys grouped by destination shard (ascending;
+ *            uint64 in the relation's canonical index order), d_recv: room
+ *            for the received keys, grouped by source shard; the transfer
+ *            must be complete when fn returns;
+ *   phase 2  (once per recursive iteration, before deciding to stop)
+ *            counts[0] in: this shard's new-delta size; out: the sum over
+ *            all shards.
+ * `stream` is the database's cudaStream_t (synchronised before phase 1).
+ * fn returns 0 on success; anything else fails the run (status 2).
+ * fn = NULL removes it.  No reference counterpart. */
+typedef int (*srdl_exchange_fn)(void* user, int phase, const char* rel, uint64_t* counts,
+                                const uint64_t* d_send, uint64_t* d_recv, void* stream);
+int srdl_set_exchange(srdl_db* db, srdl_exchange_fn fn, void* user);
+
+/* Stream-ordered device copy (any direction under unified addressing),
+ * complete on return: for exchange callbacks that move keys between
+ * buffers the caller owns. */
+int srdl_copy_device(void* dst, const void* src, uint64_t bytes, void* stream);
+
 /* Kernels this process has launched through libsrdl so far. */
 uint64_t srdl_launch_count(void);
 

@@ -195,6 +195,22 @@ int srdl_set_option(srdl_db* h, const char* name, int64_t value) {
   SRDL_GUARD(0, h->db->set_option(name, value); return 0;)
 }
 
+int srdl_set_exchange(srdl_db* h, srdl_exchange_fn fn, void* user) {
+  if (!h) return kErrArg;
+  SRDL_GUARD(0, h->db->set_exchange(fn, user); return 0;)
+}
+
+int srdl_copy_device(void* dst, const void* src, uint64_t bytes, void* stream) {
+  if ((!dst || !src) && bytes) return kErrArg;
+  SRDL_GUARD(0, {
+    if (bytes) {
+      SRDL_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, (cudaStream_t)stream));
+      SRDL_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    }
+    return 0;
+  })
+}
+
 int srdl_set_count_groups(srdl_db* h, const char* rule, const uint32_t* bounds,
                           uint64_t n_bounds) {
   if (!h || !rule) return kErrArg;

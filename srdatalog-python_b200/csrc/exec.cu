@@ -491,6 +491,74 @@ void Database::op_merge(const Op& op) {
   r.v[kFull].idx[op.index] = std::move(m);
 }
 
+uint64_t Database::shards_sum(uint64_t local) {
+  std::vector<uint64_t> c((size_t)shard_world_, 0);
+  c[0] = local;
+  SRDL_REQUIRE(xfn_(xuser_, 2, "", c.data(), nullptr, nullptr, (void*)L_.stream) == 0, kErrState,
+               "exchange callback failed (convergence vote)");
+  return c[0];
+}
+
+// Sends the relation's NEW tuples to the shards that own their first
+// declared column and keeps the ones received (one NEW chunk, canonical
+// order).  Nothing to do on a single shard.
+void Database::op_exchange(const Op& op) {
+  if (shard_world_ <= 1) return;
+  SRDL_REQUIRE(xfn_ != nullptr, kErrState,
+               "plan exchanges tuples of " + op.rel + " between shards: set an exchange callback");
+  Relation& r = rel(op.rel);
+  SRDL_REQUIRE(r.arity <= 2, kErrUnsupported, "exchange of relation " + r.name + " of arity > 2");
+  RelVersion& nv = r.v[kNew];
+  const std::vector<int>& order = r.canonical;
+  uint64_t total = 0;
+  for (auto& c : nv.chunks) total += c.n;
+  // gather NEW in canonical order
+  DevBuf keys(std::max<uint64_t>(total, 1) * 8, L_.stream);
+  uint64_t off = 0;
+  for (auto& c : nv.chunks) {
+    if (!c.n) continue;
+    if (c.order == order)
+      SRDL_CUDA(cudaMemcpyAsync(keys.as<uint64_t>() + off, c.keys.as<uint64_t>(), c.n * 8,
+                                cudaMemcpyDeviceToDevice, L_.stream));
+    else
+      swap_halves(L_, c.keys.as<uint64_t>(), c.n, keys.as<uint64_t>() + off);
+    off += c.n;
+  }
+  nv.chunks.clear();
+  nv.idx.clear();
+  const uint32_t world = (uint32_t)shard_world_;
+  const bool col0_lo = !order.empty() && order[0] != 0;
+  // group the keys by destination shard: one order-preserving selection per shard
+  DevBuf send(std::max<uint64_t>(total, 1) * 8, L_.stream);
+  std::vector<uint64_t> counts(world, 0);
+  if (total) {
+    DevBuf scratch(shard_select_scratch_bytes(total) + 1024, L_.stream);
+    uint64_t acc = 0;
+    for (uint32_t d = 0; d < world; d++) {
+      Scratch s{scratch.as<char>(), scratch.bytes(), 0};
+      shard_select(L_, keys.as<uint64_t>(), total, col0_lo, world, d, send.as<uint64_t>() + acc,
+                   d_small_.as<uint64_t>(), s);
+      counts[d] = read_scalar(0);
+      acc += counts[d];
+    }
+    SRDL_REQUIRE(acc == total, kErrState, "exchange: keys lost while grouping by shard");
+  }
+  std::vector<uint64_t> io = counts;
+  SRDL_REQUIRE(xfn_(xuser_, 0, r.name.c_str(), io.data(), nullptr, nullptr, (void*)L_.stream) == 0,
+               kErrState, "exchange callback failed (counts of " + r.name + ")");
+  uint64_t recv = 0;
+  for (uint64_t v : io) recv += v;
+  Chunk ch;
+  ch.order = order;
+  ch.keys = DevBuf(std::max<uint64_t>(recv, 1) * 8, L_.stream);
+  ch.n = recv;
+  SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  SRDL_REQUIRE(xfn_(xuser_, 1, r.name.c_str(), io.data(), send.as<uint64_t>(),
+                    ch.keys.as<uint64_t>(), (void*)L_.stream) == 0,
+               kErrState, "exchange callback failed (tuples of " + r.name + ")");
+  nv.chunks.push_back(std::move(ch));
+}
+
 static const char* op_kind_name(Op::Kind k) {
   switch (k) {
     case Op::Execute: return "execute_pipeline";
@@ -502,6 +570,7 @@ static const char* op_kind_name(Op::Kind k) {
     case Op::RebuildFrom: return "rebuild_index_from";
     case Op::Reconstruct: return "reconstruct";
     case Op::Hook: return "inject_cpp_hook";
+    case Op::Exchange: return "exchange";
   }
   return "other";
 }
@@ -534,6 +603,7 @@ void Database::exec_ops(const Step& st, uint64_t it) {
       case Op::RebuildFrom: ensure_index(rel(op.rel), op.ver, op.index); break;
       case Op::Reconstruct: break;
       case Op::Hook: break;
+      case Op::Exchange: op_exchange(op); break;
     }
   }
 }
@@ -572,6 +642,8 @@ void Database::run(uint64_t max_iters) {
               total += kv.second.n;
               break;
             }
+          // sharded with exchanges: stop only when every shard's delta is empty
+          if (xfn_ && shard_world_ > 1) total = shards_sum(total);
           if (total == 0) break;
         }
         exec_ops(st, it);

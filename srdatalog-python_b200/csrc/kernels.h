@@ -115,6 +115,13 @@ void child_hash_build(const Launch& L, const uint64_t* keys, uint64_t n, const u
 void bounds_positions(const Launch& L, const uint64_t* keys, uint64_t n, const uint32_t* bounds,
                       uint64_t n_bounds, uint64_t* pos);
 
+// Keys whose first declared column (the key's low word when `col0_lo`, else
+// its high word) is owned by shard `dest` of `world` (shard_owner), in
+// order, to out; their count to *d_nout.
+size_t shard_select_scratch_bytes(uint64_t n);
+void shard_select(const Launch& L, const uint64_t* keys, uint64_t n, bool col0_lo, uint32_t world,
+                  uint32_t dest, uint64_t* out, uint64_t* d_nout, Scratch& s);
+
 // Swap the two 32-bit halves of every key (index permutation (1,0) <-> (0,1)).
 void swap_halves(const Launch& L, const uint64_t* in, uint64_t n, uint64_t* out);
 

@@ -273,7 +273,10 @@ void Database::parse_plan(const std::string& plan_json) {
             op.shard = Op::Key;
             op.shard_var = oj.at("shard_var").s();
           } else {
-            SRDL_REQUIRE(sh.empty(), kErrPlan, "rule " + op.rule + ": unknown shard mode " + sh);
+            // "exchange": the rule runs unrestricted, its tuples go to their
+            // owners by the exchange op that follows it
+            SRDL_REQUIRE(sh.empty() || sh == "exchange", kErrPlan,
+                         "rule " + op.rule + ": unknown shard mode " + sh);
           }
         }
         for (auto& pj : oj.at("pipeline").a()) {
@@ -334,6 +337,8 @@ void Database::parse_plan(const std::string& plan_json) {
         } else if (k == "merge_index") {
           op.kind = Op::Merge;
           op.index = oj.at("index").ints();
+        } else if (k == "exchange") {
+          op.kind = Op::Exchange;
         } else if (k == "rebuild_index_from_index") {
           op.kind = Op::RebuildFrom;
           op.ver = parse_ver(oj.at("ver").s());

@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 
+#include "../../include/srdl.h"
 #include "json.h"
 #include "kernels.h"
 
@@ -149,7 +150,8 @@ struct PipeOp {
 struct Op {
   // Hook: an injected C++ hook of the reference (mir/types.py:358), kept in
   // the plan and skipped (there is no C++ code generation here).
-  enum Kind { Execute, Rebuild, Clear, CheckSize, ComputeDelta, Merge, RebuildFrom, Reconstruct, Hook } kind;
+  // Exchange: send NEW tuples to the shards owning their first column.
+  enum Kind { Execute, Rebuild, Clear, CheckSize, ComputeDelta, Merge, RebuildFrom, Reconstruct, Hook, Exchange } kind;
   std::string rel, rule;
   Ver ver = kFull;
   std::vector<int> index, source_index;
@@ -214,6 +216,10 @@ class Database {
   void set_stream(cudaStream_t s);
   void set_profiling(bool on) { profile_ = on; }
   void set_option(const std::string& name, int64_t value);
+  void set_exchange(srdl_exchange_fn fn, void* user) {
+    xfn_ = fn;
+    xuser_ = user;
+  }
   void load_csv(const std::string& rel, const std::string& path);
   void load_all(const std::string& dir);
   void run(uint64_t max_iters);
@@ -256,6 +262,8 @@ class Database {
   int64_t opt_hash_min_ = -1;       // -1: SRDL_HASH_MIN or off
   int64_t opt_lsm_pct_ = 10;        // HEAD -> FULL merge threshold (% of FULL)
   int64_t shard_rank_ = 0, shard_world_ = 1;  // this database's shard among shard_world_
+  srdl_exchange_fn xfn_ = nullptr;  // moves tuples between shards (exchange ops)
+  void* xuser_ = nullptr;
   struct KEvent {
     std::string name;
     cudaEvent_t a, b;
@@ -297,6 +305,9 @@ class Database {
   void op_rebuild(const Step& st, size_t pos, const Op& op);
   void op_compute_delta(const Op& op);
   void op_merge(const Op& op);
+  void op_exchange(const Op& op);
+  // Sum of a count over all shards (the exchange callback's phase 2).
+  uint64_t shards_sum(uint64_t local);
 };
 
 std::vector<int> identity_perm(int arity);

@@ -192,6 +192,32 @@ void swap_halves(const Launch& L, const uint64_t* in, uint64_t n, uint64_t* out)
   count_launches(1);
 }
 
+// ---- partition by owning shard (exchange ops) --------------------------------
+
+// Keeps the keys whose first declared column (the key's low word when
+// `col0_lo`, else its high word) belongs to shard `dest`; order-preserving.
+struct OwnerSel {
+  const uint64_t* keys;
+  uint64_t* out;
+  bool col0_lo;
+  uint32_t world, dest;
+  __device__ void block_setup(uint64_t, uint64_t) {}
+  __device__ bool select(uint64_t i) const {
+    const uint64_t k = keys[i];
+    return shard_owner(col0_lo ? (uint32_t)k : (uint32_t)(k >> 32), world) == dest;
+  }
+  __device__ void emit(uint64_t i, uint64_t pos) const { out[pos] = keys[i]; }
+};
+
+size_t shard_select_scratch_bytes(uint64_t n) { return cp_scratch_bytes(n); }
+
+void shard_select(const Launch& L, const uint64_t* keys, uint64_t n, bool col0_lo, uint32_t world,
+                  uint32_t dest, uint64_t* out, uint64_t* d_nout, Scratch& s) {
+  SRDL_REQUIRE(world >= 1 && dest < world, kErrArg, "shard_select: destination out of range");
+  OwnerSel sel{keys, out, col0_lo, world, dest};
+  compact(L, sel, n, d_nout, s);
+}
+
 __global__ void hash_size_kernel(const uint32_t* __restrict__ dir, uint32_t nv, uint32_t min_len,
                                  uint64_t* __restrict__ sizes) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < nv;

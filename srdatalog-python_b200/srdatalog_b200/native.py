@@ -22,6 +22,10 @@ _vp = ctypes.c_void_p
 _cp = ctypes.c_char_p
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 
+# srdl_exchange_fn: (user, phase, rel, counts, d_send, d_recv, stream) -> int
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, _vp, ctypes.c_int, _cp, ctypes.POINTER(_u64), _vp, _vp,
+                               _vp)
+
 # name -> (restype, argtypes); mirrors include/srdl.h
 SIGNATURES = {
   'srdl_last_error': (_cp, []),
@@ -54,6 +58,8 @@ SIGNATURES = {
   'srdl_sort_unique_u64_noalloc': (ctypes.c_int, [_vp, _u64, ctypes.c_int, _vp, _vp, _vp]),
   'srdl_sort_unique_noalloc_max_keys': (_u64, []),
   'srdl_set_option': (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64]),
+  'srdl_set_exchange': (ctypes.c_int, [_vp, EXCHANGE_FN, _vp]),
+  'srdl_copy_device': (ctypes.c_int, [_vp, _vp, _u64, _vp]),
 }
 
 _LIB = None
@@ -143,6 +149,28 @@ class Database:
   def set_profiling(self, on: bool = True) -> None:
     check(lib().srdl_set_profiling(self._h, 1 if on else 0), 'srdl_set_profiling')
 
+  def set_exchange(self, fn) -> None:
+    '''fn(phase, rel, counts, send_ptr, recv_ptr, stream_ptr) moves tuples
+    between shards (see srdl_set_exchange); counts is a ctypes uint64 array
+    of shard_world entries, updated in place.  An exception inside fn fails
+    the run.  None removes it.'''
+    if fn is None:
+      self._xfn = None
+      check(lib().srdl_set_exchange(self._h, EXCHANGE_FN(), None), 'srdl_set_exchange')
+      return
+
+    def tramp(_user, phase, rel, counts, send, recv, stream):
+      try:
+        fn(int(phase), rel.decode() if rel else '', counts, send or 0, recv or 0, stream or 0)
+        return 0
+      except Exception as e:  # reported through the run's error
+        self._xerr = e
+        return 1
+
+    self._xerr = None
+    self._xfn = EXCHANGE_FN(tramp)  # kept alive with the handle
+    check(lib().srdl_set_exchange(self._h, self._xfn, None), 'srdl_set_exchange')
+
   def set_option(self, name: str, value: int) -> None:
     '''Tuning option (srdl_set_option): bitmap_mb, hash_min, lsm_compact_pct.'''
     check(lib().srdl_set_option(self._h, name.encode(), int(value)), 'srdl_set_option')
@@ -176,7 +204,12 @@ class Database:
     return int(lib().srdl_staged_rows(self._h, rel.encode()))
 
   def run(self, max_iters: int = 0) -> None:
-    check(lib().srdl_run(self._h, max_iters), 'srdl_run')
+    rc = lib().srdl_run(self._h, max_iters)
+    xerr = getattr(self, '_xerr', None)
+    if rc and xerr is not None:
+      self._xerr = None
+      raise SrdlError('srdl_run', rc, f'exchange callback raised {xerr!r}') from xerr
+    check(rc, 'srdl_run')
 
   def size(self, rel: str) -> int:
     return int(lib().srdl_size(self._h, rel.encode()))

@@ -22,18 +22,31 @@ every rule keeps the partition key in place:
 * a relation derived only from replicated relations, outside recursion,
   stays replicated (every shard computes it; cheap loads like TC's Edge).
 
-Plans in which a recursive rule moves the key (same generation:
-``SG(x,y) <= Edge(a,x), SG(a,b), Edge(b,y)`` reads SG keyed by a but derives
-keys x) would need an exchange of deltas every iteration; for those
-``shard_plan`` falls back to replicating every relation, and only count-only
-rules are split.  The reference evaluates on one GPU (its multi-node MPI
-code is unused), so this layer has no counterpart there; each shard's
-evaluation is the single-GPU one.
+* a rule whose positive partitioned atoms share one key variable other
+  than the head's (same generation: ``SG(x,y) <= Edge(a,x), SG(a,b),
+  Edge(b,y)`` reads SG keyed by a, derives keys x; left-recursive TC) has its
+  bindings confined to this shard's keys but derives tuples for any shard:
+  the plan gets an ``exchange`` op for the head relation before its NEW
+  version is indexed, which sends every derived tuple to its owner (one
+  all-to-all per iteration), and the fixpoint stops when every shard's
+  delta is empty (one sum per iteration).  The exchange itself is a
+  callback: ``LocalExchange`` for shards run by threads of one process,
+  ``TorchExchange`` for one process per GPU under torch.distributed.
+
+Plans in which one rule reads partitioned relations on two different keys
+(Andersen's ``PointsTo(x,z), PointsTo(z,w)``) would need more than an
+exchange of derived tuples; for those ``shard_plan`` falls back to
+replicating every relation, and only count-only rules are split.  The
+reference evaluates on one GPU (its multi-node MPI code is unused), so this
+layer has no counterpart there; each shard's evaluation is the single-GPU
+one.
 '''
 
 from __future__ import annotations
 
 import copy
+import ctypes
+import threading
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -55,8 +68,9 @@ class ShardSpec:
   plan: dict                                  # the plan with per-rule shard marks
   partitioned: list = field(default_factory=list)  # relations split by column 0
   replicated: list = field(default_factory=list)
-  modes: dict = field(default_factory=dict)   # rule -> 'work' | 'key' | ''
+  modes: dict = field(default_factory=dict)   # rule -> 'work' | 'key' | 'exchange' | ''
   fallback: str = ''                          # why partitioning was given up, if it was
+  exchanged: list = field(default_factory=list)  # relations sent between shards each iteration
 
   @property
   def useful(self) -> bool:
@@ -156,12 +170,39 @@ def _modes(plan: dict, part: set) -> dict:
       modes[op['rule']] = ''
       continue
     k = ins['vars'][0]
-    if keys - {k}:
+    if not atoms or keys == {k}:
+      modes[op['rule']] = '' if positive else ('key', k)
+    elif len(keys) == 1 and None not in keys and positive:
+      # bindings confined to this shard's keys; derived tuples go to their owners
+      modes[op['rule']] = 'exchange'
+    else:
       bad = sorted(str(x) for x in keys - {k})
       raise ShardError(f'rule {op["rule"]} derives {ins["rel"]} keyed by {k} from partitioned '
-                       f'relations keyed by {", ".join(bad)}: needs an exchange per iteration')
-    modes[op['rule']] = '' if positive else ('key', k)
+                       f'relations keyed by {", ".join(bad)}: the join itself needs tuples of '
+                       f'other shards')
   return modes
+
+
+def _insert_exchanges(plan: dict, modes: dict) -> list:
+  '''Adds an exchange op for every relation an 'exchange' rule of a step
+  derives, before the step's first rebuild of its NEW version.'''
+  sent = []
+  for st in plan['steps']:
+    rels = []
+    for op in st['ops']:
+      if op['op'] == 'execute_pipeline' and modes.get(op['rule']) == 'exchange':
+        r = _insert(op)['rel']
+        if r not in rels:
+          rels.append(r)
+    for r in rels:
+      pos = next((i for i, op in enumerate(st['ops']) if op['op'] == 'rebuild_index' and
+                  op['rel'] == r and op.get('ver') == 'NEW'), None)
+      if pos is None:
+        raise ShardError(f'no rebuild of NEW {r} to exchange before')
+      st['ops'].insert(pos, {'op': 'exchange', 'rel': r})
+      if r not in sent:
+        sent.append(r)
+  return sent
 
 
 def shard_plan(plan: dict) -> ShardSpec:
@@ -176,6 +217,7 @@ def shard_plan(plan: dict) -> ShardSpec:
     part = set()
     modes = _modes(plan, part)
   p = copy.deepcopy(plan)
+  sent = _insert_exchanges(p, modes)
   flat = {}
   for _, _, op in _rules(p):
     m = modes[op['rule']]
@@ -190,7 +232,8 @@ def shard_plan(plan: dict) -> ShardSpec:
     else:
       flat[op['rule']] = ''
   return ShardSpec(plan=p, partitioned=[n for n in names if n in part],
-                   replicated=[n for n in names if n not in part], modes=flat, fallback=fallback)
+                   replicated=[n for n in names if n not in part], modes=flat, fallback=fallback,
+                   exchanged=sent)
 
 
 def shard_rows(rows, world: int, rank: int) -> np.ndarray:
@@ -206,14 +249,18 @@ class ShardedDatabase:
   shard `rank` of `world`.  Inputs are loaded in full (replicated); rows
   loaded into a partitioned relation are cut to this shard's part.'''
 
-  def __init__(self, spec: ShardSpec, rank: int, world: int, device: int = 0):
+  def __init__(self, spec: ShardSpec, rank: int, world: int, device: int = 0, exchange=None):
     from .native import Database
     if not 0 <= rank < world:
       raise ValueError(f'rank {rank} outside [0, {world})')
+    if spec.exchanged and world > 1 and exchange is None:
+      raise ValueError(f'plan exchanges {spec.exchanged} between shards: pass exchange=')
     self.spec, self.rank, self.world = spec, rank, world
     self.db = Database(spec.plan, device=device)
     self.db.set_option('shard_world', world)
     self.db.set_option('shard_rank', rank)
+    if exchange is not None:
+      self.db.set_exchange(exchange.callback(rank))
 
   def load_rows(self, rel: str, rows) -> None:
     if rel in self.spec.partitioned:
@@ -240,6 +287,153 @@ class ShardedDatabase:
 
   def __exit__(self, *exc):
     self.close()
+
+
+def _device_copy(dst: int, src: int, nbytes: int, stream: int) -> None:
+  from . import native
+  native.check(native.lib().srdl_copy_device(ctypes.c_void_p(dst), ctypes.c_void_p(src), nbytes,
+                                              ctypes.c_void_p(stream)), 'srdl_copy_device')
+
+
+class LocalExchange:
+  '''Exchange among `world` shards that are run by threads of one process
+  (ShardedDatabase(..., exchange=ex) per thread).  Shards meet at a barrier
+  in every phase; a receiver copies its slices straight out of the senders'
+  buffers (peer copies when the shards sit on different GPUs of the
+  process).  `copy(dst, src, nbytes, stream)` may replace the device copy.
+  A shard whose run fails should call abort(), so the others stop waiting.'''
+
+  def __init__(self, world: int, timeout: float = 600.0, copy=None):
+    self.world = world
+    self.barrier = threading.Barrier(world, timeout=timeout)
+    self.slots: list = [None] * world
+    self.sent: list = [None] * world  # each shard's send counts of the current exchange
+    self.copy = copy or _device_copy
+
+  def abort(self) -> None:
+    self.barrier.abort()
+
+  def callback(self, rank: int):
+    w = self.world
+
+    def fn(phase, rel, counts, send, recv, stream):
+      if phase == 0:    # counts: sent to each shard -> received from each shard
+        self.sent[rank] = [int(counts[i]) for i in range(w)]
+        self.barrier.wait()
+        for src in range(w):
+          counts[src] = self.sent[src][rank]
+        self.barrier.wait()
+      elif phase == 1:  # move the keys: my slice of every sender's buffer, in sender order
+        self.slots[rank] = (send, list(self.sent[rank]))
+        self.barrier.wait()
+        pos = 0
+        for src in range(w):
+          sptr, scounts = self.slots[src]
+          n = scounts[rank]
+          if n:
+            self.copy(recv + 8 * pos, sptr + 8 * sum(scounts[:rank]), 8 * n, stream)
+          pos += n
+        self.barrier.wait()  # senders keep their buffers until every slice is copied
+      elif phase == 2:  # convergence vote
+        self.slots[rank] = int(counts[0])
+        self.barrier.wait()
+        counts[0] = sum(self.slots)
+        self.barrier.wait()
+      else:
+        raise ValueError(f'unknown exchange phase {phase}')
+
+    return fn
+
+
+class TorchExchange:
+  '''Exchange for one process per GPU under torch.distributed: counts and
+  keys move with all_to_all_single (NCCL moves device tensors, gloo host
+  ones), the vote is an all_reduce.  The engine's buffers are copied into
+  and out of torch tensors on the database's stream.'''
+
+  def __init__(self, group=None, copy=None):
+    import torch.distributed as dist
+    self.dist = dist
+    self.group = group
+    self.copy = copy or _device_copy
+
+  def _device(self):
+    import torch
+    if self.dist.get_backend(self.group) == 'nccl':
+      return torch.device('cuda', torch.cuda.current_device())
+    return torch.device('cpu')
+
+  def callback(self, rank: int):
+    import torch
+    dist = self.dist
+    w = dist.get_world_size(self.group)
+    state = {}
+
+    def fn(phase, rel, counts, send, recv, stream):
+      dev = self._device()
+      if phase == 0:
+        sent = torch.tensor([int(counts[i]) for i in range(w)], dtype=torch.int64, device=dev)
+        got = torch.empty_like(sent)
+        dist.all_to_all_single(got, sent, group=self.group)
+        state['sent'] = [int(x) for x in sent.tolist()]
+        state['got'] = [int(x) for x in got.tolist()]
+        for i in range(w):
+          counts[i] = state['got'][i]
+      elif phase == 1:
+        ns, nr = sum(state['sent']), sum(state['got'])
+        src = torch.empty(max(ns, 1), dtype=torch.int64, device=dev)
+        dst = torch.empty(max(nr, 1), dtype=torch.int64, device=dev)
+        if ns:
+          self.copy(src.data_ptr(), send, 8 * ns, stream)
+        dist.all_to_all_single(dst[:nr], src[:ns], output_split_sizes=state['got'],
+                               input_split_sizes=state['sent'], group=self.group)
+        if dev.type == 'cuda':
+          torch.cuda.current_stream(dev).synchronize()
+        if nr:
+          self.copy(recv, dst.data_ptr(), 8 * nr, stream)
+      elif phase == 2:
+        t = torch.tensor([int(counts[0])], dtype=torch.int64, device=dev)
+        dist.all_reduce(t, group=self.group)
+        counts[0] = int(t.item())
+      else:
+        raise ValueError(f'unknown exchange phase {phase}')
+
+    return fn
+
+
+def run_local_shards(spec: ShardSpec, world: int, inputs: dict, device=0, max_iters: int = 0,
+                     exchange: LocalExchange | None = None) -> list:
+  '''Runs the `world` shards of `spec` in threads of this process (shard r
+  on device[r] when `device` is a list, else all on one device) and returns
+  the open ShardedDatabase of every shard (the caller reads and closes
+  them).  Exchanges, if the plan has any, go through a LocalExchange.'''
+  ex = exchange or (LocalExchange(world) if spec.exchanged and world > 1 else None)
+  devs = device if isinstance(device, (list, tuple)) else [device] * world
+  shards = [ShardedDatabase(spec, r, world, device=devs[r], exchange=ex) for r in range(world)]
+  for sd in shards:
+    for rel, rows in inputs.items():
+      sd.load_rows(rel, rows)
+  errors: list = [None] * world
+
+  def work(r):
+    try:
+      shards[r].run(max_iters)
+    except BaseException as e:  # noqa: BLE001 -- reported after the join
+      errors[r] = e
+      if ex is not None:
+        ex.abort()
+
+  threads = [threading.Thread(target=work, args=(r,)) for r in range(world)]
+  for th in threads:
+    th.start()
+  for th in threads:
+    th.join()
+  failed = [e for e in errors if e is not None]
+  if failed:
+    for sd in shards:
+      sd.close()
+    raise failed[0]
+  return shards
 
 
 def combine_sizes(spec: ShardSpec, per_shard: list) -> dict:
@@ -292,5 +486,6 @@ def allreduce_results(spec: ShardSpec, sizes: dict, counts: dict, group=None) ->
   return out_sizes, out_counts
 
 
-__all__ = ['ShardError', 'ShardSpec', 'ShardedDatabase', 'owner', 'shard_plan', 'shard_rows',
-           'combine_sizes', 'combine_dumps', 'allreduce_results']
+__all__ = ['ShardError', 'ShardSpec', 'ShardedDatabase', 'LocalExchange', 'TorchExchange',
+           'run_local_shards', 'owner', 'shard_plan', 'shard_rows', 'combine_sizes',
+           'combine_dumps', 'allreduce_results']

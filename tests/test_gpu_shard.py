@@ -1,16 +1,16 @@
-'''Sharded evaluation: a program split over `world` shards (run here one
-after another on one GPU -- each shard's evaluation is independent, nothing
-waits on another shard) gives, once combined, exactly the unsharded result:
-partitioned relations are disjoint and their union is the relation, counts
-add up, replicated relations are equal on every shard.'''
+'''Sharded evaluation: a program split over `world` shards (run here by
+threads of one process on one GPU; shards meet only at host-side barriers
+of the exchange callback, no kernel waits on another shard's) gives, once
+combined, exactly the unsharded result: partitioned relations are disjoint
+and their union is the relation, counts add up, replicated relations are
+equal on every shard.'''
 
 import numpy as np
 import oracle
 import pytest
 from conftest import load_plan
 from srdatalog_b200 import workloads as W
-from srdatalog_b200.shard import (ShardedDatabase, combine_dumps, combine_sizes, owner,
-                                  shard_plan)
+from srdatalog_b200.shard import combine_dumps, combine_sizes, owner, run_local_shards, shard_plan
 
 pytestmark = pytest.mark.gpu
 
@@ -18,11 +18,9 @@ pytestmark = pytest.mark.gpu
 def run_shards(plan_name, inputs, world, rels=(), rules=()):
   spec = shard_plan(load_plan(plan_name))
   sizes, counts, dumps = [], [], {r: [] for r in rels}
-  for rank in range(world):
-    with ShardedDatabase(spec, rank, world) as sd:
-      for rel, rows in inputs.items():
-        sd.load_rows(rel, rows)
-      sd.run()
+  shards = run_local_shards(spec, world, inputs)
+  for rank, sd in enumerate(shards):
+    with sd:
       sizes.append({r: sd.local_size(r) for r in rels})
       counts.append({r: sd.local_count(r) for r in rules})
       for r in rels:
@@ -104,11 +102,34 @@ def test_lsqb_counts_sharded():
   assert cnt == want
 
 
-def test_sg_falls_back_to_replicas(expected):
-  '''Same generation moves the key in its recursive rule: every relation is
-  replicated and each shard computes the whole result.'''
+@pytest.mark.parametrize('world', [2, 3, 5])
+def test_sg_sharded_with_exchange(expected, world):
+  '''Same generation moves the key in its recursive rule: each iteration's
+  derived tuples go to the shards owning them, and the fixpoint stops when
+  every shard's delta is empty.'''
   exp = expected['sg_2k']
-  spec, sizes, _, dumps = run_shards('sg', {'Arc': W.sg_forest(2000, seed=4)}, 2, rels=('Sg',))
-  assert spec.partitioned == [] and spec.fallback
+  spec, sizes, _, dumps = run_shards('sg', {'Arc': W.sg_forest(2000, seed=4)}, world, rels=('Sg',))
+  assert spec.partitioned == ['Sg'] and spec.exchanged == ['Sg']
   assert sizes['Sg'] == exp['size']
   assert oracle.dump_hash(dumps['Sg']) == exp['sha256']
+
+
+@pytest.mark.parametrize('world', [2, 4])
+def test_left_recursive_tc_sharded_with_exchange(expected, world):
+  exp = expected['tc_mid']
+  e = W.uniform_edges(2000, 6000, 7)
+  spec, sizes, _, dumps = run_shards('tc_left', {'ArcInput': e}, world, rels=('Path',))
+  assert spec.exchanged == ['Path']
+  assert sizes['Path'] == exp['size']
+  assert oracle.dump_hash(dumps['Path']) == exp['sha256']
+
+
+def test_sg_shards_small_and_empty():
+  '''Shards that own no tuple still take part in every exchange and vote.'''
+  e = np.array([[0, 1], [0, 2], [1, 3], [2, 4]], np.uint32)
+  want, _ = oracle.run_plan(load_plan('sg'), {'Arc': e})
+  _, sizes, _, dumps = run_shards('sg', {'Arc': e}, 7, rels=('Sg',))
+  assert sizes['Sg'] == len(want['Sg'])
+  assert {tuple(map(int, r)) for r in dumps['Sg']} == set(want['Sg'])
+  _, sizes, _, _ = run_shards('sg', {'Arc': np.zeros((0, 2), np.uint32)}, 3, rels=('Sg',))
+  assert sizes['Sg'] == 0

@@ -2,6 +2,7 @@
 that marks rules for sharded evaluation, result combination, and the final
 sum over two gloo ranks.'''
 
+import ctypes
 import os
 import socket
 
@@ -14,19 +15,20 @@ from srdatalog_b200.shard import (ShardError, ShardSpec, allreduce_results, comb
 PLANS = ['andersen', 'cspa', 'lsqb_q6', 'lsqb_q7', 'reach_avoid', 'sg', 'tc', 'tc_left',
          'tc_lsm', 'triangle']
 
-# plan -> (partitioned relations, {rule: mode} for the marked rules, falls back)
+# plan -> (partitioned relations, {rule: mode} for the marked rules, falls back,
+#          relations exchanged between shards)
 EXPECTED = {
-  'andersen': ([], {}, True),
-  'cspa': ([], {}, True),
-  'lsqb_q6': ([], {'TwoHopPath': 'work'}, False),
+  'andersen': ([], {}, True, []),
+  'cspa': ([], {}, True, []),
+  'lsqb_q6': ([], {'TwoHopPath': 'work'}, False, []),
   'lsqb_q7': ([], {'Case1Both': 'work', 'Case2ReplyOnly': 'work', 'Case3LikeOnly': 'work',
-                   'Case4Neither': 'work'}, False),
-  'reach_avoid': (['Reach', 'Cut'], {'ReachBase': 'key', 'CutPairs': 'key'}, False),
-  'sg': ([], {}, True),
-  'tc': (['Path'], {'TCBase': 'key'}, False),
-  'tc_left': ([], {}, True),
-  'tc_lsm': (['Path'], {'TCBase': 'key'}, False),
-  'triangle': ([], {'TriangleJoin': 'work'}, False),
+                   'Case4Neither': 'work'}, False, []),
+  'reach_avoid': (['Reach', 'Cut'], {'ReachBase': 'key', 'CutPairs': 'key'}, False, []),
+  'sg': (['Sg'], {'SGBase': 'key', 'SGRec_D1': 'exchange'}, False, ['Sg']),
+  'tc': (['Path'], {'TCBase': 'key'}, False, []),
+  'tc_left': (['Path'], {'TCBase': 'key', 'TCRecL_D1': 'exchange'}, False, ['Path']),
+  'tc_lsm': (['Path'], {'TCBase': 'key'}, False, []),
+  'triangle': ([], {'TriangleJoin': 'work'}, False, []),
 }
 
 
@@ -46,10 +48,11 @@ def test_owner_matches_formula_and_spreads_keys():
 def test_shard_plan_marks(name):
   plan = load_plan(name)
   spec = shard_plan(plan)
-  part, marks, falls_back = EXPECTED[name]
+  part, marks, falls_back, sent = EXPECTED[name]
   assert spec.partitioned == part
   assert {r: m for r, m in spec.modes.items() if m} == marks
   assert bool(spec.fallback) == falls_back
+  assert spec.exchanged == sent
   assert sorted(spec.partitioned + spec.replicated) == sorted(r['name'] for r in plan['relations'])
   # the marks sit on the plan's rules; the input plan is left alone
   for st in spec.plan['steps']:
@@ -57,7 +60,15 @@ def test_shard_plan_marks(name):
       if op['op'] == 'execute_pipeline':
         assert op.get('shard', '') == marks.get(op['rule'], '')
         assert ('shard_var' in op) == (op.get('shard') == 'key')
-  assert 'shard' not in str(plan)
+  # an exchange op right before every rebuild of a relation an exchange rule derives
+  for st in spec.plan['steps']:
+    ops = st['ops']
+    for i, op in enumerate(ops):
+      if op['op'] == 'exchange':
+        assert op['rel'] in sent
+        assert ops[i + 1]['op'] == 'rebuild_index' and ops[i + 1]['rel'] == op['rel']
+        assert any(o.get('shard') == 'exchange' for o in ops[:i] if o['op'] == 'execute_pipeline')
+  assert 'shard' not in str(plan) and 'exchange' not in str(plan)
 
 
 def test_key_mode_uses_head_key():
@@ -66,9 +77,54 @@ def test_key_mode_uses_head_key():
   assert op['shard_var'] == 'x'
 
 
-def test_exchange_needed_is_reported():
-  spec = shard_plan(load_plan('sg'))
-  assert 'exchange' in spec.fallback and not spec.useful
+def test_join_across_keys_is_reported():
+  spec = shard_plan(load_plan('andersen'))
+  assert 'other shards' in spec.fallback and not spec.useful
+
+
+def _host_copy(dst, src, nbytes, stream):
+  ctypes.memmove(dst, src, nbytes)
+
+
+def _exchange_round(ex, world, sends):
+  '''Drives one exchange (phases 0, 1, 2) of `world` threads over host
+  buffers: sends[r][d] = keys shard r sends to shard d.'''
+  import threading
+  out = [None] * world
+
+  def work(r):
+    fn = ex.callback(r)
+    counts = (ctypes.c_uint64 * world)(*[len(sends[r][d]) for d in range(world)])
+    fn(0, 'R', counts, 0, 0, 0)
+    got = [counts[i] for i in range(world)]
+    flat = [k for d in range(world) for k in sends[r][d]]
+    sbuf = (ctypes.c_uint64 * max(1, len(flat)))(*flat)
+    rbuf = (ctypes.c_uint64 * max(1, sum(got)))()
+    fn(1, 'R', counts, ctypes.addressof(sbuf), ctypes.addressof(rbuf), 0)
+    vote = (ctypes.c_uint64 * world)(len(flat))
+    fn(2, '', vote, 0, 0, 0)
+    out[r] = (got, list(rbuf)[:sum(got)], vote[0])
+
+  ths = [threading.Thread(target=work, args=(r,)) for r in range(world)]
+  for t in ths:
+    t.start()
+  for t in ths:
+    t.join(timeout=60)
+  return out
+
+
+def test_local_exchange_moves_keys_to_owners():
+  from srdatalog_b200.shard import LocalExchange
+  world = 3
+  sends = [[[100 * r + 10 * d + k for k in range(r + d)] for d in range(world)]
+           for r in range(world)]
+  out = _exchange_round(LocalExchange(world, timeout=30, copy=_host_copy), world, sends)
+  total = sum(len(sends[r][d]) for r in range(world) for d in range(world))
+  for d in range(world):
+    got, keys, vote = out[d]
+    assert got == [len(sends[s][d]) for s in range(world)]
+    assert keys == [k for s in range(world) for k in sends[s][d]]  # grouped by source
+    assert vote == total
 
 
 def test_marked_plans_load_in_native_library():
@@ -134,6 +190,51 @@ def _rank_main(rank, world, port, out):
     out.put((rank, sizes, counts))
   finally:
     dist.destroy_process_group()
+
+
+def _torch_exchange_rank(rank, world, port, out):
+  import sys
+  repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+  sys.path[:0] = [os.path.join(repo, 'srdatalog-python_b200'), os.path.join(repo, 'tests')]
+  import torch.distributed as dist
+  from srdatalog_b200.shard import TorchExchange
+  os.environ.update(MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port))
+  dist.init_process_group('gloo', rank=rank, world_size=world)
+  try:
+    fn = TorchExchange(copy=lambda dst, src, n, s: ctypes.memmove(dst, src, n)).callback(rank)
+    sends = [[7 * rank + d] * (rank + d + 1) for d in range(world)]
+    counts = (ctypes.c_uint64 * world)(*[len(s) for s in sends])
+    fn(0, 'R', counts, 0, 0, 0)
+    got = [counts[i] for i in range(world)]
+    flat = [k for s in sends for k in s]
+    sbuf = (ctypes.c_uint64 * len(flat))(*flat)
+    rbuf = (ctypes.c_uint64 * sum(got))()
+    fn(1, 'R', counts, ctypes.addressof(sbuf), ctypes.addressof(rbuf), 0)
+    vote = (ctypes.c_uint64 * world)(len(flat))
+    fn(2, '', vote, 0, 0, 0)
+    out.put((rank, got, list(rbuf), vote[0]))
+  finally:
+    dist.destroy_process_group()
+
+
+def test_two_rank_torch_exchange():
+  import torch.multiprocessing as mp
+  ctx = mp.get_context('spawn')
+  q = ctx.Queue()
+  port = _free_port()
+  world = 2
+  procs = [ctx.Process(target=_torch_exchange_rank, args=(r, world, port, q)) for r in range(world)]
+  for p in procs:
+    p.start()
+  res = sorted(q.get(timeout=120) for _ in procs)
+  for p in procs:
+    p.join(timeout=60)
+    assert p.exitcode == 0
+  total = sum(r + d + 1 for r in range(world) for d in range(world))
+  for d, got, keys, vote in res:
+    assert got == [s + d + 1 for s in range(world)]
+    assert keys == [k for s in range(world) for k in [7 * s + d] * (s + d + 1)]
+    assert vote == total
 
 
 def test_two_rank_allreduce_of_results():
