@@ -83,6 +83,10 @@ int srdl_set_profiling(srdl_db* db, int enable);
  *   "lsm_compact_pct"  Device2LevelIndex: merge HEAD into FULL once HEAD
  *                      exceeds this percentage of FULL (default 10, the
  *                      reference's kCompactRatio, device_2level_index.h:300)
+ *   "radix_bits"       widest radix-sort digit, 1..8 (default 8): a sort of
+ *                      b-bit keys runs ceil(b / radix_bits) passes
+ *   "join_blocks_per_sm"  join launches use at most this many blocks per
+ *                      SM, 1..64 (default 16): the candidates per warp
  *   "shard_world",     evaluate as shard "shard_rank" of "shard_world"
  *   "shard_rank"       (default 0 of 1): rules the plan marks
  *                      "shard": "key" keep only bindings whose "shard_var"

@@ -211,7 +211,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
   for (size_t li = 0; li < levels.size(); li++) {
     LevelSpec& lv = levels[li];
     const bool last = li + 1 == levels.size();
-    DevBuf wscr(join_work_scratch_bytes(cur.n) + join_expand_scratch_bytes(L_.num_sms), L_.stream);
+    DevBuf wscr(join_work_scratch_bytes(cur.n) + join_expand_scratch_bytes(L_), L_.stream);
     Scratch s{wscr.as<char>(), wscr.bytes(), 0};
     size_t pid = prof_begin("join_count");
     JoinWork w = join_count(L_, lv, cur, s);

@@ -622,15 +622,15 @@ size_t join_work_scratch_bytes(uint64_t rows) {
          scan_scratch_bytes(rows) + 1024;
 }
 
-static int jgrid(uint64_t n, int sms) {
+static int jgrid(uint64_t n, const Launch& L) {
   uint64_t g = (n + kJThreads - 1) / kJThreads;
-  uint64_t cap = (uint64_t)sms * 16;
+  uint64_t cap = (uint64_t)L.num_sms * (L.join_bpsm > 0 ? L.join_bpsm : 16);
   if (g > cap) g = cap;
   return g ? (int)g : 1;
 }
 
-size_t join_expand_scratch_bytes(int num_sms) {
-  const uint64_t warps = (uint64_t)num_sms * 16 * (kJThreads / 32);
+size_t join_expand_scratch_bytes(const Launch& L) {
+  const uint64_t warps = (uint64_t)L.num_sms * (L.join_bpsm > 0 ? L.join_bpsm : 16) * (kJThreads / 32);
   return 2 * ((warps + 1) * 8 + 255) + scan_scratch_bytes(warps) + 1024;
 }
 
@@ -644,7 +644,7 @@ JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scrat
   if (lv.kind == kColumnJoin && lv.nsrc == 2 && (lv.src[0].t.bdir || lv.src[1].t.bdir))
     w.obm = s.take<uint32_t>(in.n ? in.n : 1);
   if (in.n) {
-    join_count_kernel<<<jgrid(in.n, L.num_sms), kJThreads, 0, L.stream>>>(lv, in, work, w.drv,
+    join_count_kernel<<<jgrid(in.n, L), kJThreads, 0, L.stream>>>(lv, in, work, w.drv,
                                                                           w.beg, w.orange, w.obm);
     SRDL_CUDA(cudaGetLastError());
     count_launches(1);
@@ -658,7 +658,7 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
                  Scratch& s) {
   if (total == 0) return;
   auto* cnt = reinterpret_cast<unsigned long long*>(d_out_n);
-  const int g = jgrid(total, L.num_sms);
+  const int g = jgrid(total, L);
   const uint64_t warps = (uint64_t)g * (kJThreads / 32);
   const uint64_t chunk = ((total + warps - 1) / warps + 31) & ~uint64_t(31);
   Table out = out_table ? *out_table : Table{};

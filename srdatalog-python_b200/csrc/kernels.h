@@ -15,6 +15,8 @@ struct Launch {
   cudaStream_t stream = 0;
   int num_sms = 148;
   uint32_t* d_err = nullptr;  // device error word (bounded-wait failures etc.)
+  int radix_bits = 8;         // widest radix-sort digit (1..8): passes = ceil(key bits / this)
+  int join_bpsm = 16;         // join launches: at most this many blocks per SM (work per warp)
 };
 
 // Bump allocator over a caller-provided scratch region.  Every piece starts
@@ -207,7 +209,7 @@ JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scrat
 // order: the table stays sorted), to `out_keys` (emit keys, any order) or
 // counted (emit count) via *d_out_n, which the caller zeroes.  Output
 // capacity = total.
-size_t join_expand_scratch_bytes(int num_sms);
+size_t join_expand_scratch_bytes(const Launch& L);
 void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const JoinWork& w,
                  uint64_t total, Table* out_table, uint64_t* out_keys, uint64_t* d_out_n,
                  Scratch& s);

@@ -798,6 +798,13 @@ void Database::set_option(const std::string& name, int64_t value) {
     SRDL_REQUIRE(value >= 1 && value <= 65536, kErrArg, "set_option: shard_world out of [1, 65536]");
     shard_world_ = value;
   } else if (name == "shard_rank") shard_rank_ = value;
+  else if (name == "radix_bits") {
+    SRDL_REQUIRE(value >= 1 && value <= 8, kErrArg, "set_option: radix_bits out of [1, 8]");
+    L_.radix_bits = (int)value;
+  } else if (name == "join_blocks_per_sm") {
+    SRDL_REQUIRE(value >= 1 && value <= 64, kErrArg, "set_option: join_blocks_per_sm out of [1, 64]");
+    L_.join_bpsm = (int)value;
+  }
   else throw Error{kErrArg, "set_option: unknown option " + name};
 }
 

@@ -10,7 +10,7 @@
 // from the loaded inputs (and rule constants), so the runtime knows a bound
 // 2^bits on all values.  A two-column key (hi, lo) is compressed to
 // (hi << bits) | lo -- 32 bits when 2*bits <= 32 -- and sorted with
-// ceil(2*bits / 8) stable counting passes.  Each pass is a histogram launch
+// ceil(2*bits / 8) stable counting passes (digits of at most Launch::radix_bits).  Each pass is a histogram launch
 // (shared-memory counters per block), a per-digit scan over the blocks, and a
 // scatter launch in which every warp ranks its keys with one ballot per digit
 // bit, the tile is staged in shared memory in digit order and written out
@@ -312,7 +312,8 @@ static void sort_dedup_t(const Launch& L, const uint64_t* in, uint64_t n, int bi
   uint32_t* digit_tot = s.take<uint32_t>(kRsBins);
 
   const int total_bits = 2 * bits;
-  const int passes = (total_bits + 7) / 8;
+  const int maxw = L.radix_bits >= 1 && L.radix_bits <= 8 ? L.radix_bits : 8;
+  const int passes = (total_bits + maxw - 1) / maxw;
   int shift = 0;
   for (int p = 0; p < passes && n > 1; p++) {
     const int w = total_bits / passes + (p < total_bits % passes ? 1 : 0);

@@ -9,7 +9,10 @@ None of the knobs changes a result; they trade memory and work:
 * ``bitmap_mb``: budget for bitmaps of the longest child lists of probed FULL
   indexes (0 turns them off);
 * ``lsm_compact_pct``: HEAD is merged into FULL once it exceeds this
-  percentage of FULL (only tried when some relation uses the LSM policy).
+  percentage of FULL (only tried when some relation uses the LSM policy);
+* ``radix_bits``: widest radix-sort digit (passes = key bits / this);
+* ``join_blocks_per_sm``: grid cap of the join launches, i.e. the
+  candidates each warp walks (the work-splitting chunk).
 
 Search: coordinate descent from the defaults -- each knob in turn takes every
 value of its range with the others fixed, and the fastest (median of ``reps``
@@ -36,7 +39,12 @@ LSM = 'SRDatalog::GPU::Device2LevelIndex'
 DEFAULT_SPACE = {
   'bitmap_mb': [0, 64, 256, 1024],
   'lsm_compact_pct': [5, 10, 25],
+  'radix_bits': [6, 7, 8],
+  'join_blocks_per_sm': [8, 16, 32],
 }
+
+# library defaults: the tuner's starting point
+DEFAULTS = {'bitmap_mb': 256, 'lsm_compact_pct': 10, 'radix_bits': 8, 'join_blocks_per_sm': 16}
 
 
 @dataclass
@@ -145,7 +153,7 @@ def autotune(plan: dict, inputs: dict, device: int = 0, reps: int = 3, space: di
   knobs += [(k, list(v)) for k, v in space.items()]
   setting = {f'index_type:{r}': next(x['index_type'] for x in plan['relations'] if x['name'] == r)
              for r in rec}
-  setting.update({'bitmap_mb': 256, 'lsm_compact_pct': 10})
+  setting.update(DEFAULTS)
   setting = {k: v for k, v in setting.items() if any(k == kk for kk, _ in knobs)}
   trials: list = []
   seen: dict = {}

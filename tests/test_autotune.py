@@ -15,6 +15,8 @@ def fake_timer(costs, sig=(('Path', 7),)):
     ms = 100.0
     ms -= 30 if idx.get('Path') == LSM else 0
     ms -= costs.get(('bitmap_mb', options.get('bitmap_mb')), 0)
+    for k in ('radix_bits', 'join_blocks_per_sm'):
+      ms -= costs.get((k, options.get(k)), 0)
     if idx.get('Path') == LSM:
       ms -= costs.get(('lsm_compact_pct', options.get('lsm_compact_pct')), 0)
     calls.append((idx.get('Path'), dict(options)))
@@ -30,11 +32,13 @@ def test_recursive_relations():
 
 
 def test_finds_the_fastest_setting():
-  t = fake_timer({('bitmap_mb', 64): 5, ('lsm_compact_pct', 25): 3})
+  t = fake_timer({('bitmap_mb', 64): 5, ('lsm_compact_pct', 25): 3, ('radix_bits', 7): 2,
+                  ('join_blocks_per_sm', 32): 1})
   r = autotune(load_plan('tc'), {'ArcInput': [[0, 1]]}, timer=t)
   assert r.index_types == {'Path': LSM}
-  assert r.options == {'bitmap_mb': 64, 'lsm_compact_pct': 25}
-  assert r.ms == 100 - 30 - 5 - 3
+  assert r.options == {'bitmap_mb': 64, 'lsm_compact_pct': 25, 'radix_bits': 7,
+                       'join_blocks_per_sm': 32}
+  assert r.ms == 100 - 30 - 5 - 3 - 2 - 1
   # the compaction knob is only tried with the LSM policy on
   assert all('lsm_compact_pct' not in o for p, o in t.calls if p != LSM)
 

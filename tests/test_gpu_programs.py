@@ -322,3 +322,22 @@ def test_reach_avoid_negation(n, m, seed):
     w = np.array(want[rel], np.uint32).reshape(-1, 2)
     assert db.size(rel) == w.shape[0], rel
     assert oracle.dump_hash(db.dump(rel)) == oracle.dump_hash(w), rel
+
+
+@pytest.mark.parametrize('radix_bits,jbpsm', [(5, 8), (6, 32), (7, 16), (8, 1)])
+def test_tuning_options_keep_results(expected, radix_bits, jbpsm):
+  '''The autotuner's sort-digit and join-grid knobs change no result.'''
+  e = W.uniform_edges(2000, 6000, 7)
+  db = native.Database(load_plan('tc'))
+  db.set_option('radix_bits', radix_bits)
+  db.set_option('join_blocks_per_sm', jbpsm)
+  db.load_rows('ArcInput', e)
+  db.run()
+  assert db.size('Path') == expected['tc_mid']['size']
+  assert oracle.dump_hash(db.dump('Path')) == expected['tc_mid']['sha256']
+  t = native.Database(load_plan('triangle'))
+  t.set_option('radix_bits', radix_bits)
+  t.set_option('join_blocks_per_sm', jbpsm)
+  t.load_rows('KnowsInput', W.rmat_edges(14, 1 << 18, seed=5))
+  t.run()
+  assert t.count('TriangleJoin') == expected['triangle_rmat14']['count']

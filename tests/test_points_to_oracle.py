@@ -74,4 +74,10 @@ def test_set_option_rejects_unknown_names():
   with pytest.raises(Exception):
     db.set_option('bitmap_mb', -1)
   db.set_option('bitmap_mb', 0)
+  db.set_option('radix_bits', 7)
+  db.set_option('join_blocks_per_sm', 32)
+  for name, bad in (('radix_bits', 0), ('radix_bits', 9), ('join_blocks_per_sm', 0),
+                    ('join_blocks_per_sm', 65)):
+    with pytest.raises(Exception):
+      db.set_option(name, bad)
   db.close()
