@@ -336,7 +336,7 @@ def run_served(args, rank, world):
   offs = poisson_arrivals(SERVE_REQUESTS, rate, seed=5)
   torch.cuda.init()
   with Server(progs, workers=args.serve_workers, budget_bytes=120 << 30,
-              batch_max_edges=args.batch_max_edges) as srv:
+              batch_max_edges=args.batch_max_edges, max_batch=args.serve_max_batch) as srv:
     for w in range(args.warmup):  # warm-up replays (handles, pools, caches)
       replay(srv, serve_requests(pool, 64, seed=900 + w), poisson_arrivals(64, rate, seed=w))
     results, sums = None, []
@@ -360,7 +360,8 @@ def run_served(args, rank, world):
     'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'u32',
     'data': 'synthetic',
     'config': {'workload': SERVE_DESC, 'offered_rate': rate, 'requests_per_step': SERVE_REQUESTS,
-               'workers': args.serve_workers, 'batch_max_edges': args.batch_max_edges},
+               'workers': args.serve_workers, 'batch_max_edges': args.batch_max_edges,
+               'max_batch': args.serve_max_batch},
     'latency_ms': {'p50': statistics.median(s['p50_ms'] for s in sums),
                    'p99': statistics.median(s['p99_ms'] for s in sums)},
     'mean_batch': statistics.median(s['mean_batch'] for s in sums),
@@ -381,9 +382,11 @@ def main():
   ap.add_argument('--impl', default='srdl', choices=['srdl', 'reference'])
   ap.add_argument('--workload', default='triangle', choices=sorted(WORKLOADS) + ['served'])
   ap.add_argument('--rate', type=float, default=2000.0, help='served: offered load (req/s)')
-  ap.add_argument('--serve-workers', type=int, default=4, help='served: concurrent workers')
+  ap.add_argument('--serve-workers', type=int, default=8, help='served: concurrent workers')
   ap.add_argument('--batch-max-edges', type=int, default=1 << 20,
                   help='served: largest request (input edges) that is unioned with others')
+  ap.add_argument('--serve-max-batch', type=int, default=16,
+                  help='served: most requests evaluated as one union')
   ap.add_argument('--no-cpu-baseline', action='store_true')
   ap.add_argument('--quick', action='store_true',
                   help='kernel-resident path only (no e2e, no CPU baseline): for profiler runs')

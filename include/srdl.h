@@ -182,6 +182,13 @@ int64_t srdl_dump(srdl_db* db, const char* rel, uint32_t* out_rows, uint64_t cap
 /* JSON run statistics (iterations per step, timings, derived rows). */
 int srdl_stats_json(srdl_db* db, char* buf, uint64_t cap);
 
+/* SHA-256 of FULL(rel) as srdl_dump returns it (rows sorted, declared
+ * column order, row-major little-endian uint32) into out32[32]: the parity
+ * check's digest, computed next to the data.  srdl_sha256 hashes any host
+ * buffer the same way.  No reference counterpart. */
+int srdl_hash(srdl_db* db, const char* rel, unsigned char* out32);
+int srdl_sha256(const void* data, uint64_t n_bytes, unsigned char* out32);
+
 /* ------------------------------------------------------------------------
  * Kernel primitives.  Keys are uint64 = (index column 0 << 32) | column 1;
  * every value must be < 2^value_bits.  Pointers are device pointers, work

@@ -10,8 +10,10 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <cmath>
 #include <cstring>
 #include <fstream>
+#include <vector>
 #include <sstream>
 
 #include "../../include/srdl.h"
@@ -267,6 +269,96 @@ int64_t srdl_dump(srdl_db* h, const char* rel, uint32_t* out_rows, uint64_t cap_
     set_error(e.msg);
     return -(int64_t)e.code;
   }
+}
+
+// SHA-256 (FIPS 180-4).  The round constants are the first 32 bits of the
+// fractional parts of the cube roots of the first 64 primes, the initial
+// hash the same of the square roots of the first 8; both are derived here
+// in extended precision.
+namespace {
+struct Sha256 {
+  uint32_t k[64], h0[8];
+  Sha256() {
+    int primes[64], np = 0;
+    for (int c = 2; np < 64; c++) {
+      bool prime = true;
+      for (int d = 2; d * d <= c; d++) prime &= c % d != 0;
+      if (prime) primes[np++] = c;
+    }
+    for (int i = 0; i < 64; i++) {
+      const long double r = cbrtl((long double)primes[i]);
+      k[i] = (uint32_t)((r - floorl(r)) * 4294967296.0L);
+    }
+    for (int i = 0; i < 8; i++) {
+      const long double r = sqrtl((long double)primes[i]);
+      h0[i] = (uint32_t)((r - floorl(r)) * 4294967296.0L);
+    }
+  }
+  static uint32_t rotr(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
+  void block(uint32_t* h, const unsigned char* p) const {
+    uint32_t w[64];
+    for (int i = 0; i < 16; i++)
+      w[i] = (uint32_t)p[4 * i] << 24 | (uint32_t)p[4 * i + 1] << 16 | (uint32_t)p[4 * i + 2] << 8 | p[4 * i + 3];
+    for (int i = 16; i < 64; i++) {
+      const uint32_t s0 = rotr(w[i - 15], 7) ^ rotr(w[i - 15], 18) ^ (w[i - 15] >> 3);
+      const uint32_t s1 = rotr(w[i - 2], 17) ^ rotr(w[i - 2], 19) ^ (w[i - 2] >> 10);
+      w[i] = w[i - 16] + s0 + w[i - 7] + s1;
+    }
+    uint32_t a = h[0], b = h[1], c = h[2], d = h[3], e = h[4], f = h[5], g = h[6], hh = h[7];
+    for (int i = 0; i < 64; i++) {
+      const uint32_t t1 = hh + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) + ((e & f) ^ (~e & g)) + k[i] + w[i];
+      const uint32_t t2 = (rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
+      hh = g;
+      g = f;
+      f = e;
+      e = d + t1;
+      d = c;
+      c = b;
+      b = a;
+      a = t1 + t2;
+    }
+    h[0] += a; h[1] += b; h[2] += c; h[3] += d; h[4] += e; h[5] += f; h[6] += g; h[7] += hh;
+  }
+  void digest(const unsigned char* data, uint64_t n, unsigned char out[32]) const {
+    uint32_t h[8];
+    for (int i = 0; i < 8; i++) h[i] = h0[i];
+    uint64_t i = 0;
+    for (; i + 64 <= n; i += 64) block(h, data + i);
+    unsigned char tail[128] = {0};
+    const uint64_t rem = n - i;
+    for (uint64_t j = 0; j < rem; j++) tail[j] = data[i + j];
+    tail[rem] = 0x80;
+    const uint64_t tl = rem + 1 + 8 <= 64 ? 64 : 128;
+    const uint64_t bits = n * 8;
+    for (int j = 0; j < 8; j++) tail[tl - 1 - j] = (unsigned char)(bits >> (8 * j));
+    for (uint64_t j = 0; j < tl; j += 64) block(h, tail + j);
+    for (int j = 0; j < 8; j++)
+      for (int b = 0; b < 4; b++) out[4 * j + b] = (unsigned char)(h[j] >> (24 - 8 * b));
+  }
+};
+const Sha256& sha256() {
+  static const Sha256 s;
+  return s;
+}
+}  // namespace
+
+int srdl_sha256(const void* data, uint64_t n_bytes, unsigned char* out32) {
+  if ((!data && n_bytes) || !out32) return kErrArg;
+  sha256().digest(static_cast<const unsigned char*>(data), n_bytes, out32);
+  return 0;
+}
+
+int srdl_hash(srdl_db* h, const char* rel, unsigned char* out32) {
+  if (!h || !rel || !out32) return kErrArg;
+  SRDL_GUARD(0, {
+    const int64_t rows = h->db->dump(rel, nullptr, 0);
+    const int arity = h->db->rel(rel).arity;
+    std::vector<uint32_t> buf((size_t)rows * arity + 1);
+    h->db->dump(rel, buf.data(), (uint64_t)rows);
+    sha256().digest(reinterpret_cast<const unsigned char*>(buf.data()),
+                    (uint64_t)rows * arity * 4, out32);
+    return 0;
+  })
 }
 
 int srdl_stats_json(srdl_db* h, char* buf, uint64_t cap) {

@@ -60,7 +60,17 @@ SIGNATURES = {
   'srdl_set_option': (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64]),
   'srdl_set_exchange': (ctypes.c_int, [_vp, EXCHANGE_FN, _vp]),
   'srdl_copy_device': (ctypes.c_int, [_vp, _vp, _u64, _vp]),
+  'srdl_hash': (ctypes.c_int, [_vp, _cp, ctypes.c_char_p]),
+  'srdl_sha256': (ctypes.c_int, [_vp, _u64, ctypes.c_char_p]),
 }
+
+
+def sha256(data: bytes) -> str:
+  '''SHA-256 (hex) computed by libsrdl.'''
+  out = ctypes.create_string_buffer(32)
+  buf = ctypes.create_string_buffer(bytes(data), max(1, len(data)))
+  check(lib().srdl_sha256(buf, len(data), out), 'srdl_sha256')
+  return out.raw.hex()
 
 _LIB = None
 
@@ -210,6 +220,13 @@ class Database:
       self._xerr = None
       raise SrdlError('srdl_run', rc, f'exchange callback raised {xerr!r}') from xerr
     check(rc, 'srdl_run')
+
+  def hash(self, rel: str) -> str:
+    '''SHA-256 (hex) of FULL(rel) as dump() returns it (sorted rows,
+    little-endian uint32, row-major), computed in libsrdl.'''
+    out = ctypes.create_string_buffer(32)
+    check(lib().srdl_hash(self._h, rel.encode(), out), 'srdl_hash')
+    return out.raw.hex()
 
   def size(self, rel: str) -> int:
     return int(lib().srdl_size(self._h, rel.encode()))

@@ -85,8 +85,8 @@ class ServeStats:
 class Server:
   '''Admission-controlled, continuously batching request loop (see module doc).'''
 
-  def __init__(self, programs: dict, device: int = 0, workers: int = 4,
-               budget_bytes: int = 120 << 30, max_batch: int = 256, batching: bool = True,
+  def __init__(self, programs: dict, device: int = 0, workers: int = 8,
+               budget_bytes: int = 120 << 30, max_batch: int = 16, batching: bool = True,
                keep_rows: bool = False, batch_max_edges: int = 1 << 20,
                batch_max_span: int = 1 << 23):
     self.programs = programs

@@ -124,3 +124,10 @@ def test_generated_shim_abi(tmp_path):
   assert lib.srdatalog_size(b'Unknown') == 0
   assert rt.srdatalog_shutdown() == 0
   assert lib.srdatalog_size(b'Path') == 0
+
+
+@pytest.mark.parametrize('n', [0, 1, 3, 55, 56, 63, 64, 65, 119, 120, 1000, 1 << 20])
+def test_library_sha256_matches_hashlib(n):
+  import hashlib
+  data = np.random.default_rng(n).integers(0, 256, n, dtype=np.uint8).tobytes()
+  assert native.sha256(data) == hashlib.sha256(data).hexdigest()

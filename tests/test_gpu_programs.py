@@ -134,7 +134,17 @@ def test_shim_end_to_end(tmp_path, expected):
   buf = np.empty((n, 2), np.uint32)
   assert lib.srdatalog_dump(b'Path', buf.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), n) == n
   assert oracle.dump_hash(buf) == expected['tc_mid']['sha256']
+  digest = ctypes.create_string_buffer(32)
+  assert lib.srdatalog_hash(b'Path', digest) == 0   # computed in the library
+  assert digest.raw.hex() == expected['tc_mid']['sha256']
   assert lib.srdatalog_shutdown() == 0
+
+
+def test_library_hash_matches_oracle(expected):
+  db = run('sg', {'Arc': W.sg_forest(2000, seed=4)})
+  assert db.hash('Sg') == expected['sg_2k']['sha256'] == oracle.dump_hash(db.dump('Sg'))
+  t = run('triangle', {'KnowsInput': W.rmat_edges(12, 40000, seed=5)})
+  assert t.hash('Knows') == oracle.dump_hash(t.dump('Knows'))
 
 
 def test_triangle_large_ids_sparse_path():
