@@ -18,6 +18,11 @@ iteration's derived tuples to their owners with one all-to-all; inputs
 replicated, one final all-reduce of the result), value = the job's tuples
 over the max per-rank time (strong scaling); plans the analysis cannot
 shard run as independent replicas (weak scaling).
+SRDL_BENCH_BACKEND=gloo runs the collectives on the host (ranks may then
+share a GPU, which exercises the N>1 path but times nothing meaningful).
+--workload served: the request server (8 workers, unions of at most 16
+requests: --serve-workers, --serve-max-batch) against the plain loop at
+--rate offered requests/s.
 --impl reference: the CPU restatement of the reference's evaluation on
 the host cores, on a bounded sample of the same workload.
 '''
