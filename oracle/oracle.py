@@ -403,6 +403,70 @@ def lsqb_q6(inputs: dict) -> int:
   return int(np.sum((deg - 1) * s))
 
 
+def _adj(rows) -> dict:
+  out: dict = {}
+  for a, b in np.unique(np.asarray(rows, np.int64).reshape(-1, 2), axis=0).tolist():
+    out.setdefault(a, set()).add(b)
+  return out
+
+
+def lsqb_q3(inputs: dict) -> list:
+  '''Triangle of examples/lsqb_q3_triangle.py:66-85, by Python sets:
+  (p1, p2, p3) with Knows(p1,p2), Knows(p2,p3), Knows(p3,p1) whose three
+  people are located in cities of one country.'''
+  knows = _adj(inputs['KnowsInput'])
+  city = {p: c for p, c in np.asarray(inputs['IsLocatedInInput']).tolist()}
+  country = {c: k for c, k in np.asarray(inputs['IsPartOfInput']).tolist()}
+  loc = _adj(inputs['IsLocatedInInput'])
+  part = _adj(inputs['IsPartOfInput'])
+  del city, country
+  out = set()
+  for p1, n1 in knows.items():
+    for p2 in n1:
+      for p3 in knows.get(p2, ()):
+        if p1 not in knows.get(p3, ()):
+          continue
+        cos = [set().union(*(part.get(c, set()) for c in loc.get(p, ()))) for p in (p1, p2, p3)]
+        if cos[0] & cos[1] & cos[2]:
+          out.add((p1, p2, p3))
+  return sorted(out)
+
+
+def lsqb_two_hop(inputs: dict, second: str | None = None, negate: bool = False,
+                 as_planned: bool = True) -> set:
+  '''Path of examples/lsqb_q6_2hop.py:66-85 (second hop over a second Knows
+  copy: lsqb_q6_nosj.py; ends that do not know each other: lsqb_q9_neg2hop.py
+  :66-90), by Python sets: (p1, p2, p3, t) with Knows(p1,p2),
+  Knows'(p2,p3), HasInterest(p3,t), p1 != p3 (and not Knows(p1,p3)).
+
+  as_planned: the reference's planner lowers the first atom of the 2hop and
+  nosj rules to a join on Knows' column 0 for p2 (fixtures
+  tests/fixtures/integration/lsqb_q6_2hop.mir.sexpr, lsqb_q6_nosj.mir.sexpr:
+  both p2 sources use index (0 1) with an empty prefix, p1 then comes from
+  Knows[p2]), i.e. it evaluates Knows(p2,p1); the reference executes that
+  plan, so its output is this reading.  Q9's plan reads Knows(p1,p2) through
+  index (1 0), the rule as written.'''
+  k1 = _adj(inputs['KnowsInput'])
+  k2 = _adj(inputs[second]) if second else k1
+  hi = _adj(inputs['HasInterestInput'])
+  first = k1
+  if as_planned and not negate:
+    rev: dict = {}
+    for a, bs in k1.items():
+      for b in bs:
+        rev.setdefault(b, set()).add(a)
+    first = rev  # first[p1] = {p2 : Knows(p2, p1)}
+  out = set()
+  for p1, n1 in first.items():
+    for p2 in n1:
+      for p3 in k2.get(p2, ()):
+        if p1 == p3 or (negate and p3 in k1.get(p1, ())):
+          continue
+        for t in hi.get(p3, ()):
+          out.add((p1, p2, p3, t))
+  return out
+
+
 def reach_avoid(edges: np.ndarray, blocked: np.ndarray) -> dict:
   '''Reach = transitive closure of Edge minus Blocked edges; Cut = Blocked
   pairs not in Reach (the reach_avoid test program), by Python sets.'''

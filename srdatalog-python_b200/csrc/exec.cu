@@ -199,9 +199,13 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
   }
 
   Relation* target = &rel(insert->rel);
-  if (!op.count)
-    SRDL_REQUIRE(target->arity <= 2, kErrUnsupported,
-                 "rule " + op.rule + ": materialising relations of arity > 2 is not supported");
+  if (!op.count && target->arity > 2) {
+    SRDL_REQUIRE(target->arity <= 4 && target->pack_half > 0, kErrUnsupported,
+                 "rule " + op.rule + ": materialising " + target->name + " needs arity <= 4 and " +
+                     "arity x value bits <= 64");
+    SRDL_REQUIRE(insert->index == target->canonical, kErrUnsupported,
+                 "rule " + op.rule + ": " + target->name + " is written in its canonical order only");
+  }
 
   // Walk the levels over a table of partial bindings.
   Table cur;
@@ -266,6 +270,8 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
       } else {
         lv.emit = kEmitKeys;
         lv.key_arity = target->arity;
+        lv.pack_bits = target->pack_bits;
+        lv.pack_half = target->pack_half;
         for (int c = 0; c < target->arity; c++) lv.key_slot[c] = slot_of(insert->vars[insert->index[c]]);
         Chunk ch;
         ch.order = insert->index;
@@ -314,11 +320,18 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
 void Database::op_rebuild(const Step& st, size_t pos, const Op& op) {
   Relation& r = rel(op.rel);
   RelVersion& rv = r.v[op.ver];
-  if (r.arity > 2) {
+  if (r.arity > 2 && (rv.chunks.empty() || r.pack_half == 0)) {
+    // nothing materialised (count-only heads, or no output this time)
     rv.chunks.clear();
     rv.idx[op.index];
     return;
   }
+  // packed tuples of arity 3-4 sort as binary keys of pack_half-bit halves
+  const int key_bits = r.arity > 2 ? r.pack_half : 0;
+  if (r.arity > 2)
+    for (auto& c : rv.chunks)
+      SRDL_REQUIRE(c.order == op.index, kErrUnsupported,
+                   "relation " + r.name + " of arity > 2 rebuilt in another order");
   uint64_t total = 0;
   for (auto& c : rv.chunks) total += c.n;
   // Gather the chunks into one buffer packed in the target order.
@@ -359,13 +372,13 @@ void Database::op_rebuild(const Step& st, size_t pos, const Op& op) {
     if (r.v[kFull].has_index())
       full = r.lsm ? &full_base(r, op.index) : &ensure_index(r, kFull, op.index);
     const Index* head = r.lsm && op.index == r.canonical && r.head.n ? &r.head : nullptr;
-    sort_into(r.pending, in ? in : nullptr, total, false, full, head);
+    sort_into(r.pending, in ? in : nullptr, total, false, full, head, key_bits);
     r.pending_delta = true;
     rv.chunks.clear();
     rv.idx.clear();
   } else {
     Index fresh;
-    sort_into(fresh, in, total, false, nullptr);
+    sort_into(fresh, in, total, false, nullptr, nullptr, key_bits);
     rv.chunks.clear();
     rv.idx.clear();
     rv.idx[op.index] = std::move(fresh);
@@ -383,8 +396,11 @@ void Database::op_compute_delta(const Op& op) {
     return;
   }
   if (r.arity > 2) {
-    r.v[kDelta].idx[op.index];
-    return;
+    auto it = r.v[kNew].idx.find(op.index);
+    if (r.pack_half == 0 || it == r.v[kNew].idx.end() || it->second.n == 0) {
+      r.v[kDelta].idx[op.index];
+      return;
+    }
   }
   Index& nw = ensure_index(r, kNew, op.index);
   Index& d = r.v[kDelta].idx[op.index];
@@ -410,8 +426,11 @@ void Database::op_compute_delta(const Op& op) {
 void Database::op_merge(const Op& op) {
   Relation& r = rel(op.rel);
   if (r.arity > 2) {
-    r.v[kFull].idx[op.index];
-    return;
+    auto it = r.v[kDelta].idx.find(op.index);
+    if (r.pack_half == 0 || it == r.v[kDelta].idx.end() || it->second.n == 0) {
+      r.v[kFull].idx[op.index];
+      return;
+    }
   }
   RelVersion& dv = r.v[kDelta];
   Index* d = nullptr;
@@ -689,7 +708,37 @@ uint64_t Database::count(const std::string& rule) const {
 
 int64_t Database::dump(const std::string& name, uint32_t* out, uint64_t cap_rows) {
   Relation& r = rel(name);
-  if (!r.v[kFull].has_index() || r.arity > 2) return 0;
+  if (!r.v[kFull].has_index()) return 0;
+  if (r.arity > 2) {
+    // packed tuples: unpack in index order, place in declared column order
+    auto it = r.v[kFull].idx.find(r.canonical);
+    if (r.pack_half == 0 || it == r.v[kFull].idx.end()) return 0;
+    Index& ix = it->second;
+    if (!out) return (int64_t)ix.n;
+    SRDL_CUDA(cudaSetDevice(device_));
+    const uint64_t n = std::min(ix.n, cap_rows);
+    std::vector<uint64_t> keys(n);
+    if (n)
+      SRDL_CUDA(cudaMemcpyAsync(keys.data(), ix.keys.as<uint64_t>(), n * 8, cudaMemcpyDeviceToHost,
+                                L_.stream));
+    SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+    const int k = r.arity, b = r.pack_bits, h = r.pack_half;
+    const uint64_t cmask = (1ull << b) - 1, hmask = (1ull << h) - 1;
+    for (uint64_t i = 0; i < n; i++) {
+      const uint64_t p = ((keys[i] >> 32) << h) | (keys[i] & hmask);
+      for (int c = 0; c < k; c++)
+        out[i * k + r.canonical[c]] = (uint32_t)((p >> (b * (k - 1 - c))) & cmask);
+    }
+    bool identity = true;
+    for (int c = 0; c < k; c++) identity &= r.canonical[c] == c;
+    if (!identity) {  // rows must come sorted in declared column order
+      std::vector<std::vector<uint32_t>> rows(n);
+      for (uint64_t i = 0; i < n; i++) rows[i].assign(out + i * k, out + (i + 1) * k);
+      std::sort(rows.begin(), rows.end());
+      for (uint64_t i = 0; i < n; i++) std::copy(rows[i].begin(), rows[i].end(), out + i * k);
+    }
+    return (int64_t)ix.n;
+  }
   SRDL_CUDA(cudaSetDevice(device_));
   Index& ix = ensure_index(r, kFull, identity_perm(r.arity));
   if (!out) return (int64_t)ix.n;

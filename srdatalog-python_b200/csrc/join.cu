@@ -215,6 +215,19 @@ struct SegWalk {
   }
 };
 
+// Key of an emitted binding from its column values c[0..key_arity) in the
+// target index order: (c0 << 32) | c1 for two columns (c0 << 32 for one);
+// three or four columns packed pack_bits apiece into P and split at
+// pack_half bits, (P >> pack_half) << 32 | (P mod 2^pack_half).
+__device__ __forceinline__ uint64_t emit_key(const LevelSpec& lv, const uint32_t (&c)[4]) {
+  if (lv.key_arity <= 2) return ((uint64_t)c[0] << 32) | (lv.key_arity > 1 ? c[1] : 0u);
+  uint64_t p = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+    if (i < lv.key_arity) p = (p << lv.pack_bits) | c[i];
+  return ((p >> lv.pack_half) << 32) | (p & ((1ull << lv.pack_half) - 1));
+}
+
 enum ExpandMode : int { kModeCount = 0, kModeKeys = 1, kModeTableCount = 2, kModeTableWrite = 3 };
 
 // in.col[k][r] with a compile-time slot index, so the Table parameter is
@@ -394,11 +407,13 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
           if (lane == leader) pos0 = atomicAdd(d_out_n, (unsigned long long)__popc(m));
           pos0 = __shfl_sync(kAllLanes, pos0, leader);
           if (ok) {
-            const int k0 = lv.key_slot[0], k1 = lv.key_slot[1];
-            const uint64_t hi = k0 < lv.n_in_slots ? slot_value(in, k0, r) : v;
-            const uint64_t lo =
-                lv.key_arity > 1 ? (k1 < lv.n_in_slots ? slot_value(in, k1, r) : v) : 0;
-            out_keys[pos0 + __popc(m & lanemask_lt())] = (hi << 32) | lo;
+            uint32_t kc[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              const int ks = lv.key_slot[i];
+              kc[i] = i < lv.key_arity ? (ks < lv.n_in_slots ? slot_value(in, ks, r) : v) : 0u;
+            }
+            out_keys[pos0 + __popc(m & lanemask_lt())] = emit_key(lv, kc);
           }
         }
       } else {
@@ -494,9 +509,10 @@ __global__ void __launch_bounds__(kJThreads) join_expand_kernel(
           if (lane == leader) pos0 = atomicAdd(d_out_n, (unsigned long long)__popc(m));
           pos0 = __shfl_sync(kAllLanes, pos0, leader);
           if (ok) {
-            const uint64_t hi = val(lv.key_slot[0]);
-            const uint64_t lo = lv.key_arity > 1 ? val(lv.key_slot[1]) : 0;
-            out_keys[pos0 + __popc(m & lanemask_lt())] = (hi << 32) | lo;
+            uint32_t kc[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) kc[i] = i < lv.key_arity ? val(lv.key_slot[i]) : 0u;
+            out_keys[pos0 + __popc(m & lanemask_lt())] = emit_key(lv, kc);
           }
         }
       } else {  // ordered table write
@@ -564,13 +580,13 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
       if (MODE == kModeKeys && lv.nfilt == 0) {
         // every candidate is a result: candidate index = output position
         if (ok) {
-          const int k0 = lv.key_slot[0], k1 = lv.key_slot[1];
-          const uint64_t hi = k0 == s0 ? v0 : k0 == s1 ? v1 : slot_value(in, k0, r);
-          const uint64_t lo = lv.key_arity < 2 ? 0
-                              : k1 == s0       ? v0
-                              : k1 == s1       ? v1
-                                               : slot_value(in, k1, r);
-          out_keys[base + lane] = (hi << 32) | lo;
+          uint32_t kc[4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const int ks = lv.key_slot[i];
+            kc[i] = i >= lv.key_arity ? 0u : ks == s0 ? v0 : ks == s1 ? v1 : slot_value(in, ks, r);
+          }
+          out_keys[base + lane] = emit_key(lv, kc);
         }
         r0 = __shfl_sync(kAllLanes, r, 31);
         continue;
@@ -585,13 +601,13 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
           if (lane == leader) pos0 = atomicAdd(d_out_n, (unsigned long long)__popc(m));
           pos0 = __shfl_sync(kAllLanes, pos0, leader);
           if (ok) {
-            const int k0 = lv.key_slot[0], k1 = lv.key_slot[1];
-            const uint64_t hi = k0 == s0 ? v0 : k0 == s1 ? v1 : slot_value(in, k0, r);
-            const uint64_t lo = lv.key_arity < 2 ? 0
-                                : k1 == s0       ? v0
-                                : k1 == s1       ? v1
-                                                 : slot_value(in, k1, r);
-            out_keys[pos0 + __popc(m & lanemask_lt())] = (hi << 32) | lo;
+            uint32_t kc[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              const int ks = lv.key_slot[i];
+              kc[i] = i >= lv.key_arity ? 0u : ks == s0 ? v0 : ks == s1 ? v1 : slot_value(in, ks, r);
+            }
+            out_keys[pos0 + __popc(m & lanemask_lt())] = emit_key(lv, kc);
           }
         }
       } else {

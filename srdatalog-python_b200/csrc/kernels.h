@@ -170,8 +170,10 @@ struct LevelSpec {
   FiltSpec filt[kMaxFilt];
   int n_in_slots = 0;                   // slots bound by the input table
   int emit = kEmitTable;
-  int key_slot[2] = {-1, -1};           // emit keys: slots of the target index columns
+  int key_slot[4] = {-1, -1, -1, -1};   // emit keys: slots of the target index columns
   int key_arity = 2;
+  // emit keys of arity 3-4: columns packed pack_bits apiece, split at pack_half
+  int pack_bits = 0, pack_half = 0;
   // Count mode only: also add every counted binding to grp_counts[g] for the
   // group g with grp_bounds[g] <= (value of slot 0) < grp_bounds[g+1].
   const uint32_t* grp_bounds = nullptr;  // n_groups + 1 sorted entries

@@ -599,19 +599,21 @@ void Database::load_device_rows(const std::string& name, const uint32_t* d_rows,
 // Sorted unique keys of `in` (packed in some order) into `out`, optionally
 // dropping keys present in `full`.
 void Database::sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full,
-                         const Index* head) {
+                         const Index* head, int key_bits) {
+  // key halves hold at most key_bits bits (0: the value bits of the inputs)
+  const int kb = key_bits > 0 ? key_bits : bits_;
   out.keys = DevBuf(std::max<uint64_t>(n, 1) * 8, L_.stream);
   out.trie = false;
   if (n == 0) {
     out.n = 0;
     return;
   }
-  DevBuf scratch(sort_scratch_bytes(n, bits_), L_.stream);
+  DevBuf scratch(sort_scratch_bytes(n, kb), L_.stream);
   Scratch s{scratch.as<char>(), scratch.bytes(), 0};
   const bool hd = head && head->n;
   const bool diff = (full && full->n) || hd;
   size_t pid = prof_begin(diff ? "sort_dedup_diff" : "sort_dedup");
-  sort_dedup(L_, in, n, bits_, swap, full && full->n ? full->keys.as<uint64_t>() : nullptr,
+  sort_dedup(L_, in, n, kb, swap, full && full->n ? full->keys.as<uint64_t>() : nullptr,
              full ? full->n : 0, out.keys.as<uint64_t>(), d_small_.as<uint64_t>(), s,
              hd ? head->keys.as<uint64_t>() : nullptr, hd ? head->n : 0);
   prof_end(pid, 0, (double)n);
@@ -625,8 +627,8 @@ void Database::sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, 
     // keys once; packing reads the input; the dedup pass reads the sorted
     // keys and writes the distinct ones (plus one probe word per key into
     // FULL when the delta is fused).
-    const double ks = 2 * bits_ <= 32 ? 4 : 8;
-    const double passes = (2 * bits_ + 7) / 8;
+    const double ks = 2 * kb <= 32 ? 4 : 8;
+    const double passes = (2 * kb + L_.radix_bits - 1) / L_.radix_bits;
     kev_[pid].bytes = passes * 2 * ks * n + 8.0 * n + ks * n + ks * n + 8.0 * out.n +
                       (diff ? 8.0 * n : 0);
   }
@@ -640,6 +642,13 @@ void Database::upload_inputs() {
   }
   dom_max_ = mx;
   bits_ = value_bits(mx);
+  for (auto& kv : rels_) {
+    Relation& r = *kv.second;
+    if (r.arity <= 2) continue;
+    const int total = r.arity * bits_;
+    r.pack_bits = total <= 64 ? bits_ : 0;
+    r.pack_half = total <= 64 ? (total + 1) / 2 : 0;
+  }
   for (auto& kv : rels_) {
     Relation& r = *kv.second;
     if (!r.loaded) continue;

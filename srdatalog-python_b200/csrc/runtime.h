@@ -120,6 +120,12 @@ struct Relation {
   // other permutations are dropped whenever HEAD changes and are rebuilt from
   // the merged canonical array on demand.
   bool lsm = false;
+  // Materialised relations of arity 3 or 4: a tuple is stored as one uint64,
+  // its columns (in index order) packed pack_bits apiece into P and split at
+  // pack_half bits, key = (P >> pack_half) << 32 | (P mod 2^pack_half), so
+  // key order is tuple order and the binary-key sort, difference and merge
+  // apply unchanged.  pack_half = 0: the tuple does not fit 64 bits.
+  int pack_bits = 0, pack_half = 0;
   Index head;
   // Every compute_delta_index makes a new DELTA (delta_epoch).  full_epoch is
   // the last one any permutation of FULL has absorbed, base_epoch the one
@@ -299,7 +305,7 @@ class Database {
   void ensure_hash(Index& ix);
   void ensure_bitmaps(Index& ix);
   void sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full,
-                 const Index* head = nullptr);
+                 const Index* head = nullptr, int key_bits = 0);
   void exec_ops(const Step& st, uint64_t iteration);
   void exec_pipeline(const Op& op, bool recursive, uint64_t iteration);
   void op_rebuild(const Step& st, size_t pos, const Op& op);

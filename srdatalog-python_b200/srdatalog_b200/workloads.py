@@ -208,3 +208,26 @@ def lsqb_q6_inputs(n_persons: int, m_knows: int, seed: int, tags: int = 200) -> 
   p = np.repeat(np.arange(n_persons, dtype=np.uint32), k)
   t = rng.integers(0, tags, p.shape[0], dtype=np.uint32)
   return {'KnowsInput': knows, 'HasInterestInput': _dedup_in_order(p, t)}
+
+
+def lsqb_q3_inputs(n_persons: int, m_knows: int, seed: int, cities: int = 40,
+                   countries: int = 4) -> dict:
+  '''Inputs of LSQB Q3 (examples/lsqb_q3_triangle.py): uniform Knows pairs,
+  every person in one city, every city in one country (ids of cities and
+  countries start after the persons', as one id space).'''
+  rng = _rng(seed)
+  knows = uniform_edges(n_persons, m_knows, seed)
+  person = np.arange(n_persons, dtype=np.uint32)
+  city = (n_persons + rng.integers(0, cities, n_persons)).astype(np.uint32)
+  cid = np.arange(n_persons, n_persons + cities, dtype=np.uint32)
+  country = (n_persons + cities + rng.integers(0, countries, cities)).astype(np.uint32)
+  return {'KnowsInput': knows, 'IsLocatedInInput': np.stack([person, city], 1),
+          'IsPartOfInput': np.stack([cid, country], 1)}
+
+
+def lsqb_q6_nosj_inputs(n_persons: int, m_knows: int, seed: int, tags: int = 200) -> dict:
+  '''Inputs of the Q6 variant without self-join (examples/lsqb_q6_nosj.py):
+  Q6's inputs plus a second, independent Knows.'''
+  inp = lsqb_q6_inputs(n_persons, m_knows, seed, tags)
+  inp['KnowsInput2'] = uniform_edges(n_persons, m_knows, seed + 1000)
+  return inp

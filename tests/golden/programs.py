@@ -199,6 +199,81 @@ def lsqb_q6_program() -> Program:
   ])
 
 
+def lsqb_q3_program() -> Program:
+  '''LSQB Q3 (examples/lsqb_q3_triangle.py): triangles of Knows whose three
+  people live in cities of one country; the arity-3 Triangle is
+  materialised (nine atoms, a three-source column join on the country).'''
+  knows_in = Relation('KnowsInput', 2, column_types=(int, int), input_file='Person_knows_Person.csv')
+  loc_in = Relation('IsLocatedInInput', 2, column_types=(int, int),
+                    input_file='Person_isLocatedIn_City.csv')
+  part_in = Relation('IsPartOfInput', 2, column_types=(int, int), input_file='City_isPartOf_Country.csv')
+  knows = Relation('Knows', 2, column_types=(int, int))
+  loc = Relation('IsLocatedIn', 2, column_types=(int, int))
+  part = Relation('IsPartOf', 2, column_types=(int, int))
+  tri = Relation('Triangle', 3, column_types=(int, int, int), print_size=True)
+  c, c1, c2, c3, co = Var('c'), Var('c1'), Var('c2'), Var('c3'), Var('co')
+  p, p1, p2, p3, x, y = Var('p'), Var('p1'), Var('p2'), Var('p3'), Var('x'), Var('y')
+  return Program(rules=[
+    (knows(x, y) <= knows_in(x, y)).named('KnowsLoad'),
+    (loc(p, c) <= loc_in(p, c)).named('LocLoad'),
+    (part(c, co) <= part_in(c, co)).named('PartOfLoad'),
+    (tri(p1, p2, p3)
+     <= knows(p1, p2) & knows(p2, p3) & knows(p3, p1)
+     & loc(p1, c1) & loc(p2, c2) & loc(p3, c3)
+     & part(c1, co) & part(c2, co) & part(c3, co))
+    .named('LabeledTriangle').with_plan(var_order=['p1', 'p2', 'p3', 'c1', 'c2', 'c3', 'co']),
+  ])
+
+
+def _two_hop(second: str | None, count: bool, negate: bool = False):
+  knows_in = Relation('KnowsInput', 2, column_types=(int, int), input_file='Person_knows_Person.csv')
+  interest_in = Relation('HasInterestInput', 2, column_types=(int, int),
+                         input_file='Person_hasInterest_Tag.csv')
+  knows = Relation('Knows', 2, column_types=(int, int))
+  has_interest = Relation('HasInterest', 2, column_types=(int, int))
+  path = Relation('Path', 4, column_types=(int, int, int, int), print_size=True)
+  p, p1, p2, p3, t, x, y = (Var(n) for n in ('p', 'p1', 'p2', 'p3', 't', 'x', 'y'))
+  rules = [(knows(x, y) <= knows_in(x, y)).named('KnowsLoad')]
+  hop2 = knows
+  if second:
+    knows2_in = Relation('KnowsInput2', 2, column_types=(int, int), input_file='Person_knows_Person.csv')
+    hop2 = Relation(second, 2, column_types=(int, int))
+    rules.append((hop2(x, y) <= knows2_in(x, y)).named(second + 'Load'))
+  rules.append((has_interest(p, t) <= interest_in(p, t)).named('InterestLoad'))
+  body = knows(p1, p2) & hop2(p2, p3) & has_interest(p3, t)
+  if negate:
+    body = body & ~knows(p1, p3)
+  body = body & Filter(('p1', 'p3'), 'return p1 != p3;')
+  return path, p1, p2, p3, t, body, rules
+
+
+def lsqb_q6_2hop_program() -> Program:
+  '''LSQB Q6 two-hop (examples/lsqb_q6_2hop.py): the arity-4 Path of
+  people two Knows hops apart with an interest of the last one, p1 != p3,
+  materialised.'''
+  path, p1, p2, p3, t, body, rules = _two_hop(None, False)
+  return Program(rules=rules + [
+    (path(p1, p2, p3, t) <= body).named('TwoHopPath').with_plan(var_order=['p1', 'p2', 'p3', 't'])])
+
+
+def lsqb_q6_nosj_program() -> Program:
+  '''LSQB Q6 without self-join (examples/lsqb_q6_nosj.py): the second hop
+  over a second copy of Knows.'''
+  path, p1, p2, p3, t, body, rules = _two_hop('Knows2', False)
+  return Program(rules=rules + [
+    (path(p1, p2, p3, t) <= body).named('TwoHopPath').with_plan(var_order=['p1', 'p2', 'p3', 't'])])
+
+
+def lsqb_q9_program() -> Program:
+  '''LSQB Q9 (examples/lsqb_q9_neg2hop.py): two-hop paths whose ends do not
+  know each other, counted: a negation of a binary relation on two bound
+  variables in a count-only arity-4 rule.'''
+  path, p1, p2, p3, t, body, rules = _two_hop(None, True, negate=True)
+  return Program(rules=rules + [
+    (path(p1, p2, p3, t) <= body).named('NegPath')
+    .with_plan(var_order=['p2', 'p3', 'p1', 't']).with_count()])
+
+
 def reach_avoid_program() -> Program:
   '''Reachability that avoids blocked edges, and the blocked pairs that are
   not reachable: negation of a binary relation on two bound variables, once
@@ -228,4 +303,8 @@ PROGRAMS = {
   'lsqb_q7': (lsqb_q7_program, 'LsqbQ7Plan', 'integration/lsqb_q7_optional.mir.sexpr'),
   'lsqb_q6': (lsqb_q6_program, 'LsqbQ6Plan', 'integration/lsqb_q6_count.mir.sexpr'),
   'reach_avoid': (reach_avoid_program, 'ReachAvoidPlan', None),
+  'lsqb_q3': (lsqb_q3_program, 'LsqbQ3Plan', 'integration/lsqb_q3_triangle.mir.sexpr'),
+  'lsqb_q6_2hop': (lsqb_q6_2hop_program, 'LsqbQ62HopPlan', 'integration/lsqb_q6_2hop.mir.sexpr'),
+  'lsqb_q6_nosj': (lsqb_q6_nosj_program, 'LsqbQ6NosjPlan', 'integration/lsqb_q6_nosj.mir.sexpr'),
+  'lsqb_q9': (lsqb_q9_program, 'LsqbQ9Plan', None),
 }

@@ -351,3 +351,45 @@ def test_tuning_options_keep_results(expected, radix_bits, jbpsm):
   t.load_rows('KnowsInput', W.rmat_edges(14, 1 << 18, seed=5))
   t.run()
   assert t.count('TriangleJoin') == expected['triangle_rmat14']['count']
+
+
+@pytest.mark.parametrize('n,m,seed', [(60, 400, 0), (3000, 60_000, 1)])
+def test_lsqb_q3_materialised_arity3(n, m, seed):
+  '''LSQB Q3: a materialised arity-3 relation (packed keys), nine atoms, a
+  three-source column join; bit-exact against the set restatement.'''
+  inp = W.lsqb_q3_inputs(n, m, seed)
+  db = run('lsqb_q3', inp)
+  want = np.array(oracle.lsqb_q3(inp), np.uint32).reshape(-1, 3)
+  assert db.size('Triangle') == want.shape[0]
+  assert oracle.dump_hash(db.dump('Triangle')) == oracle.dump_hash(want)
+  assert db.hash('Triangle') == oracle.dump_hash(want)
+
+
+@pytest.mark.parametrize('plan_name,second', [('lsqb_q6_2hop', None), ('lsqb_q6_nosj', 'KnowsInput2')])
+@pytest.mark.parametrize('n,m,seed', [(40, 150, 0), (3000, 30_000, 1)])
+def test_lsqb_two_hop_materialised_arity4(plan_name, second, n, m, seed):
+  inp = (W.lsqb_q6_nosj_inputs if second else W.lsqb_q6_inputs)(n, m, seed)
+  db = run(plan_name, inp)
+  want = np.array(sorted(oracle.lsqb_two_hop(inp, second)), np.uint32).reshape(-1, 4)
+  assert db.size('Path') == want.shape[0]
+  assert oracle.dump_hash(db.dump('Path')) == oracle.dump_hash(want)
+
+
+@pytest.mark.parametrize('n,m,seed', [(40, 150, 0), (5000, 40_000, 2)])
+def test_lsqb_q9_negated_two_hop_count(n, m, seed):
+  inp = W.lsqb_q6_inputs(n, m, seed)
+  db = run('lsqb_q9', inp)
+  assert db.count('NegPath') == len(oracle.lsqb_two_hop(inp, negate=True))
+
+
+def test_arity4_beyond_64_bits_is_refused():
+  '''Four columns of 20-bit values do not pack into 64 bits: the run fails
+  with a clear status instead of truncating.'''
+  inp = W.lsqb_q6_inputs(40, 150, 0)
+  inp['HasInterestInput'] = np.concatenate([inp['HasInterestInput'],
+                                            np.array([[3, 1_000_000]], np.uint32)])
+  db = native.Database(load_plan('lsqb_q6_2hop'))
+  for rel, rows in inp.items():
+    db.load_rows(rel, rows)
+  with pytest.raises(native.SrdlError, match='arity x value bits'):
+    db.run()

@@ -53,6 +53,30 @@ def test_lsqb_q6_interpreter_vs_closed_form(seed):
 
 
 @pytest.mark.parametrize('seed', [0, 1, 2])
+def test_lsqb_q3_interpreter_vs_sets(seed):
+  '''LSQB Q3: the materialised arity-3 Triangle of the plan interpreter equals
+  the set restatement.'''
+  inp = W.lsqb_q3_inputs(50, 400, seed, cities=8, countries=2)
+  got, _ = oracle.run_plan(load_plan('lsqb_q3'), inp)
+  assert sorted(got['Triangle']) == oracle.lsqb_q3(inp)
+
+
+@pytest.mark.parametrize('seed', [0, 1])
+def test_lsqb_two_hop_variants_interpreter_vs_sets(seed):
+  '''LSQB Q6 two-hop and no-self-join (materialised arity-4 Path) and Q9
+  (count with a negated binary relation): interpreter == set restatement of
+  the plans the reference's planner emits.'''
+  inp = W.lsqb_q6_inputs(40, 150, seed, tags=6)
+  got, _ = oracle.run_plan(load_plan('lsqb_q6_2hop'), inp)
+  assert set(got['Path']) == oracle.lsqb_two_hop(inp)
+  nosj = W.lsqb_q6_nosj_inputs(40, 150, seed, tags=6)
+  got, _ = oracle.run_plan(load_plan('lsqb_q6_nosj'), nosj)
+  assert set(got['Path']) == oracle.lsqb_two_hop(nosj, 'KnowsInput2')
+  _, counts = oracle.run_plan(load_plan('lsqb_q9'), inp)
+  assert counts['NegPath'] == len(oracle.lsqb_two_hop(inp, negate=True))
+
+
+@pytest.mark.parametrize('seed', [0, 1, 2])
 def test_reach_avoid_interpreter_vs_sets(seed):
   '''Negation on two bound variables (inside a recursive join and in a later
   stratum): interpreter == set restatement.'''
