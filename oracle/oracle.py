@@ -432,6 +432,19 @@ def lsqb_q3(inputs: dict) -> list:
   return sorted(out)
 
 
+def triangle3(a, b, c) -> list:
+  '''Z(x,y,z) <= A(x,y), B(y,z), C(z,x) (examples/debug_triangle.py:55-59;
+  examples/gen_jit_code.py:39-43 with A = B = C = Edge), by Python sets.'''
+  ab, bb, cb = _adj(a), _adj(b), _adj(c)
+  out = []
+  for x, ys in ab.items():
+    for y in ys:
+      for z in bb.get(y, ()):
+        if x in cb.get(z, ()):
+          out.append((x, y, z))
+  return sorted(out)
+
+
 def lsqb_two_hop(inputs: dict, second: str | None = None, negate: bool = False,
                  as_planned: bool = True) -> set:
   '''Path of examples/lsqb_q6_2hop.py:66-85 (second hop over a second Knows

@@ -225,13 +225,14 @@ def lsqb_q3_program() -> Program:
   ])
 
 
-def _two_hop(second: str | None, count: bool, negate: bool = False):
+def _two_hop(second: str | None, count: bool, negate: bool = False, path_name: str = 'Path',
+             print_size: bool = True):
   knows_in = Relation('KnowsInput', 2, column_types=(int, int), input_file='Person_knows_Person.csv')
   interest_in = Relation('HasInterestInput', 2, column_types=(int, int),
                          input_file='Person_hasInterest_Tag.csv')
   knows = Relation('Knows', 2, column_types=(int, int))
   has_interest = Relation('HasInterest', 2, column_types=(int, int))
-  path = Relation('Path', 4, column_types=(int, int, int, int), print_size=True)
+  path = Relation(path_name, 4, column_types=(int, int, int, int), print_size=print_size)
   p, p1, p2, p3, t, x, y = (Var(n) for n in ('p', 'p1', 'p2', 'p3', 't', 'x', 'y'))
   rules = [(knows(x, y) <= knows_in(x, y)).named('KnowsLoad')]
   hop2 = knows
@@ -274,6 +275,76 @@ def lsqb_q9_program() -> Program:
     .with_plan(var_order=['p2', 'p3', 'p1', 't']).with_count()])
 
 
+def lsqb_q6_bg_program() -> Program:
+  '''LSQB Q6 with the block-group plan hint (examples/lsqb_q6_bg_test.py):
+  the no-self-join two-hop into an arity-4 PathBG, variables ordered p2
+  first.'''
+  path, p1, p2, p3, t, body, rules = _two_hop('Knows2', False, path_name='PathBG', print_size=False)
+  return Program(rules=rules + [
+    (path(p1, p2, p3, t) <= body).named('TwoHopBG')
+    .with_plan(var_order=['p2', 'p3', 'p1', 't'], block_group=True)])
+
+
+def _triangle3(names, rule_name: str) -> Program:
+  '''A directed triangle materialised into an arity-3 relation:
+  Z(x,y,z) <= A(x,y), B(y,z), C(z,x) over binary relations without input
+  files (loaded as rows).'''
+  rels = {n: Relation(n, 2, column_types=(int, int)) for n in dict.fromkeys(names[:3])}
+  z_rel = Relation(names[3], 3, column_types=(int, int, int))
+  a, b, c = (rels[n] for n in names[:3])
+  x, y, z = Var('x'), Var('y'), Var('z')
+  return Program(rules=[
+    (z_rel(x, y, z) <= a(x, y) & b(y, z) & c(z, x)).named(rule_name)
+    .with_plan(var_order=['x', 'y', 'z'])])
+
+
+def debug_triangle_program() -> Program:
+  '''examples/debug_triangle.py: ZRel(x,y,z) <= RRel(x,y), SRel(y,z), TRel(z,x).'''
+  return _triangle3(('RRel', 'SRel', 'TRel', 'ZRel'), 'TriangleDebug')
+
+
+def gen_jit_triangle_program() -> Program:
+  '''examples/gen_jit_code.py: Z(x,y,z) <= Edge(x,y), Edge(y,z), Edge(z,x).'''
+  return _triangle3(('Edge', 'Edge', 'Edge', 'Z'), 'Triangle')
+
+
+def tc_2level_bg_program() -> Program:
+  '''examples/tc_2level_bg.py: TC with Path as a Device2LevelIndex and the
+  recursive rule planned y, x, z with the block-group hint.'''
+  arc = Relation('ArcInput', 2, column_types=(int, int), input_file='Arc.csv')
+  edge = Relation('Edge', 2, column_types=(int, int))
+  path = Relation('Path', 2, column_types=(int, int), print_size=True,
+                  index_type='SRDatalog::GPU::Device2LevelIndex')
+  x, y, z = Var('x'), Var('y'), Var('z')
+  return Program(rules=[
+    (edge(x, y) <= arc(x, y)).named('EdgeLoad'),
+    (path(x, y) <= edge(x, y)).named('TCBase'),
+    (path(x, z) <= path(x, y) & edge(y, z)).named('TCRec')
+    .with_plan(delta=0, var_order=['y', 'x', 'z'], block_group=True),
+  ])
+
+
+def print_mir_program() -> Program:
+  '''examples/print_mir.py: the Andersen rules over relations without input
+  files, the Load rule's second delta planned z, w, x, y.'''
+  address_of, assign, load, store = (_bin(n) for n in ('AddressOf', 'Assign', 'Load', 'Store'))
+  points_to = _bin('PointsTo')
+  w, x, y, z = Var('w'), Var('x'), Var('y'), Var('z')
+  return Program(rules=[
+    (points_to(y, x) <= address_of(y, x)).named('Base').with_plan(var_order=['y', 'x']),
+    (points_to(y, x) <= points_to(z, x) & assign(y, z))
+    .named('Assign').with_plan(var_order=['z', 'x', 'y']),
+    (points_to(y, w) <= points_to(x, z) & load(y, x) & points_to(z, w))
+    .named('Load')
+    .with_plan(delta=0, var_order=['x', 'z', 'y', 'w'])
+    .with_plan(delta=2, var_order=['z', 'w', 'x', 'y']),
+    (points_to(z, w) <= points_to(y, z) & store(y, x) & points_to(x, w))
+    .named('Store')
+    .with_plan(delta=0, var_order=['y', 'x', 'z', 'w'])
+    .with_plan(delta=2, var_order=['x', 'y', 'w', 'z']),
+  ])
+
+
 def reach_avoid_program() -> Program:
   '''Reachability that avoids blocked edges, and the blocked pairs that are
   not reachable: negation of a binary relation on two bound variables, once
@@ -306,5 +377,11 @@ PROGRAMS = {
   'lsqb_q3': (lsqb_q3_program, 'LsqbQ3Plan', 'integration/lsqb_q3_triangle.mir.sexpr'),
   'lsqb_q6_2hop': (lsqb_q6_2hop_program, 'LsqbQ62HopPlan', 'integration/lsqb_q6_2hop.mir.sexpr'),
   'lsqb_q6_nosj': (lsqb_q6_nosj_program, 'LsqbQ6NosjPlan', 'integration/lsqb_q6_nosj.mir.sexpr'),
-  'lsqb_q9': (lsqb_q9_program, 'LsqbQ9Plan', None),
+  'lsqb_q9': (lsqb_q9_program, 'LsqbQ9Plan', 'integration/lsqb_q9_neg2hop.mir.sexpr'),
+  'lsqb_q6_bg': (lsqb_q6_bg_program, 'LsqbQ6BgPlan', 'integration/lsqb_q6_bg_test.mir.sexpr'),
+  'debug_triangle': (debug_triangle_program, 'DebugTrianglePlan',
+                     'integration/debug_triangle.mir.sexpr'),
+  'gen_jit_triangle': (gen_jit_triangle_program, 'GenJitPlan', 'integration/gen_jit_code.mir.sexpr'),
+  'tc_2level_bg': (tc_2level_bg_program, 'Tc2LevelBgPlan', 'integration/tc_2level_bg.mir.sexpr'),
+  'print_mir': (print_mir_program, 'PrintMirPlan', 'integration/print_mir.mir.sexpr'),
 }

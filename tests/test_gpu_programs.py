@@ -393,3 +393,46 @@ def test_arity4_beyond_64_bits_is_refused():
     db.load_rows(rel, rows)
   with pytest.raises(native.SrdlError, match='arity x value bits'):
     db.run()
+
+
+@pytest.mark.parametrize('n,m,seed', [(30, 200, 0), (2000, 40_000, 1)])
+def test_arity3_triangle_programs(n, m, seed):
+  '''examples/debug_triangle.py and gen_jit_code.py: directed triangles
+  materialised into arity-3 relations, from rows loaded straight into
+  relations without input files.'''
+  r, s, t = (W.uniform_edges(n, m, seed + k) for k in (1, 2, 3))
+  db = run('debug_triangle', {'RRel': r, 'SRel': s, 'TRel': t})
+  want = np.array(oracle.triangle3(r, s, t), np.uint32).reshape(-1, 3)
+  assert db.size('ZRel') == want.shape[0]
+  assert oracle.dump_hash(db.dump('ZRel')) == oracle.dump_hash(want)
+  db = run('gen_jit_triangle', {'Edge': r})
+  want = np.array(oracle.triangle3(r, r, r), np.uint32).reshape(-1, 3)
+  assert db.size('Z') == want.shape[0]
+  assert oracle.dump_hash(db.dump('Z')) == oracle.dump_hash(want)
+
+
+def test_tc_2level_bg_program(expected):
+  exp = expected['tc_mid']
+  db = run('tc_2level_bg', {'ArcInput': W.uniform_edges(2000, 6000, 7)})
+  assert db.size('Path') == exp['size']
+  assert oracle.dump_hash(db.dump('Path')) == exp['sha256']
+
+
+def test_lsqb_q6_bg_program():
+  inp = W.lsqb_q6_nosj_inputs(3000, 30_000, 3)
+  db = run('lsqb_q6_bg', inp)
+  want = np.array(sorted(oracle.lsqb_two_hop(inp, 'KnowsInput2', as_planned=False)),
+                  np.uint32).reshape(-1, 4)
+  assert db.size('PathBG') == want.shape[0]
+  assert oracle.dump_hash(db.dump('PathBG')) == oracle.dump_hash(want)
+
+
+@pytest.mark.parametrize('n,m,seed', [(50, 140, 0), (1000, 1600, 2)])
+def test_print_mir_program(n, m, seed):
+  '''examples/print_mir.py: the Andersen rules with another plan for Load's
+  second delta, against the naive restatement.'''
+  inp = W.andersen_inputs(n, m, seed)
+  db = run('print_mir', inp)
+  want = np.array(oracle.andersen(inp), np.uint32).reshape(-1, 2)
+  assert db.size('PointsTo') == want.shape[0]
+  assert oracle.dump_hash(db.dump('PointsTo')) == oracle.dump_hash(want)

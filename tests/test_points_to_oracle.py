@@ -76,6 +76,29 @@ def test_lsqb_two_hop_variants_interpreter_vs_sets(seed):
   assert counts['NegPath'] == len(oracle.lsqb_two_hop(inp, negate=True))
 
 
+@pytest.mark.parametrize('seed', [0, 1])
+def test_more_reference_programs_interpreter_vs_sets(seed):
+  '''debug_triangle / gen_jit_code (arity-3 Z), tc_2level_bg, lsqb_q6_bg_test
+  and print_mir (the Andersen rules with other plans): the plan interpreter
+  equals the set restatements.'''
+  r, s, t = (W.uniform_edges(30, 200, seed + k) for k in (1, 2, 3))
+  got, _ = oracle.run_plan(load_plan('debug_triangle'), {'RRel': r, 'SRel': s, 'TRel': t})
+  assert sorted(got['ZRel']) == oracle.triangle3(r, s, t)
+  e = W.uniform_edges(30, 250, seed + 4)
+  got, _ = oracle.run_plan(load_plan('gen_jit_triangle'), {'Edge': e})
+  assert sorted(got['Z']) == oracle.triangle3(e, e, e)
+  e = W.uniform_edges(50, 120, seed + 6)
+  got, _ = oracle.run_plan(load_plan('tc_2level_bg'), {'ArcInput': e})
+  keys, _, _ = oracle.tc(e)
+  assert len(got['Path']) == keys.shape[0]
+  inp = W.lsqb_q6_nosj_inputs(40, 150, seed + 5, tags=6)
+  got, _ = oracle.run_plan(load_plan('lsqb_q6_bg'), inp)
+  assert set(got['PathBG']) == oracle.lsqb_two_hop(inp, 'KnowsInput2', as_planned=False)
+  inp = W.andersen_inputs(40, 120, seed + 7)
+  got, _ = oracle.run_plan(load_plan('print_mir'), inp)
+  assert sorted(got['PointsTo']) == sorted(oracle.andersen(inp))
+
+
 @pytest.mark.parametrize('seed', [0, 1, 2])
 def test_reach_avoid_interpreter_vs_sets(seed):
   '''Negation on two bound variables (inside a recursive join and in a later
