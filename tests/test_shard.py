@@ -127,6 +127,33 @@ def test_local_exchange_moves_keys_to_owners():
     assert vote == total
 
 
+def test_local_exchange_abort_releases_the_other_shards():
+  '''A shard whose run fails aborts the exchange: the shards waiting in the
+  barrier get an error at once instead of waiting for it.'''
+  import threading
+  import time
+  from srdatalog_b200.shard import LocalExchange
+  ex = LocalExchange(3, timeout=60, copy=_host_copy)
+  errors = []
+
+  def waiting(r):
+    counts = (ctypes.c_uint64 * 3)(1, 1, 1)
+    try:
+      ex.callback(r)(0, 'R', counts, 0, 0, 0)
+    except threading.BrokenBarrierError as e:
+      errors.append(e)
+
+  ths = [threading.Thread(target=waiting, args=(r,)) for r in (0, 1)]
+  t0 = time.monotonic()
+  for t in ths:
+    t.start()
+  time.sleep(0.2)
+  ex.abort()  # shard 2 failed before reaching the exchange
+  for t in ths:
+    t.join(timeout=30)
+  assert len(errors) == 2 and time.monotonic() - t0 < 30
+
+
 def test_marked_plans_load_in_native_library():
   from srdatalog_b200 import native
   for name in PLANS:
