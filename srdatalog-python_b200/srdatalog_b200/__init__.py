@@ -19,6 +19,7 @@ from .loader import (SHIM_ENTRY_POINTS, EntryPoint, JitRuntime, build_and_load,
                      gen_runtime_shim_template)
 from .native import Database, SrdlError
 from .plan import PlanError, plan_from_mir, plan_from_program, validate_plan
+from .plugin import IndexPlugin, PluginError, register_index_plugin, resolve_plugin
 
 __version__ = '0.1.0'
 
@@ -26,5 +27,6 @@ __all__ = [
   'BuildResult', 'CompileResult', 'CompilerConfig', 'build_project', 'compile_jit_project',
   'write_project', 'EntryPoint', 'JitRuntime', 'build_and_load', 'gen_runtime_shim_template',
   'SHIM_ENTRY_POINTS', 'Database', 'SrdlError', 'PlanError', 'plan_from_mir',
-  'plan_from_program', 'validate_plan',
+  'plan_from_program', 'validate_plan', 'IndexPlugin', 'PluginError', 'register_index_plugin',
+  'resolve_plugin',
 ]

@@ -28,6 +28,8 @@ import json
 import warnings
 from typing import Any
 
+from .plugin import runtime_index_type
+
 PLAN_VERSION = 1
 
 
@@ -145,6 +147,8 @@ def plan_from_mir(mir_program: Any, relation_decls: list, name: str,
 
   `canonical` maps relation -> canonical index (the reference merges the
   per-stratum maps, later strata winning: src/srdatalog/pipeline.py:112-116).
+  Each relation's `index_type` is resolved through the index-plugin
+  registry (`srdatalog_b200.plugin`) to the runtime policy's string.
   '''
   canonical = dict(canonical or {})
   rels = []
@@ -155,7 +159,7 @@ def plan_from_mir(mir_program: Any, relation_decls: list, name: str,
       'arity': arity,
       'input_file': d.input_file or '',
       'print_size': bool(d.print_size),
-      'index_type': d.index_type or '',
+      'index_type': runtime_index_type(d.index_type or ''),
       'canonical': list(canonical.get(d.rel_name, list(range(arity)))),
     })
   steps = [_step(p, rec) for (p, rec) in mir_program.steps]
