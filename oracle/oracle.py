@@ -197,6 +197,9 @@ def run_plan(plan: dict, inputs: dict, max_iters: int = 0):
   db = {(n, v): set() for n in rels for v in ('FULL', 'DELTA', 'NEW')}
   for name, rows in inputs.items():
     db[(name, 'FULL')] = {tuple(int(x) for x in r) for r in np.asarray(rows).reshape(-1, rels[name]['arity'])}
+  for name, r in rels.items():
+    # rows the plan carries (the one-tuple relations of head constants)
+    db[(name, 'FULL')] |= {tuple(int(x) for x in row) for row in r.get('facts', ())}
   counts: dict[str, int] = {}
   cap = max_iters or (2**31 - 1)
 
@@ -495,3 +498,28 @@ def reach_avoid(edges: np.ndarray, blocked: np.ndarray) -> dict:
     reach |= new
     frontier = new
   return {'Reach': sorted(reach), 'Cut': sorted(p for p in blk if p not in reach)}
+
+
+def head_const(edges: np.ndarray, sources: np.ndarray) -> list:
+  '''Mark of the head_const test program, by Python sets: (r, 7) for every
+  node r reachable from a source (sources included), (x, 9) for every edge
+  (x, y) whose target y is such a node.'''
+  succ: dict = {}
+  pairs = [tuple(e) for e in np.asarray(edges).reshape(-1, 2).tolist()]
+  for a, b in pairs:
+    succ.setdefault(a, set()).add(b)
+  reach = set(np.asarray(sources).reshape(-1).tolist())
+  frontier = set(reach)
+  while frontier:
+    frontier = {z for y in frontier for z in succ.get(y, ())} - reach
+    reach |= frontier
+  return sorted({(r, 7) for r in reach} | {(x, 9) for x, y in pairs if y in reach})
+
+
+def rewrite_consts(in3: np.ndarray, in2: np.ndarray) -> dict:
+  '''P and Q of the reference's rewrite_consts program
+  (tests/test_rule_rewrite.py:99): P = {x | (x, 42, 99) in In},
+  Q = {(x, 7) | x in In2}.'''
+  p = {(int(r[0]),) for r in np.asarray(in3).reshape(-1, 3) if r[1] == 42 and r[2] == 99}
+  q = {(int(x), 7) for x in np.asarray(in2).reshape(-1)}
+  return {'P': sorted(p), 'Q': sorted(q)}

@@ -252,8 +252,23 @@ void Database::parse_plan(const std::string& plan_json) {
     rel->canonical = r.at("canonical").ints();
     SRDL_REQUIRE((int)rel->canonical.size() == rel->arity, kErrPlan,
                  "plan: canonical index arity mismatch for " + rel->name);
+    if (r.has("facts")) {
+      for (auto& row : r.at("facts").a()) {
+        const auto& vals = row.a();
+        SRDL_REQUIRE((int)vals.size() == rel->arity, kErrPlan,
+                     "plan: facts row of the wrong arity for " + rel->name);
+        for (auto& x : vals) {
+          SRDL_REQUIRE(x.i() >= 0 && x.i() <= 0xffffffffLL, kErrPlan,
+                       "plan: facts value out of range for " + rel->name);
+          rel->facts.push_back((uint32_t)x.i());
+        }
+      }
+    }
     if (!rel->input_file.empty()) inputs_.push_back(rel->name);
-    rels_[rel->name] = std::move(rel);
+    const std::string name = rel->name;
+    const bool has_facts = !rel->facts.empty();
+    rels_[name] = std::move(rel);
+    if (has_facts) stage_facts(*rels_[name]);
   }
   for (auto& sj : p.at("steps").a()) {
     Step st;
@@ -365,9 +380,14 @@ Relation& Database::rel(const std::string& name) {
 }
 
 bool Database::any_loaded() const {
+  // rows a plan carries (facts) do not count as loaded inputs
   for (auto& kv : rels_)
-    if (kv.second->loaded) return true;
+    if (kv.second->loaded && kv.second->facts.empty()) return true;
   return false;
+}
+
+void Database::stage_facts(Relation& r) {
+  load_rows(r.name, r.facts.data(), r.facts.size() / r.arity);
 }
 
 // ------------------------------------------------------------------ device
@@ -550,6 +570,7 @@ void Database::clear_inputs() {
     r.dstaged_n = 0;
     r.dstaged_max = 0;
     r.loaded = false;
+    if (!r.facts.empty()) stage_facts(r);
   }
 }
 

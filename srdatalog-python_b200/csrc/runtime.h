@@ -101,6 +101,7 @@ struct Relation {
   std::string index_type;
   std::vector<int> canonical;
   RelVersion v[3];
+  std::vector<uint32_t> facts;   // rows the plan itself carries (head constants), row-major
   std::vector<uint32_t> staged;  // host rows loaded before run (row-major)
   uint32_t staged_max = 0;       // largest value in `staged` (kept as rows are added)
   uint32_t* pinned = nullptr;    // page-locked copy of `staged` used for the upload
@@ -235,6 +236,7 @@ class Database {
   int64_t dump(const std::string& rel, uint32_t* out, uint64_t cap_rows);
   std::string stats_json() const;
   bool any_loaded() const;
+  void stage_facts(Relation& r);
   uint64_t staged_rows(const std::string& name) {
     Relation& r = rel(name);
     return r.staged.size() / r.arity + r.dstaged_n;

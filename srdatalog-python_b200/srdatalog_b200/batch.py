@@ -11,8 +11,8 @@ cover all instances that still have a delta; instances that converged early
 simply contribute nothing -- and instance j's result is read back as the
 rows whose first column lies in its range.
 
-Requirements checked here: the plan's filters use no constants (a constant
-would have to be shifted per instance), and the union's values fit in
+Requirements checked here: the plan's filters and rule heads use no
+constants (a constant would have to be shifted per instance), and the union's values fit in
 uint32.  Count-only rules are counted per instance too: the count of every
 binding is also added to the group of its first variable's value
 (srdl_set_count_groups), and each instance is one group.
@@ -38,7 +38,11 @@ def count_rules(plan: dict) -> list:
 
 
 def check_batchable(plan: dict) -> None:
-  '''Reject plans whose filters compare with constants.'''
+  '''Reject plans whose filters compare with constants or whose rule
+  heads hold constants (relations with facts).'''
+  for r in plan['relations']:
+    if r.get('facts'):
+      raise BatchError(f'relation {r["name"]}: a head constant prevents value shifting')
   for step in plan['steps']:
     for op in step['ops']:
       if op['op'] != 'execute_pipeline':

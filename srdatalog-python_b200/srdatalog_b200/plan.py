@@ -13,13 +13,17 @@ Plan layout (version 1)::
 
   {"version": 1, "name": <project>,
    "relations": [{"name", "arity", "input_file", "print_size",
-                  "index_type", "canonical": [cols]}],
+                  "index_type", "canonical": [cols], ["facts": [[v, ...], ...]]}],
    "steps": [{"recursive": bool, "ops": [op, ...]}]}
 
 op kinds: execute_pipeline, rebuild_index, clear_relation, check_size,
 compute_delta_index, merge_index, rebuild_index_from_index,
 post_stratum_reconstruct, inject_cpp_hook (kept, not executed).  Pipeline
 ops: scan, column_join, cartesian_join, filter, negation, insert_into.
+
+A MIR `constant-bind` (a head constant, mir/types.py:99-109) becomes a
+column join over a one-tuple relation `__const_<value>` whose tuple the plan
+carries in "facts"; the runtime loads facts when it reads the plan.
 '''
 
 from __future__ import annotations
@@ -31,6 +35,7 @@ from typing import Any
 from .plugin import runtime_index_type
 
 PLAN_VERSION = 1
+CONST_PREFIX = '__const_'
 
 
 class PlanError(ValueError):
@@ -79,10 +84,50 @@ def _pipeline_op(node: Any) -> dict:
       raise PlanError(f'negation on {node.rel_name} with constant arguments is not supported')
     return {'op': 'negation', 'rel': node.rel_name, 'ver': _ver(node.version),
             'index': [int(c) for c in node.index], 'prefix': list(node.prefix_vars)}
+  if kind == 'ConstantBind':
+    # binding v to a literal = joining with the one-tuple relation {(value)}
+    value = _const_literal(node)
+    return {'op': 'column_join', 'var': node.var_name,
+            'sources': [{'rel': f'{CONST_PREFIX}{value}', 'ver': 'FULL', 'index': [0],
+                         'prefix': []}]}
   if kind == 'InsertInto':
     return {'op': 'insert_into', 'rel': node.rel_name, 'ver': _ver(node.version),
             'vars': list(node.vars), 'index': [int(c) for c in node.index]}
   raise PlanError(f'pipeline op {kind} is not supported by this runtime')
+
+
+def _const_literal(node: Any) -> int:
+  '''Value of a constant-bind whose code is an unsigned 32-bit literal
+  (optionally `return <n>;` or parenthesised); other code is rejected.'''
+  code = node.code.strip()
+  if code.startswith('return') and code.endswith(';'):
+    code = code[len('return'):-1].strip()
+  code = code.strip('()').strip()
+  if code[-1:] in ('u', 'U'):
+    code = code[:-1]
+  if not code.isdigit() or int(code) >= 2**32:
+    raise PlanError(f'constant-bind of {node.var_name}: code {node.code!r} is not an unsigned '
+                    '32-bit literal')
+  return int(code)
+
+
+def _const_relations(steps: list, declared: set) -> list:
+  '''The one-tuple relations that lowered constant-binds read.'''
+  values = set()
+  for st in steps:
+    for op in st['ops']:
+      for p in op.get('pipeline', ()):
+        for s in p.get('sources', ()):
+          if s['rel'].startswith(CONST_PREFIX):
+            values.add(int(s['rel'][len(CONST_PREFIX):]))
+  out = []
+  for v in sorted(values):
+    name = f'{CONST_PREFIX}{v}'
+    if name in declared:
+      raise PlanError(f'relation name {name} is reserved for head constants')
+    out.append({'name': name, 'arity': 1, 'input_file': '', 'print_size': False,
+                'index_type': '', 'canonical': [0], 'facts': [[v]]})
+  return out
 
 
 def _instr(node: Any) -> dict:
@@ -163,6 +208,7 @@ def plan_from_mir(mir_program: Any, relation_decls: list, name: str,
       'canonical': list(canonical.get(d.rel_name, list(range(arity)))),
     })
   steps = [_step(p, rec) for (p, rec) in mir_program.steps]
+  rels += _const_relations(steps, {r['name'] for r in rels})
   plan = {'version': PLAN_VERSION, 'name': name, 'relations': rels, 'steps': steps}
   validate_plan(plan)
   return plan
@@ -222,6 +268,10 @@ def validate_plan(plan: dict) -> None:
   if plan.get('version') != PLAN_VERSION:
     raise PlanError('plan version mismatch')
   arity = {r['name']: r['arity'] for r in plan['relations']}
+  for r in plan['relations']:
+    for row in r.get('facts', ()):
+      if len(row) != r['arity'] or not all(isinstance(x, int) and 0 <= x < 2**32 for x in row):
+        raise PlanError(f'facts of {r["name"]}: {row!r} is not a row of {r["arity"]} uint32 values')
   for st in plan['steps']:
     for op in st['ops']:
       if op['op'] == 'inject_cpp_hook':

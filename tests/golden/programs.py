@@ -362,6 +362,38 @@ def reach_avoid_program() -> Program:
   ])
 
 
+def rewrite_consts_program() -> Program:
+  '''Body and head constants (the reference's tests/test_rule_rewrite.py:99,
+  MIR pinned by tests/fixtures/rewrite_consts.mir.sexpr): P(x) <= In(x, 42, 99)
+  lowers to a filter, Q(x, 7) <= In2(x) to a constant-bind.'''
+  x = Var('x')
+  inp = Relation('In', 3)
+  in2 = Relation('In2', 1)
+  p = Relation('P', 1)
+  q = Relation('Q', 2)
+  return Program(rules=[
+    (p(x) <= inp(x, 42, 99)).named('BodyConst'),
+    (q(x, 7) <= in2(x)).named('HeadConst'),
+  ])
+
+
+def head_const_program() -> Program:
+  '''Head and body constants inside a recursive stratum: nodes reachable
+  from the sources are tagged 7, their predecessors 9.  No reference fixture
+  pins it (its constant-binds have the shape of rewrite_consts' HeadConst).'''
+  arc = Relation('ArcInput', 2, column_types=(int, int), input_file='Arc.csv')
+  src = Relation('SourceInput', 1, column_types=(int,), input_file='Source.csv')
+  edge = Relation('Edge', 2, column_types=(int, int))
+  mark = Relation('Mark', 2, column_types=(int, int), print_size=True)
+  x, y = Var('x'), Var('y')
+  return Program(rules=[
+    (edge(x, y) <= arc(x, y)).named('EdgeLoad'),
+    (mark(x, 7) <= src(x)).named('MarkSource'),
+    (mark(y, 7) <= mark(x, 7) & edge(x, y)).named('MarkStep'),
+    (mark(x, 9) <= edge(x, y) & mark(y, 7)).named('MarkPred'),
+  ])
+
+
 # name -> (builder, project name, reference MIR fixture or None)
 PROGRAMS = {
   'tc': (tc_program, 'TcPlan', 'tc.mir.sexpr'),
@@ -384,4 +416,6 @@ PROGRAMS = {
   'gen_jit_triangle': (gen_jit_triangle_program, 'GenJitPlan', 'integration/gen_jit_code.mir.sexpr'),
   'tc_2level_bg': (tc_2level_bg_program, 'Tc2LevelBgPlan', 'integration/tc_2level_bg.mir.sexpr'),
   'print_mir': (print_mir_program, 'PrintMirPlan', 'integration/print_mir.mir.sexpr'),
+  'rewrite_consts': (rewrite_consts_program, 'RewriteConstsPlan', 'rewrite_consts.mir.sexpr'),
+  'head_const': (head_const_program, 'HeadConstPlan', None),
 }

@@ -30,10 +30,21 @@ def test_library_exports_every_header_symbol():
   assert lib.srdl_version() == 1
 
 
-@pytest.mark.parametrize('name', ['tc', 'sg', 'triangle', 'tc_left', 'tc_lsm'])
+@pytest.mark.parametrize('name', ['tc', 'sg', 'triangle', 'tc_left', 'tc_lsm', 'head_const',
+                                  'rewrite_consts'])
 def test_open_committed_plans(name):
   db = native.Database(load_plan(name))
   db.close()
+
+
+def test_plan_facts_checked_by_the_loader():
+  h = ctypes.c_void_p()
+  lib = native.lib()
+  for facts, msg in ([[7, 1]], 'wrong arity'), ([[-1]], 'out of range'), ([[2**32]], 'out of range'):
+    plan = load_plan('head_const')
+    next(r for r in plan['relations'] if r['name'] == '__const_7')['facts'] = facts
+    assert lib.srdl_open(json.dumps(plan).encode(), 0, ctypes.byref(h)) == 4
+    assert msg in native.last_error()
 
 
 def test_plan_errors():

@@ -334,6 +334,24 @@ def test_reach_avoid_negation(n, m, seed):
     assert oracle.dump_hash(db.dump(rel)) == oracle.dump_hash(w), rel
 
 
+@pytest.mark.parametrize('n,m,seed', [(60, 90, 0), (3000, 7000, 3)])
+def test_head_constants(n, m, seed):
+  '''Head constants (constant-bind joins over the plan's one-tuple
+  relations) and body constants, inside a recursive stratum; a second run
+  after clear_inputs still sees the plan's facts.'''
+  e = W.uniform_edges(n, m, seed)
+  src = np.array([[seed], [seed + 11]], np.uint32)
+  want = np.array(oracle.head_const(e, src), np.uint32).reshape(-1, 2)
+  db = native.Database(load_plan('head_const'))
+  for _ in range(2):
+    db.clear_inputs()
+    db.load_rows('ArcInput', e)
+    db.load_rows('SourceInput', src)
+    db.run()
+    assert db.size('Mark') == want.shape[0]
+    assert oracle.dump_hash(db.dump('Mark')) == oracle.dump_hash(want)
+
+
 @pytest.mark.parametrize('radix_bits,jbpsm', [(5, 8), (6, 32), (7, 16), (8, 1)])
 def test_tuning_options_keep_results(expected, radix_bits, jbpsm):
   '''The autotuner's sort-digit and join-grid knobs change no result.'''
