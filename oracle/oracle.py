@@ -216,6 +216,17 @@ def run_plan(plan: dict, inputs: dict, max_iters: int = 0):
         out.add(t[col])
     return out
 
+  def tuples(src, bind, iteration, k):
+    # distinct values of the k index columns after the prefix
+    ver = src['ver']
+    if ver == 'DELTA' and iteration == 0:
+      ver = 'FULL'
+    idx = src['index']
+    pre = [bind[v] for v in src['prefix']]
+    cols = idx[len(pre):len(pre) + k]
+    return {tuple(t[c] for c in cols) for t in db[(src['rel'], ver)]
+            if all(t[idx[i]] == pre[i] for i in range(len(pre)))}
+
   def execute(op, iteration):
     binds = [dict()]
     for p in op['pipeline']:
@@ -247,15 +258,24 @@ def run_plan(plan: dict, inputs: dict, max_iters: int = 0):
             c[p['var']] = v
             nb.append(c)
       elif k == 'cartesian_join':
+        # a source binds the len(vars) columns after its prefix, in index
+        # order (a ternary source under one bound column binds two); an
+        # empty var list only requires the prefix to be present
         for b in binds:
           lists = []
+          empty = False
           for s, vars_ in zip(p['sources'], p['var_from_source']):
+            vs = tuples(s, b, iteration, max(1, len(vars_)))
+            empty |= not vs
             if vars_:
-              lists.append((vars_[0], sorted(values(s, b, iteration))))
+              lists.append((vars_, sorted(vs)))
+          if empty:
+            continue
           for combo in itertools.product(*[lst for _, lst in lists]):
             c = dict(b)
-            for (v, _), val in zip(lists, combo):
-              c[v] = val
+            for (vars_, _), vals in zip(lists, combo):
+              for v, val in zip(vars_, vals):
+                c[v] = val
             nb.append(c)
       elif k == 'filter':
         ev = _filter_fn(p['code'])
@@ -523,3 +543,52 @@ def rewrite_consts(in3: np.ndarray, in2: np.ndarray) -> dict:
   p = {(int(r[0]),) for r in np.asarray(in3).reshape(-1, 3) if r[1] == 42 and r[2] == 99}
   q = {(int(x), 7) for x in np.asarray(in2).reshape(-1)}
   return {'P': sorted(p), 'Q': sorted(q)}
+
+
+def galen(inputs: dict) -> dict:
+  '''OutP and OutQ of the Galen program (examples/galen.py rules LoadP ..
+  Join3c), by naive iteration over Python sets until nothing changes.'''
+  def rows(name, k):
+    return {tuple(int(x) for x in r) for r in np.asarray(inputs[name]).reshape(-1, k).tolist()}
+  p_in, s_in = rows('PInput', 2), rows('SInput', 2)
+  q_in, r_in, c_in, u_in = (rows(n, 3) for n in ('QInput', 'RInput', 'CInput', 'UInput'))
+  out_p, out_q = set(p_in), set(q_in)
+  s_by, r_by, u_by = {}, {}, {}
+  for r, q in s_in:
+    s_by.setdefault(r, set()).add(q)
+  for y, u, e in r_in:
+    r_by.setdefault(y, set()).add((u, e))
+  for w, r, z in u_in:
+    u_by.setdefault(w, set()).add((r, z))
+  while True:
+    p_from, q_from, q_xry = {}, {}, {}
+    for x, y in out_p:
+      p_from.setdefault(x, set()).add(y)
+    for x, r, z in out_q:
+      q_from.setdefault(x, set()).add((r, z))
+      q_xry.setdefault((r, z), set()).add(x)
+    new_p, new_q = set(), set()
+    for x, y in out_p:
+      for z in p_from.get(y, ()):                        # TC
+        new_p.add((x, z))
+      for r, z in q_from.get(y, ()):                     # PropQ
+        new_q.add((x, r, z))
+    for y, w in out_p:                                   # Join3a: OutQ(x, r, y)
+      for r, z in u_by.get(w, ()):
+        for x in q_xry.get((r, y), ()):
+          new_p.add((x, z))
+    for y, w, z in c_in:                                 # Join3b
+      for x, ys in p_from.items():
+        if w in ys and y in ys:
+          new_p.add((x, z))
+    for x, r, z in out_q:
+      for q in s_by.get(r, ()):                          # PropQS
+        new_q.add((x, q, z))
+      for u, e in r_by.get(r, ()):                       # Join3c, y = r
+        for uu, o in q_from.get(z, ()):
+          if uu == u:
+            new_q.add((x, e, o))
+    if new_p <= out_p and new_q <= out_q:
+      return {'OutP': sorted(out_p), 'OutQ': sorted(out_q)}
+    out_p |= new_p
+    out_q |= new_q

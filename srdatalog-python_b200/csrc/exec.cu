@@ -87,9 +87,51 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
     SRDL_REQUIRE(it != slot.end(), kErrPlan, "rule " + op.rule + ": unbound variable " + v);
     return it->second;
   };
+  // Ternary relations are stored in their canonical column order only; a
+  // read in another order goes through that order's pair / row views.
+  auto ternary = [&](const SourceDesc& d) -> Split3& {
+    Relation& r = rel(d.rel);
+    Ver v = (d.ver == kDelta && recursive && iteration == 0) ? kFull : d.ver;
+    SRDL_REQUIRE(r.pack_half > 0, kErrUnsupported,
+                 "relation " + r.name + ": ternary reads need arity x value bits <= 64");
+    return ensure_split(r, ensure_index(r, v, r.canonical), d.index);
+  };
+  auto rows_src = [&](const SourceDesc& d) {
+    SRDL_REQUIRE(d.prefix.size() <= 1, kErrUnsupported,
+                 "rule " + op.rule + ": ternary rows read with " + std::to_string(d.prefix.size()) +
+                     " bound columns");
+    Split3& sp = ternary(d);
+    SrcSpec s;
+    s.mode = kSrcRows;
+    s.t = view2(sp.rows);
+    s.pair = view2(sp.pair);
+    s.prefix_slot = d.prefix.empty() ? -1 : slot_of(d.prefix[0]);
+    return s;
+  };
   auto make_src = [&](const SourceDesc& d, bool probed) {
     Relation& r = rel(d.rel);
     Ver v = (d.ver == kDelta && recursive && iteration == 0) ? kFull : d.ver;
+    if (r.arity == 3) {
+      SRDL_REQUIRE(d.prefix.size() <= 2, kErrPlan, "rule " + op.rule + ": prefix too long on " + r.name);
+      Split3& sp = ternary(d);
+      SrcSpec s;
+      if (d.prefix.size() <= 1) {
+        // c0 or c1 as the next value: the pair index read as a binary relation
+        if (probed && !d.prefix.empty() && v == kFull) {
+          ensure_hash(sp.pair);
+          ensure_bitmaps(sp.pair);
+        }
+        s.t = view2(sp.pair);
+        s.prefix_slot = d.prefix.empty() ? -1 : slot_of(d.prefix[0]);
+      } else {
+        s.mode = kSrcPair;
+        s.t = view2(sp.rows);
+        s.pair = view2(sp.pair);
+        s.prefix_slot = slot_of(d.prefix[0]);
+        s.prefix_slot2 = slot_of(d.prefix[1]);
+      }
+      return s;
+    }
     SRDL_REQUIRE(r.arity <= 2, kErrUnsupported, "join over relation " + r.name + " of arity > 2");
     SRDL_REQUIRE(d.prefix.size() < (size_t)std::max(r.arity, 2), kErrUnsupported,
                  "rule " + op.rule + ": prefix too long on " + r.name);
@@ -150,7 +192,12 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
       const SourceDesc& d = po.sources[0];
       lv.kind = kScan;
       lv.nsrc = 1;
-      lv.src[0] = make_src(d, false);
+      if (rel(d.rel).arity == 3) {
+        lv.src[0] = rows_src(d);
+        lv.wide = 1;
+      } else {
+        lv.src[0] = make_src(d, false);
+      }
       SRDL_REQUIRE(po.vars.size() == d.index.size(), kErrPlan, "scan arity mismatch");
       for (size_t j = d.prefix.size(); j < po.vars.size(); j++) lv.scan_slot[j] = bind(po.vars[j]);
     } else if (po.kind == PipeOp::ColumnJoin) {
@@ -158,20 +205,39 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
       SRDL_REQUIRE(po.sources.size() <= (size_t)kMaxSrc && !po.sources.empty(), kErrUnsupported,
                    "column join with too many sources");
       // every list but the per-row shortest is probed: hash the long ones
-      for (auto& d : po.sources) lv.src[lv.nsrc++] = make_src(d, po.sources.size() > 1);
+      for (auto& d : po.sources) {
+        lv.src[lv.nsrc] = make_src(d, po.sources.size() > 1);
+        if (lv.src[lv.nsrc].mode != kSrcPlain) lv.wide = 1;
+        lv.nsrc++;
+      }
       lv.cj_slot = bind(po.var);
     } else {
       lv.kind = kCartesian;
       SRDL_REQUIRE(po.sources.size() <= (size_t)kMaxSrc, kErrUnsupported, "cartesian too wide");
       for (size_t i = 0; i < po.sources.size(); i++) {
-        lv.src[lv.nsrc] = make_src(po.sources[i], false);
         const auto& vs = i < po.var_from_source.size() ? po.var_from_source[i]
                                                         : std::vector<std::string>{};
-        SRDL_REQUIRE(vs.size() <= 1, kErrUnsupported, "cartesian source binding several variables");
-        lv.src[lv.nsrc].out_slot = vs.empty() ? -1 : bind(vs[0]);
+        const SourceDesc& d = po.sources[i];
+        if (vs.size() == 2 && rel(d.rel).arity == 3) {
+          // a ternary source under one bound column binds the other two
+          SRDL_REQUIRE(d.prefix.size() == 1, kErrUnsupported,
+                       "rule " + op.rule + ": ternary source binding two variables needs one bound column");
+          lv.src[lv.nsrc] = rows_src(d);
+          lv.src[lv.nsrc].out_slot = bind(vs[0]);
+          lv.src[lv.nsrc].out_slot2 = bind(vs[1]);
+        } else {
+          SRDL_REQUIRE(vs.size() <= 1, kErrUnsupported, "cartesian source binding several variables");
+          lv.src[lv.nsrc] = make_src(d, false);
+          lv.src[lv.nsrc].out_slot = vs.empty() ? -1 : bind(vs[0]);
+        }
+        if (lv.src[lv.nsrc].mode != kSrcPlain) lv.wide = 1;
         lv.nsrc++;
       }
     }
+    // the expand kernels hold the values a level binds in kMaxSrc + 1 registers
+    SRDL_REQUIRE(nslots - lv.n_in_slots <= kMaxSrc + 1, kErrUnsupported,
+                 "rule " + op.rule + ": a join level binds more than " + std::to_string(kMaxSrc + 1) +
+                     " variables");
     levels.push_back(lv);
   }
   SRDL_REQUIRE(insert && !levels.empty(), kErrPlan, "rule " + op.rule + ": no insert_into");
@@ -387,6 +453,8 @@ void Database::op_rebuild(const Step& st, size_t pos, const Op& op) {
 
 void Database::op_compute_delta(const Op& op) {
   Relation& r = rel(op.rel);
+  SRDL_REQUIRE(r.arity <= 2 || op.index == r.canonical, kErrUnsupported,
+               "relation " + r.name + " of arity > 2: delta in a non-canonical order");
   r.v[kDelta].clear();
   r.delta_epoch++;
   if (r.pending_delta) {
@@ -425,6 +493,7 @@ void Database::op_compute_delta(const Op& op) {
 
 void Database::op_merge(const Op& op) {
   Relation& r = rel(op.rel);
+  if (r.arity > 2 && op.index != r.canonical) return;  // stored in the canonical order only
   if (r.arity > 2) {
     auto it = r.v[kDelta].idx.find(op.index);
     if (r.pack_half == 0 || it == r.v[kDelta].idx.end() || it->second.n == 0) {
@@ -619,7 +688,13 @@ void Database::exec_ops(const Step& st, uint64_t it) {
       case Op::CheckSize: break;
       case Op::ComputeDelta: op_compute_delta(op); break;
       case Op::Merge: op_merge(op); break;
-      case Op::RebuildFrom: ensure_index(rel(op.rel), op.ver, op.index); break;
+      case Op::RebuildFrom: {
+        // relations of arity > 2 keep their canonical order only (other
+        // orders are derived views, built when a join reads them)
+        Relation& r = rel(op.rel);
+        if (r.arity <= 2) ensure_index(r, op.ver, op.index);
+        break;
+      }
       case Op::Reconstruct: break;
       case Op::Hook: break;
       case Op::Exchange: op_exchange(op); break;

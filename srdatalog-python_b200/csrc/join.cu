@@ -31,11 +31,46 @@
 namespace srdl {
 
 constexpr int kJThreads = 256;
-// List of source s for input row r: [b, b+len) over roots (no prefix) or
-// over child values (prefix bound).
+constexpr uint32_t kNoPair = 0xffffffffu;
+
+// Position of the pair (a, b) in a pair index (a binary view whose row
+// positions number the pairs), or kNoPair.
+__device__ __forceinline__ uint32_t pair_pos(const TrieView& p, uint32_t a, uint32_t b) {
+  uint32_t kb, ke;
+  trie_range(p, a, kb, ke);
+  const uint32_t q = lower_bound_u32(p.lo, kb, ke, b);
+  return (q < ke && p.lo[q] == b) ? q : kNoPair;
+}
+
+// First row of a row index whose pair position is >= g (g <= pair count).
+__device__ __forceinline__ uint32_t rows_from(const TrieView& t, uint32_t g) {
+  if (t.dir && g < t.dir_n) return t.dir[g];
+  return (uint32_t)lower_bound_u64(t.keys, 0, t.n, (uint64_t)g << 32);
+}
+
+// List of source s for input row r: [b, b+len) over roots (no prefix), over
+// child values (prefix bound), or, for the ternary modes, over the row
+// index's children of a pair (kSrcPair) or its rows under a range of pairs
+// (kSrcRows).
 __device__ __forceinline__ void src_list(const SrcSpec& s, const Table& in, uint64_t r,
                                          uint32_t& b, uint32_t& len) {
-  if (s.prefix_slot < 0) {
+  if (s.mode == kSrcPair) {
+    const uint32_t g = pair_pos(s.pair, in.col[s.prefix_slot][r], in.col[s.prefix_slot2][r]);
+    uint32_t e = 0;
+    b = 0;
+    if (g != kNoPair) trie_range(s.t, g, b, e);
+    len = e - b;
+  } else if (s.mode == kSrcRows) {
+    if (s.prefix_slot < 0) {
+      b = 0;
+      len = (uint32_t)s.t.n;
+    } else {
+      uint32_t kb, ke;
+      trie_range(s.pair, in.col[s.prefix_slot][r], kb, ke);
+      b = rows_from(s.t, kb);
+      len = rows_from(s.t, ke) - b;
+    }
+  } else if (s.prefix_slot < 0) {
     b = 0;
     len = (uint32_t)*s.t.n_roots_d;
   } else {
@@ -51,6 +86,10 @@ __device__ __forceinline__ uint32_t src_value(const SrcSpec& s, uint32_t pos) {
 
 __device__ __forceinline__ bool src_contains(const SrcSpec& s, const Table& in, uint64_t r,
                                              uint32_t v) {
+  if (s.mode == kSrcPair) {
+    const uint32_t g = pair_pos(s.pair, in.col[s.prefix_slot][r], in.col[s.prefix_slot2][r]);
+    return g != kNoPair && trie_child_contains(s.t, g, v);
+  }
   if (s.prefix_slot < 0) return trie_has_root(s.t, v);
   return trie_child_contains(s.t, in.col[s.prefix_slot][r], v);
 }
@@ -141,7 +180,11 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
       work[r] = prod;
     } else {  // scan
       const SrcSpec& s = lv.src[0];
-      if (s.prefix_slot < 0) {
+      if (s.mode == kSrcRows) {
+        uint32_t b, len;
+        src_list(s, in, r, b, len);
+        work[r] = len;
+      } else if (s.prefix_slot < 0) {
         work[r] = s.t.n;
       } else {
         uint32_t b, e;
@@ -476,18 +519,35 @@ __global__ void __launch_bounds__(kJThreads) join_expand_kernel(
             src_list(sp, in, r, b, len);
             const uint32_t idx = (uint32_t)(rem % len);
             rem /= len;
-            nv[sp.out_slot - lv.n_in_slots] = src_value(sp, b + idx);
+            if (sp.mode == kSrcRows) {
+              // a ternary row under the bound c0: c1 from the pair index, c2 from the row
+              const uint32_t i = b + idx;
+              nv[sp.out_slot - lv.n_in_slots] = sp.pair.lo[(uint32_t)(sp.t.keys[i] >> 32)];
+              nv[sp.out_slot2 - lv.n_in_slots] = sp.t.lo[i];
+            } else {
+              nv[sp.out_slot - lv.n_in_slots] = src_value(sp, b + idx);
+            }
           }
         } else {
           const SrcSpec& sp = lv.src[0];
-          uint32_t b = 0;
-          if (sp.prefix_slot >= 0) {
-            uint32_t e;
-            trie_range(sp.t, in.col[sp.prefix_slot][r], b, e);
+          if (sp.mode == kSrcRows) {
+            uint32_t b, len;
+            src_list(sp, in, r, b, len);
+            const uint32_t i = b + (uint32_t)local;
+            const uint32_t g = (uint32_t)(sp.t.keys[i] >> 32);
+            if (lv.scan_slot[0] >= 0) nv[lv.scan_slot[0] - lv.n_in_slots] = (uint32_t)(sp.pair.keys[g] >> 32);
+            if (lv.scan_slot[1] >= 0) nv[lv.scan_slot[1] - lv.n_in_slots] = sp.pair.lo[g];
+            if (lv.scan_slot[2] >= 0) nv[lv.scan_slot[2] - lv.n_in_slots] = sp.t.lo[i];
+          } else {
+            uint32_t b = 0;
+            if (sp.prefix_slot >= 0) {
+              uint32_t e;
+              trie_range(sp.t, in.col[sp.prefix_slot][r], b, e);
+            }
+            const uint64_t i = b + local;
+            if (lv.scan_slot[0] >= 0) nv[lv.scan_slot[0] - lv.n_in_slots] = (uint32_t)(sp.t.keys[i] >> 32);
+            if (lv.scan_slot[1] >= 0) nv[lv.scan_slot[1] - lv.n_in_slots] = (uint32_t)sp.t.keys[i];
           }
-          const uint64_t i = b + local;
-          if (lv.scan_slot[0] >= 0) nv[lv.scan_slot[0] - lv.n_in_slots] = (uint32_t)(sp.t.keys[i] >> 32);
-          if (lv.scan_slot[1] >= 0) nv[lv.scan_slot[1] - lv.n_in_slots] = (uint32_t)sp.t.keys[i];
         }
       }
       auto val = [&](int slot) -> uint32_t {
@@ -657,7 +717,7 @@ JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scrat
   w.drv = s.take<uint8_t>(in.n ? in.n : 1);
   w.beg = s.take<uint32_t>(in.n ? in.n : 1);
   w.orange = s.take<uint2>(in.n ? in.n : 1);
-  if (lv.kind == kColumnJoin && lv.nsrc == 2 && (lv.src[0].t.bdir || lv.src[1].t.bdir))
+  if (lv.kind == kColumnJoin && lv.nsrc == 2 && !lv.wide && (lv.src[0].t.bdir || lv.src[1].t.bdir))
     w.obm = s.take<uint32_t>(in.n ? in.n : 1);
   if (in.n) {
     join_count_kernel<<<jgrid(in.n, L), kJThreads, 0, L.stream>>>(lv, in, work, w.drv,
@@ -678,7 +738,7 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
   const uint64_t warps = (uint64_t)g * (kJThreads / 32);
   const uint64_t chunk = ((total + warps - 1) / warps + 31) & ~uint64_t(31);
   Table out = out_table ? *out_table : Table{};
-  if (lv.kind == kColumnJoin && lv.nsrc == 2 && lv.nfilt == 0) {
+  if (lv.kind == kColumnJoin && lv.nsrc == 2 && lv.nfilt == 0 && !lv.wide) {
 #define SRDL_CJ2(MODE, WC)                                                                   \
   (lv.seg ? join_cj2_kernel<MODE, true><<<g, kJThreads, 0, L.stream>>>(                       \
                 lv, in, w.offs, w.drv, w.beg, w.orange, w.obm, total, chunk, out, out_keys, cnt, WC) \
@@ -704,7 +764,8 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
     SRDL_CUDA(cudaGetLastError());
     return;
   }
-  if (lv.kind == kCartesian && lv.nsrc == 2 && lv.src[0].out_slot >= 0 && lv.src[1].out_slot >= 0) {
+  if (lv.kind == kCartesian && lv.nsrc == 2 && lv.src[0].out_slot >= 0 && lv.src[1].out_slot >= 0 &&
+      !lv.wide) {
 #define SRDL_CART2(MODE, WC)                                                                 \
   (lv.seg ? join_cart2_kernel<MODE, true><<<g, kJThreads, 0, L.stream>>>(                     \
                 lv, in, w.offs, w.beg, w.orange, total, chunk, out, out_keys, cnt, WC)          \

@@ -124,6 +124,19 @@ size_t shard_select_scratch_bytes(uint64_t n);
 void shard_select(const Launch& L, const uint64_t* keys, uint64_t n, bool col0_lo, uint32_t world,
                   uint32_t dest, uint64_t* out, uint64_t* d_nout, Scratch& s);
 
+// Ternary relations: keys pack a tuple (x0, x1, x2) `bits` apiece into P and
+// split it at `half` bits, (P >> half) << 32 | (P mod 2^half).
+// repack3: the tuples of `in` with their columns reordered, out column j =
+// in column sel[j] (out is not sorted).
+void repack3(const Launch& L, const uint64_t* in, uint64_t n, int bits, int half, const int sel[3],
+             uint64_t* out);
+// split3: for sorted unique packed keys, pair_keys = the distinct (x0, x1) as
+// x0 << 32 | x1 (room for n; the count goes to *d_npairs) and row_keys[i] =
+// (position of row i's pair in pair_keys) << 32 | x2.  Both come out sorted.
+size_t split3_scratch_bytes(uint64_t n);
+void split3(const Launch& L, const uint64_t* keys, uint64_t n, int bits, int half,
+            uint64_t* pair_keys, uint64_t* row_keys, uint64_t* d_npairs, Scratch& s);
+
 // Swap the two 32-bit halves of every key (index permutation (1,0) <-> (0,1)).
 void swap_halves(const Launch& L, const uint64_t* in, uint64_t n, uint64_t* out);
 
@@ -141,10 +154,24 @@ enum LevelKind : int { kColumnJoin = 0, kCartesian = 1, kScan = 2 };
 enum EmitKind : int { kEmitTable = 0, kEmitKeys = 1, kEmitCount = 2 };
 enum FiltOp : int { kNe = 0, kEq = 1, kLt = 2, kLe = 3, kGt = 4, kGe = 5 };
 
+// Sources over a ternary relation read two binary views of it, built per
+// column order (c0, c1, c2): the pair index P = the distinct (c0, c1) as
+// keys, and the row index R = (position of the row's (c0, c1) in P) << 32 | c2.
+// With no or one bound column a source reads P like a binary relation
+// (kSrcPlain).  kSrcPair: c0 and c1 bound (prefix_slot, prefix_slot2); the
+// list is R's children of the pair's position.  kSrcRows: the rows of R under
+// P's children of c0 (prefix_slot; all rows when -1), binding c1 from P
+// (out_slot) and c2 from R (out_slot2).
+enum SrcMode : int { kSrcPlain = 0, kSrcPair = 1, kSrcRows = 2 };
+
 struct SrcSpec {
   TrieView t;
   int prefix_slot = -1;  // binding slot holding the prefix value, -1: no prefix (roots)
   int out_slot = -1;     // cartesian: slot this source binds (-1: existence only)
+  int mode = kSrcPlain;
+  int prefix_slot2 = -1;  // kSrcPair: slot of the second bound column
+  int out_slot2 = -1;     // kSrcRows: slot bound to c2
+  TrieView pair;          // kSrcPair / kSrcRows: the pair index P (t is R)
 };
 
 struct FiltSpec {
@@ -165,7 +192,8 @@ struct LevelSpec {
   int nsrc = 0;
   SrcSpec src[kMaxSrc];
   int cj_slot = -1;                     // column join: slot of the joined variable
-  int scan_slot[2] = {-1, -1};          // scan: slots for index columns 0 and 1
+  int scan_slot[3] = {-1, -1, -1};      // scan: slots for index columns 0, 1 (and 2: kSrcRows)
+  int wide = 0;                         // a source is kSrcPair / kSrcRows: generic kernels only
   int nfilt = 0;
   FiltSpec filt[kMaxFilt];
   int n_in_slots = 0;                   // slots bound by the input table

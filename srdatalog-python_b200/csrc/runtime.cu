@@ -516,8 +516,8 @@ void Database::reset_device_state() {
 void Database::load_rows(const std::string& name, const uint32_t* rows, uint64_t n) {
   Relation& r = rel(name);
   SRDL_REQUIRE(rows || n == 0, kErrArg, "load_rows: null rows");
-  SRDL_REQUIRE(r.arity <= 2, kErrUnsupported,
-               "relation " + name + ": only arity 1 and 2 relations can be materialised");
+  SRDL_REQUIRE(r.arity <= 4, kErrUnsupported,
+               "relation " + name + ": only relations of arity 1 to 4 can be loaded");
   r.staged.insert(r.staged.end(), rows, rows + n * r.arity);
   // The value bound is taken once here, not on every run (a run re-uploads
   // the rows but never rescans them on the host).
@@ -625,6 +625,7 @@ void Database::sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, 
   const int kb = key_bits > 0 ? key_bits : bits_;
   out.keys = DevBuf(std::max<uint64_t>(n, 1) * 8, L_.stream);
   out.trie = false;
+  out.split.clear();
   if (n == 0) {
     out.n = 0;
     return;
@@ -705,15 +706,31 @@ void Database::upload_inputs() {
         SRDL_CUDA(cudaMemcpyAsync(raw.as<uint64_t>(), r.pinned, n * 8, cudaMemcpyHostToDevice,
                                   L_.stream));
       swap = (r.canonical == std::vector<int>{0, 1});
-    } else {
+    } else if (r.arity == 1) {
       std::vector<uint64_t> k(n);
       for (uint64_t i = 0; i < n; i++) k[i] = (uint64_t)r.staged[i] << 32;
       SRDL_CUDA(cudaMemcpyAsync(raw.as<uint64_t>(), k.data(), n * 8, cudaMemcpyHostToDevice,
                                 L_.stream));
       SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+    } else {
+      // arity 3-4: columns in canonical order, packed pack_bits apiece and
+      // split at pack_half bits (the layout the joins emit)
+      SRDL_REQUIRE(r.pack_half > 0, kErrUnsupported,
+                   "relation " + r.name + ": arity x value bits must be <= 64 to load it");
+      const int k = r.arity, b = r.pack_bits, h = r.pack_half;
+      std::vector<uint64_t> keys(n);
+      for (uint64_t i = 0; i < n; i++) {
+        const uint32_t* row = &r.staged[i * k];
+        uint64_t p = 0;
+        for (int j = 0; j < k; j++) p = (p << b) | row[r.canonical[j]];
+        keys[i] = ((p >> h) << 32) | (p & ((1ull << h) - 1));
+      }
+      SRDL_CUDA(cudaMemcpyAsync(raw.as<uint64_t>(), keys.data(), n * 8, cudaMemcpyHostToDevice,
+                                L_.stream));
+      SRDL_CUDA(cudaStreamSynchronize(L_.stream));
     }
     Index& ix = r.v[kFull].idx[r.canonical];
-    sort_into(ix, raw.as<uint64_t>(), n, swap, nullptr);
+    sort_into(ix, raw.as<uint64_t>(), n, swap, nullptr, nullptr, r.arity > 2 ? r.pack_half : 0);
   }
 }
 
@@ -784,9 +801,10 @@ Index& Database::ensure_index(Relation& r, Ver v, const std::vector<int>& perm) 
   return ix;
 }
 
-void Database::ensure_trie(Relation& r, Index& ix) {
+void Database::ensure_trie(Relation& r, Index& ix, int64_t hi_max) {
   (void)r;
   if (ix.trie) return;
+  const uint64_t hmax = hi_max < 0 ? (uint64_t)dom_max_ : (uint64_t)hi_max;
   const uint64_t n = ix.n;
   size_t pid = prof_begin("trie_build");
   ix.lo = DevBuf(std::max<uint64_t>(n, 1) * 4, L_.stream);
@@ -798,8 +816,8 @@ void Database::ensure_trie(Relation& r, Index& ix) {
   ix.nroots_d = DevBuf(8, L_.stream);
   build_roots(L_, ix.keys.as<uint64_t>(), n, ix.roots.as<uint32_t>(), ix.nroots_d.as<uint64_t>(), s);
   ix.dir_n = 0;
-  if ((uint64_t)dom_max_ + 2 <= kDenseDirMax) {
-    ix.dir_n = dom_max_ + 2;
+  if (hmax + 2 <= kDenseDirMax) {
+    ix.dir_n = (uint32_t)(hmax + 2);
     ix.dir = DevBuf((size_t)ix.dir_n * 4, L_.stream);
     build_dir(L_, ix.keys.as<uint64_t>(), n, ix.dir.as<uint32_t>(), ix.dir_n);
   }
@@ -909,6 +927,68 @@ void Database::ensure_bitmaps(Index& ix) {
                ix.bdir.as<uint32_t>(), ix.bpool.as<uint32_t>(), bwords,
                reinterpret_cast<unsigned int*>(cnt.as<unsigned long long>() + kBitmapLevels));
   prof_end(pid, 8.0 * ix.n + 4.0 * slots * bwords + 8.0 * ix.dir_n, (double)ix.n);
+}
+
+TrieView Database::view2(Index& ix) {
+  SRDL_REQUIRE(ix.trie, kErrState, "view of an index without its trie");
+  TrieView t;
+  t.keys = ix.keys.as<uint64_t>();
+  t.lo = ix.lo.as<uint32_t>();
+  t.roots = ix.roots.as<uint32_t>();
+  t.dir = ix.dir_n ? ix.dir.as<uint32_t>() : nullptr;
+  t.hdir = ix.hdir.bytes() ? ix.hdir.as<uint32_t>() : nullptr;
+  t.hpool = ix.hpool.bytes() ? ix.hpool.as<uint32_t>() : nullptr;
+  t.bdir = ix.bdir.bytes() ? ix.bdir.as<uint32_t>() : nullptr;
+  t.bpool = ix.bpool.bytes() ? ix.bpool.as<uint32_t>() : nullptr;
+  t.bwords = ix.bwords;
+  t.n = ix.n;
+  t.n_roots_d = ix.nroots_d.as<uint64_t>();
+  t.dir_n = ix.dir_n;
+  t.arity = 2;
+  return t;
+}
+
+// The pair and row views of a ternary relation's packed array `canon` (in the
+// relation's canonical column order) for the column order `order`: the
+// tuples are re-packed in that order and sorted when it differs, then split.
+Split3& Database::ensure_split(Relation& r, Index& canon, const std::vector<int>& order) {
+  auto it = canon.split.find(order);
+  if (it != canon.split.end()) return *it->second;
+  SRDL_REQUIRE(r.arity == 3 && r.pack_half > 0, kErrUnsupported,
+               "relation " + r.name + ": ternary reads need arity x value bits <= 64");
+  auto sp = std::make_shared<Split3>();
+  const int b = r.pack_bits, h = r.pack_half;
+  const uint64_t n = canon.n;
+  const uint64_t* keys = canon.keys.as<uint64_t>();
+  Index sorted;
+  if (order != r.canonical && n) {
+    int sel[3];
+    for (int j = 0; j < 3; j++) {
+      sel[j] = -1;
+      for (int q = 0; q < 3; q++)
+        if (r.canonical[q] == order[j]) sel[j] = q;
+      SRDL_REQUIRE(sel[j] >= 0, kErrPlan, "relation " + r.name + ": bad column order");
+    }
+    DevBuf re(n * 8, L_.stream);
+    repack3(L_, keys, n, b, h, sel, re.as<uint64_t>());
+    sort_into(sorted, re.as<uint64_t>(), n, false, nullptr, nullptr, h);
+    keys = sorted.keys.as<uint64_t>();
+  }
+  sp->pair.keys = DevBuf(std::max<uint64_t>(n, 1) * 8, L_.stream);
+  sp->rows.keys = DevBuf(std::max<uint64_t>(n, 1) * 8, L_.stream);
+  DevBuf scratch(split3_scratch_bytes(n), L_.stream);
+  Scratch s{scratch.as<char>(), scratch.bytes(), 0};
+  size_t pid = prof_begin("split3");
+  split3(L_, keys, n, b, h, sp->pair.keys.as<uint64_t>(), sp->rows.keys.as<uint64_t>(),
+         d_small_.as<uint64_t>(), s);
+  prof_end(pid, 8.0 * n + 3 * 8.0 * n + 8.0 * n, (double)n);
+  sp->pair.n = n ? read_scalar(0) : 0;
+  sp->rows.n = n;
+  ensure_trie(r, sp->pair);
+  ensure_trie(r, sp->rows, sp->pair.n ? (int64_t)sp->pair.n - 1 : 0);
+  Split3& ref = *sp;
+  canon.split[order] = std::move(sp);
+  return ref;
 }
 
 TrieView Database::view(Relation& r, Index& ix) {

@@ -60,6 +60,8 @@ class DevBuf {
   size_t cls_ = 0;  // size of the arena block backing p_
 };
 
+struct Split3;
+
 // One sorted, duplicate-free key array plus the join-side trie pieces,
 // built on first use by a join.
 struct Index {
@@ -75,6 +77,16 @@ struct Index {
   bool bitmap_done = false;  // bitmaps of long child lists built (or found unnecessary)
   DevBuf bdir, bpool;
   uint32_t bwords = 0;
+  // Ternary relations (packed keys): the pair and row views of this array in
+  // each column order a join has read it in, built on first use.
+  std::map<std::vector<int>, std::shared_ptr<Split3>> split;
+};
+
+// Read views of a ternary relation in one column order (c0, c1, c2): `pair`
+// holds the distinct (c0, c1) as binary keys, `rows` every tuple as
+// (position of its (c0, c1) in `pair`) << 32 | c2.
+struct Split3 {
+  Index pair, rows;
 };
 
 struct Chunk {
@@ -302,8 +314,11 @@ class Database {
   void compact_head(Relation& r);
   // d <- d - HEAD when d is in the canonical permutation of an LSM relation.
   void subtract_head(Relation& r, const std::vector<int>& perm, Index& d);
-  void ensure_trie(Relation& r, Index& ix);
+  // hi_max: largest first-column value of the keys (-1: the input domain's)
+  void ensure_trie(Relation& r, Index& ix, int64_t hi_max = -1);
   TrieView view(Relation& r, Index& ix);
+  TrieView view2(Index& ix);  // a binary view of derived keys (ternary pair / row views)
+  Split3& ensure_split(Relation& r, Index& canon, const std::vector<int>& order);
   void ensure_hash(Index& ix);
   void ensure_bitmaps(Index& ix);
   void sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full,

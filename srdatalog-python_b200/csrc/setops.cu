@@ -192,6 +192,89 @@ void swap_halves(const Launch& L, const uint64_t* in, uint64_t n, uint64_t* out)
   count_launches(1);
 }
 
+// ---- ternary relations: column orders and the pair / row views ---------------
+// A ternary tuple (x0, x1, x2) in some column order is one uint64 key: P =
+// x0 << 2b | x1 << b | x2, stored split at `half` bits as
+// (P >> half) << 32 | (P mod 2^half), so key order is tuple order.
+
+__device__ __forceinline__ uint64_t tern_unsplit(uint64_t k, int half) {
+  return ((k >> 32) << half) | (k & ((1ull << half) - 1));
+}
+
+__device__ __forceinline__ uint64_t tern_split(uint64_t p, int half) {
+  return ((p >> half) << 32) | (p & ((1ull << half) - 1));
+}
+
+__global__ void repack3_kernel(const uint64_t* __restrict__ in, uint64_t n, int bits, int half,
+                               int s0, int s1, int s2, uint64_t* __restrict__ out) {
+  const uint64_t mb = (1ull << bits) - 1;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t p = tern_unsplit(in[i], half);
+    const uint64_t x[3] = {p >> (2 * bits), (p >> bits) & mb, p & mb};
+    out[i] = tern_split((x[s0] << (2 * bits)) | (x[s1] << bits) | x[s2], half);
+  }
+}
+
+// flag[i] = 1 where row i starts a new (x0, x1) pair
+__global__ void split3_flag_kernel(const uint64_t* __restrict__ keys, uint64_t n, int bits, int half,
+                                   uint64_t* __restrict__ flag) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t pr = tern_unsplit(keys[i], half) >> bits;
+    flag[i] = (i == 0 || (tern_unsplit(keys[i - 1], half) >> bits) != pr) ? 1 : 0;
+  }
+}
+
+// row i's pair number = pairs started before it (excl[i]) + flag[i] - 1
+__global__ void split3_write_kernel(const uint64_t* __restrict__ keys, uint64_t n, int bits,
+                                    int half, const uint64_t* __restrict__ flag,
+                                    const uint64_t* __restrict__ excl, uint64_t* __restrict__ pair_keys,
+                                    uint64_t* __restrict__ row_keys) {
+  const uint64_t mb = (1ull << bits) - 1;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t p = tern_unsplit(keys[i], half);
+    const uint64_t g = excl[i] + flag[i] - 1;
+    row_keys[i] = (g << 32) | (p & mb);
+    if (flag[i]) pair_keys[g] = ((p >> (2 * bits)) << 32) | ((p >> bits) & mb);
+  }
+}
+
+void repack3(const Launch& L, const uint64_t* in, uint64_t n, int bits, int half, const int sel[3],
+             uint64_t* out) {
+  if (!n) return;
+  SRDL_REQUIRE(bits >= 1 && 3 * bits <= 64 && half >= 1 && half <= 32, kErrArg, "repack3: bad packing");
+  for (int j = 0; j < 3; j++) SRDL_REQUIRE(sel[j] >= 0 && sel[j] < 3, kErrArg, "repack3: bad order");
+  repack3_kernel<<<grid_for(n, L.num_sms), 256, 0, L.stream>>>(in, n, bits, half, sel[0], sel[1],
+                                                               sel[2], out);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(1);
+}
+
+size_t split3_scratch_bytes(uint64_t n) {
+  return 2 * (((n + 1) * 8 + 255) & ~size_t(255)) + scan_scratch_bytes(n) + 1024;
+}
+
+void split3(const Launch& L, const uint64_t* keys, uint64_t n, int bits, int half,
+            uint64_t* pair_keys, uint64_t* row_keys, uint64_t* d_npairs, Scratch& s) {
+  if (!n) {
+    SRDL_CUDA(cudaMemsetAsync(d_npairs, 0, 8, L.stream));
+    return;
+  }
+  SRDL_REQUIRE(bits >= 1 && 3 * bits <= 64 && half >= 1 && half <= 32, kErrArg, "split3: bad packing");
+  uint64_t* flag = s.take<uint64_t>(n + 1);
+  uint64_t* excl = s.take<uint64_t>(n + 1);
+  split3_flag_kernel<<<grid_for(n, L.num_sms), 256, 0, L.stream>>>(keys, n, bits, half, flag);
+  SRDL_CUDA(cudaGetLastError());
+  exclusive_scan_u64(L, flag, n, excl, s);
+  split3_write_kernel<<<grid_for(n, L.num_sms), 256, 0, L.stream>>>(keys, n, bits, half, flag, excl,
+                                                                    pair_keys, row_keys);
+  SRDL_CUDA(cudaGetLastError());
+  SRDL_CUDA(cudaMemcpyAsync(d_npairs, excl + n, 8, cudaMemcpyDeviceToDevice, L.stream));
+  count_launches(2);
+}
+
 // ---- partition by owning shard (exchange ops) --------------------------------
 
 // Keeps the keys whose first declared column (the key's low word when

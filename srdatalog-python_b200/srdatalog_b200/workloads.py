@@ -231,3 +231,21 @@ def lsqb_q6_nosj_inputs(n_persons: int, m_knows: int, seed: int, tags: int = 200
   inp = lsqb_q6_inputs(n_persons, m_knows, seed, tags)
   inp['KnowsInput2'] = uniform_edges(n_persons, m_knows, seed + 1000)
   return inp
+
+
+def galen_inputs(n_vals: int, m: int, seed: int) -> dict:
+  '''Inputs of the Galen program (examples/galen.py) over values
+  [0, n_vals): binary P and S, ternary Q, R, C and U, about m/6 rows each,
+  uniform and deduplicated.'''
+  rng = _rng(seed)
+  q = max(1, m // 6)
+
+  def triples() -> np.ndarray:
+    t = rng.integers(0, n_vals, (q, 3), dtype=np.uint32)
+    key = (t[:, 0].astype(np.uint64) * n_vals + t[:, 1]) * n_vals + t[:, 2]
+    _, first = np.unique(key, return_index=True)
+    first.sort()
+    return np.ascontiguousarray(t[first])
+
+  return {'PInput': _pairs(rng, n_vals, q), 'SInput': _pairs(rng, n_vals, q),
+          'QInput': triples(), 'RInput': triples(), 'CInput': triples(), 'UInput': triples()}

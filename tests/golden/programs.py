@@ -394,6 +394,32 @@ def head_const_program() -> Program:
   ])
 
 
+def galen_program() -> Program:
+  '''examples/galen.py: the Galen ontology closure over the binary OutP and
+  the ternary OutQ, with the reference's variable orders for Join3a and
+  Join3c (MIR pinned by tests/fixtures/integration/galen.mir.sexpr).'''
+  def rel(name, k, input_file=None, print_size=False):
+    return Relation(name, k, column_types=(int,) * k, input_file=input_file,
+                    print_size=print_size)
+  p_in, s_in = rel('PInput', 2, 'P.csv'), rel('SInput', 2, 'S.csv')
+  q_in, r_in = rel('QInput', 3, 'Q.csv'), rel('RInput', 3, 'R.csv')
+  c_in, u_in = rel('CInput', 3, 'C.csv'), rel('UInput', 3, 'U.csv')
+  out_p, out_q = rel('OutP', 2, print_size=True), rel('OutQ', 3, print_size=True)
+  e, o, q, r, u, w, x, y, z = (Var(n) for n in 'eoqruwxyz')
+  return Program(rules=[
+    (out_p(x, z) <= p_in(x, z)).named('LoadP'),
+    (out_q(x, r, z) <= q_in(x, r, z)).named('LoadQ'),
+    (out_p(x, z) <= out_p(x, y) & out_p(y, z)).named('TC'),
+    (out_q(x, r, z) <= out_p(x, y) & out_q(y, r, z)).named('PropQ'),
+    (out_p(x, z) <= out_p(y, w) & u_in(w, r, z) & out_q(x, r, y))
+    .named('Join3a').with_plan(delta=2, var_order=['y', 'w', 'r', 'x', 'z']),
+    (out_p(x, z) <= c_in(y, w, z) & out_p(x, w) & out_p(x, y)).named('Join3b'),
+    (out_q(x, q, z) <= out_q(x, r, z) & s_in(r, q)).named('PropQS'),
+    (out_q(x, e, o) <= out_q(x, y, z) & r_in(y, u, e) & out_q(z, u, o))
+    .named('Join3c').with_plan(delta=0, var_order=['z', 'y', 'u', 'x', 'e', 'o']),
+  ])
+
+
 # name -> (builder, project name, reference MIR fixture or None)
 PROGRAMS = {
   'tc': (tc_program, 'TcPlan', 'tc.mir.sexpr'),
@@ -418,4 +444,5 @@ PROGRAMS = {
   'print_mir': (print_mir_program, 'PrintMirPlan', 'integration/print_mir.mir.sexpr'),
   'rewrite_consts': (rewrite_consts_program, 'RewriteConstsPlan', 'rewrite_consts.mir.sexpr'),
   'head_const': (head_const_program, 'HeadConstPlan', None),
+  'galen': (galen_program, 'GalenPlan', 'integration/galen.mir.sexpr'),
 }

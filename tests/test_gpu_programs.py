@@ -352,6 +352,20 @@ def test_head_constants(n, m, seed):
     assert oracle.dump_hash(db.dump('Mark')) == oracle.dump_hash(want)
 
 
+@pytest.mark.parametrize('n,m,seed', [(12, 40, 0), (20, 120, 1), (30, 150, 2), (40, 180, 6)])
+def test_galen_ternary_joins(n, m, seed):
+  '''Galen: ternary inputs and the recursive ternary OutQ read in three
+  column orders with 0, 1 and 2 bound columns, and cartesian sources
+  binding two of its columns; bit-exact against the rules restated on sets.'''
+  inp = W.galen_inputs(n, m, seed)
+  want = oracle.galen(inp)
+  db = run('galen', inp)
+  for rel, k in (('OutP', 2), ('OutQ', 3)):
+    w = np.array(want[rel], np.uint32).reshape(-1, k)
+    assert db.size(rel) == w.shape[0], rel
+    assert oracle.dump_hash(db.dump(rel)) == oracle.dump_hash(w), rel
+
+
 @pytest.mark.parametrize('radix_bits,jbpsm', [(5, 8), (6, 32), (7, 16), (8, 1)])
 def test_tuning_options_keep_results(expected, radix_bits, jbpsm):
   '''The autotuner's sort-digit and join-grid knobs change no result.'''

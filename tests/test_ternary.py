@@ -1,0 +1,42 @@
+'''Joins over ternary relations (the Galen program, examples/galen.py, MIR
+pinned by tests/fixtures/integration/galen.mir.sexpr): the oracle
+interpreter, which binds several columns of one cartesian source, against
+a set-based restatement of the rules, and the access patterns the plan asks
+the runtime for.'''
+
+import oracle
+import pytest
+from conftest import load_plan
+from srdatalog_b200 import workloads as W
+
+CASES = [(12, 40, 0), (20, 120, 1), (30, 150, 2)]
+
+
+@pytest.mark.parametrize('n,m,seed', CASES)
+def test_galen_interpreter_vs_rules(n, m, seed):
+  inp = W.galen_inputs(n, m, seed)
+  got, _ = oracle.run_plan(load_plan('galen'), inp)
+  want = oracle.galen(inp)
+  assert got['OutP'] == want['OutP'] and got['OutQ'] == want['OutQ']
+
+
+def test_galen_access_patterns():
+  '''Ternary sources appear with 0, 1 and 2 bound columns, in three column
+  orders, and cartesian sources bind two columns of OutQ under one.'''
+  plan = load_plan('galen')
+  arity = {r['name']: r['arity'] for r in plan['relations']}
+  bound, orders, two_var = set(), set(), 0
+  for st in plan['steps']:
+    for op in st['ops']:
+      for p in op.get('pipeline', ()):
+        for i, s in enumerate(p.get('sources', ())):
+          if arity[s['rel']] == 3:
+            bound.add(len(s['prefix']))
+            orders.add(tuple(s['index']))
+            if p['op'] == 'cartesian_join' and len(p['var_from_source'][i]) == 2:
+              two_var += 1
+        if p['op'] == 'scan' and arity[p['rel']] == 3:
+          bound.add('scan')
+  assert bound == {0, 1, 2, 'scan'}
+  assert orders == {(0, 1, 2), (1, 0, 2), (2, 1, 0)}
+  assert two_var >= 2
