@@ -249,3 +249,23 @@ def galen_inputs(n_vals: int, m: int, seed: int) -> dict:
 
   return {'PInput': _pairs(rng, n_vals, q), 'SInput': _pairs(rng, n_vals, q),
           'QInput': triples(), 'RInput': triples(), 'CInput': triples(), 'UInput': triples()}
+
+
+def plan_inputs(plan: dict, n_vals: int, m: int, seed: int) -> dict:
+  '''Uniform facts for every input relation of a plan (those with an input
+  file): about m distinct rows each over values [0, n_vals), drawn in the
+  plan's relation order from one seeded generator.'''
+  rng = _rng(seed)
+  out = {}
+  for r in plan['relations']:
+    if not r['input_file']:
+      continue
+    k = r['arity']
+    t = rng.integers(0, n_vals, (m, k), dtype=np.uint32)
+    key = np.zeros(m, np.uint64)
+    for j in range(k):
+      key = key * np.uint64(n_vals) + t[:, j].astype(np.uint64)
+    _, first = np.unique(key, return_index=True)
+    first.sort()
+    out[r['name']] = np.ascontiguousarray(t[first])
+  return out

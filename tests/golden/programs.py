@@ -420,6 +420,24 @@ def galen_program() -> Program:
   ])
 
 
+def polonius_program() -> Program:
+  '''examples/polonius_test.py (Polonius borrow checking: 38 relations,
+  five of them ternary, binary negations, two-column filters).  The program
+  is the reference's own DSL module, loaded from the checkout that provides
+  the srdatalog front end (its examples/ directory); its MIR is pinned by
+  tests/fixtures/integration/polonius_test.mir.sexpr.'''
+  import importlib.util
+  import os
+
+  import srdatalog
+  root = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(srdatalog.__file__))))
+  spec = importlib.util.spec_from_file_location(
+    'polonius_test', os.path.join(root, 'examples', 'polonius_test.py'))
+  mod = importlib.util.module_from_spec(spec)
+  spec.loader.exec_module(mod)
+  return mod.build_poloniusdb_program()
+
+
 # name -> (builder, project name, reference MIR fixture or None)
 PROGRAMS = {
   'tc': (tc_program, 'TcPlan', 'tc.mir.sexpr'),
@@ -445,4 +463,5 @@ PROGRAMS = {
   'rewrite_consts': (rewrite_consts_program, 'RewriteConstsPlan', 'rewrite_consts.mir.sexpr'),
   'head_const': (head_const_program, 'HeadConstPlan', None),
   'galen': (galen_program, 'GalenPlan', 'integration/galen.mir.sexpr'),
+  'polonius': (polonius_program, 'PoloniusPlan', 'integration/polonius_test.mir.sexpr'),
 }

@@ -31,7 +31,7 @@ def test_library_exports_every_header_symbol():
 
 
 @pytest.mark.parametrize('name', ['tc', 'sg', 'triangle', 'tc_left', 'tc_lsm', 'head_const',
-                                  'rewrite_consts', 'galen'])
+                                  'rewrite_consts', 'galen', 'polonius'])
 def test_open_committed_plans(name):
   db = native.Database(load_plan(name))
   db.close()

@@ -40,3 +40,13 @@ def test_galen_access_patterns():
   assert bound == {0, 1, 2, 'scan'}
   assert orders == {(0, 1, 2), (1, 0, 2), (2, 1, 0)}
   assert two_var >= 2
+
+
+def test_polonius_interpreter_derives():
+  '''The Polonius plan (MIR pinned to the reference fixture) derives the
+  relations its rules define from uniform facts; the GPU parity test checks
+  the engine against these interpreter results.'''
+  plan = load_plan('polonius')
+  got, _ = oracle.run_plan(plan, W.plan_inputs(plan, 24, 20, 2))
+  for rel in ('subset', 'origin_live_on_entry', 'loan_live_at', 'errors', 'move_error'):
+    assert got[rel], rel
