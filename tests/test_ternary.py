@@ -50,3 +50,12 @@ def test_polonius_interpreter_derives():
   got, _ = oracle.run_plan(plan, W.plan_inputs(plan, 24, 20, 2))
   for rel in ('subset', 'origin_live_on_entry', 'loan_live_at', 'errors', 'move_error'):
     assert got[rel], rel
+
+
+def test_ternary_programs_shard_as_replicas():
+  '''Exchanges move binary tuples only: programs whose joins need other
+  shards' ternary tuples fall back to replicas, with the reason.'''
+  from srdatalog_b200.shard import shard_plan
+  for name in ('galen', 'polonius'):
+    spec = shard_plan(load_plan(name))
+    assert spec.fallback and not spec.partitioned and not spec.exchanged
