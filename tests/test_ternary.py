@@ -59,3 +59,28 @@ def test_ternary_programs_shard_as_replicas():
   for name in ('galen', 'polonius'):
     spec = shard_plan(load_plan(name))
     assert spec.fallback and not spec.partitioned and not spec.exchanged
+
+
+@pytest.mark.parametrize('n,m,seed', [(10, 8, 0), (24, 20, 2)])
+def test_polonius_liveness_rules_restated(n, m, seed):
+
+  '''Two Polonius relations of the interpreter against the rules restated on
+  sets: var_live_on_entry (vle_used, vle_cfg with its negation) and
+  origin_live_on_entry (ole_universal, ole_drop, ole_use).'''
+  plan = load_plan('polonius')
+  inp = W.plan_inputs(plan, n, m, seed)
+  got, _ = oracle.run_plan(plan, inp)
+  facts = {k: set(map(tuple, v.tolist())) for k, v in inp.items()}
+  vle = set(facts['var_used_at'])
+  while True:
+    new = {(v, p1) for (v, p2) in vle for (p1, q) in facts['cfg_edge']
+           if q == p2 and (v, p1) not in facts['var_defined_at']} - vle
+    if not new:
+      break
+    vle |= new
+  assert vle == set(got['var_live_on_entry'])
+  live = {(o, p) for (p,) in got['cfg_node'] for (o,) in facts['universal_region']}
+  live |= {(o, p) for (v, p) in got['var_drop_live_on_entry']
+           for (w, o) in facts['drop_of_var_derefs_origin'] if v == w}
+  live |= {(o, p) for (v, p) in vle for (w, o) in facts['use_of_var_derefs_origin'] if v == w}
+  assert live == set(got['origin_live_on_entry'])
