@@ -63,7 +63,6 @@ def test_ternary_programs_shard_as_replicas():
 
 @pytest.mark.parametrize('n,m,seed', [(10, 8, 0), (24, 20, 2)])
 def test_polonius_liveness_rules_restated(n, m, seed):
-
   '''Two Polonius relations of the interpreter against the rules restated on
   sets: var_live_on_entry (vle_used, vle_cfg with its negation) and
   origin_live_on_entry (ole_universal, ole_drop, ole_use).'''
