@@ -24,7 +24,8 @@ share a GPU, which exercises the N>1 path but times nothing meaningful).
 requests: --serve-workers, --serve-max-batch) against the plain loop at
 --rate offered requests/s.
 --impl reference: the CPU restatement of the reference's evaluation on
-the host cores, on a bounded sample of the same workload.
+the host cores, one full run of the same workload per step (the batched
+and served workloads: a seeded sample of their queries).
 '''
 
 from __future__ import annotations
@@ -247,13 +248,12 @@ def cpu_baseline(wl_name: str, edges: np.ndarray) -> dict:
     return {'value': len(sample) / dt, 'unit': 'queries/s', 'cores': cores, 'kind': 'port',
             'sample': f'TC of every {PLAIN_SAMPLE_STRIDE}th instance ({len(sample)}), {dt:.2f} s'}
   if wl_name == 'triangle':
-    stride = 4
-    c, t_sort, t_join = oracle.triangle_count_sample(edges, stride)
-    # full-workload estimate: one index build + stride x the sampled join
-    t_est = t_sort + stride * t_join
-    value = (c * stride) / t_est
-    sample = (f'index build over all {edges.shape[0]} edges ({t_sort:.2f} s) + join over every '
-              f'{stride}th edge ({t_join:.2f} s, {c} triangles); extrapolated x{stride}')
+    t0 = time.perf_counter()
+    c = oracle.triangle_count(edges)
+    dt = time.perf_counter() - t0
+    value = c / dt
+    sample = (f'full workload: index build + join over all {edges.shape[0]} edges '
+              f'({dt:.2f} s, {c} triangles)')
   else:
     t0 = time.perf_counter()
     if wl_name == 'tc':
@@ -572,15 +572,21 @@ def main():
   name, k = top
   peak, peak_kind = hbm_peak()
   achieved = (k['bytes'] / (k['ms'] / 1e3)) / 1e9 if k['ms'] else 0.0
-  traffic = None
+  # DRAM bytes per launch from an ncu capture of this workload's dominant
+  # kernel (profiles/traffic.json: read + write bytes and the units that
+  # capture processed, scaled to this run's units per launch)
+  traffic, traffic_src = None, None
   prof = os.path.join(REPO, 'profiles', 'traffic.json')
   if os.path.exists(prof):
-    tr = json.load(open(prof)).get(args.workload, {}).get(name)
+    with open(prof) as f:
+      tr = json.load(f).get(args.workload, {}).get(name)
     if tr:
-      traffic = tr['dram_bytes_per_unit'] * k['units'] / max(1, k['scopes'])
+      traffic = tr['dram_bytes'] / tr['units'] * k['units'] / max(1, k['scopes'])
+      traffic_src = tr['source']
   roof = {'bound': 'hbm', 'kernel': name, 'achieved': achieved, 'peak': peak,
           'peak_source': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
-          'traffic': traffic, 'bytes_per_launch': k['bytes'] / max(1, k['scopes']),
+          'traffic': traffic, 'traffic_source': traffic_src,
+          'bytes_per_launch': k['bytes'] / max(1, k['scopes']),
           'ms_per_launch': k['ms'] / max(1, k['scopes']),
           'share_of_step': k['ms'] / total_ms if world == 1 else None}
   line = {

@@ -592,3 +592,26 @@ def galen(inputs: dict) -> dict:
       return {'OutP': sorted(out_p), 'OutQ': sorted(out_q)}
     out_p |= new_p
     out_q |= new_q
+
+
+def live(inputs: dict) -> dict:
+  '''Live and Out of the live test program, by Python sets: Live(v, p) for
+  every (v, q) in Used with p reaching q over Cfg edges (p -> q), zero or
+  more steps; Out(o, p) for Live(v, p) and Derefs(v, o).'''
+  def rows(name):
+    return {tuple(int(x) for x in r) for r in np.asarray(inputs[name]).reshape(-1, 2).tolist()}
+  used, cfg, derefs = rows('Used'), rows('Cfg'), rows('Derefs')
+  pred: dict = {}
+  for p, q in cfg:
+    pred.setdefault(q, set()).add(p)
+  lv = set(used)
+  frontier = set(used)
+  while frontier:
+    new = {(v, p) for v, q in frontier for p in pred.get(q, ())} - lv
+    lv |= new
+    frontier = new
+  by_v: dict = {}
+  for v, o in derefs:
+    by_v.setdefault(v, set()).add(o)
+  out = {(o, p) for v, p in lv for o in by_v.get(v, ())}
+  return {'Live': sorted(lv), 'Out': sorted(out)}

@@ -392,7 +392,10 @@ uint64_t srdl_sort_unique_scratch_bytes(uint64_t n, int value_bits) {
 int srdl_sort_unique_u64(const uint64_t* d_in, uint64_t n, int value_bits, uint64_t* d_out,
                          uint64_t* d_n_out, void* d_scratch, uint64_t scratch_bytes,
                          void* stream) {
-  if ((!d_in && n) || !d_out || !d_n_out || value_bits < 1 || value_bits > 32) return kErrArg;
+  if ((!d_in && n) || !d_out || !d_n_out || value_bits < 1 || value_bits > 32) {
+    srdl::set_error("srdl_sort_unique_u64: bad argument");
+    return kErrArg;
+  }
   SRDL_GUARD(0, {
     Launch L = launch_for(stream);
     Scratch s{(char*)d_scratch, (size_t)scratch_bytes, 0};
@@ -406,7 +409,10 @@ uint64_t srdl_set_difference_scratch_bytes(uint64_t na) { return diff_scratch_by
 int srdl_set_difference_u64(const uint64_t* d_a, uint64_t na, const uint64_t* d_b, uint64_t nb,
                             uint64_t* d_out, uint64_t* d_n_out, void* d_scratch,
                             uint64_t scratch_bytes, void* stream) {
-  if ((!d_a && na) || (!d_b && nb) || !d_out || !d_n_out) return kErrArg;
+  if ((!d_a && na) || (!d_b && nb) || !d_out || !d_n_out) {
+    srdl::set_error("srdl_set_difference_u64: bad argument");
+    return kErrArg;
+  }
   SRDL_GUARD(0, {
     Launch L = launch_for(stream);
     Scratch s{(char*)d_scratch, (size_t)scratch_bytes, 0};
@@ -417,7 +423,10 @@ int srdl_set_difference_u64(const uint64_t* d_a, uint64_t na, const uint64_t* d_
 
 int srdl_merge_u64(const uint64_t* d_a, uint64_t na, const uint64_t* d_b, uint64_t nb,
                    uint64_t* d_out, void* stream) {
-  if ((!d_a && na) || (!d_b && nb) || !d_out) return kErrArg;
+  if ((!d_a && na) || (!d_b && nb) || !d_out) {
+    srdl::set_error("srdl_merge_u64: bad argument");
+    return kErrArg;
+  }
   SRDL_GUARD(0, {
     Launch L = launch_for(stream);
     merge_disjoint(L, d_a, na, d_b, nb, d_out);

@@ -680,7 +680,19 @@ void Database::exec_ops(const Step& st, uint64_t it) {
     } timer{opstats_[op_kind_name(op.kind)], h0};
     switch (op.kind) {
       case Op::Execute: exec_pipeline(op, st.recursive, it); break;
-      case Op::Rebuild: op_rebuild(st, i, op); break;
+      case Op::Rebuild: {
+        // NEW: sort + dedup the join output.  FULL / DELTA: make the
+        // permutation current.  The planner places RebuildIndex(FULL) after
+        // a stratum for the permutations later strata read but the stratum
+        // did not merge into (src/srdatalog/mir/passes.py:104-145), so it is
+        // rebuilt from a permutation holding every merged delta; relations
+        // of arity > 2 keep their canonical order only (other orders are
+        // derived views, built when a join reads them).
+        Relation& r = rel(op.rel);
+        if (op.ver == kNew) op_rebuild(st, i, op);
+        else if (r.arity <= 2 && r.v[op.ver].has_index()) ensure_index(r, op.ver, op.index);
+        break;
+      }
       case Op::Clear:
         // A pending fused delta survives the clear of the old DELTA.
         rel(op.rel).v[op.ver].clear();

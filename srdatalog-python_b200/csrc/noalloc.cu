@@ -11,10 +11,13 @@
 // Host code cannot use the array's name as a device address (on the host it
 // names a stand-in), so the first call on each device, with that device
 // current, resolves the address with cudaGetSymbolAddress and caches it.
-// That first call should therefore come before any stream capture.  Calls
-// that overlap on the GPU share the array and race; serialise them (one
-// stream, or events).  Every scratch word is written before it is read, so
-// nothing needs clearing between calls.
+// That first call should therefore come before any stream capture.  The
+// cached address belongs to the device's current context: it does not
+// survive cudaDeviceReset (or any other teardown of the primary context), so
+// a process that resets a device must not call this entry point on that
+// device afterwards.  Calls that overlap on the GPU share the array and
+// race; serialise them (one stream, or events).  Every scratch word is
+// written before it is read, so nothing needs clearing between calls.
 #include <mutex>
 
 #include "../../include/srdl.h"
@@ -86,6 +89,9 @@ int srdl_sort_unique_u64_noalloc(const uint64_t* d_in, uint64_t n, int value_bit
   } catch (const Error& err) {
     set_error(err.msg);
     return err.code;
+  } catch (const std::exception& err) {
+    set_error(std::string("srdl_sort_unique_u64_noalloc: ") + err.what());
+    return kErrState;
   }
 }
 

@@ -300,8 +300,11 @@ class LocalExchange:
   (ShardedDatabase(..., exchange=ex) per thread).  Shards meet at a barrier
   in every phase; a receiver copies its slices straight out of the senders'
   buffers (peer copies when the shards sit on different GPUs of the
-  process).  `copy(dst, src, nbytes, stream)` may replace the device copy.
-  A shard whose run fails should call abort(), so the others stop waiting.'''
+  process).  `copy(dst, src, nbytes, stream)` may replace the device copy;
+  it must have finished the copy when it returns (the default one
+  synchronises), because a sender's buffer goes back to its stream's arena
+  as soon as the exchange's last barrier is passed.  A shard whose run fails
+  should call abort(), so the others stop waiting.'''
 
   def __init__(self, world: int, timeout: float = 600.0, copy=None):
     self.world = world

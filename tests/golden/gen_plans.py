@@ -1,12 +1,13 @@
 '''Regenerate tests/golden/plans/*.json from the DSL programs.
 
-Needs the srdatalog front end on sys.path (pass --ref-src, default: the
-reference checkout's src/ directory).  For every program that has a
+Needs the srdatalog front end: --ref names a checkout of the reference
+(default: the SRDATALOG_REF environment variable); its src/ directory goes
+on sys.path.  For every program that has a
 reference MIR fixture, the MIR printed by the front end is first compared
 byte-for-byte with that fixture, so the committed plans are the plans the
 reference itself would execute.
 
-  python tests/golden/gen_plans.py --ref /root/reference
+  SRDATALOG_REF=/root/reference python tests/golden/gen_plans.py
 '''
 
 from __future__ import annotations
@@ -22,9 +23,11 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 
 def main() -> int:
   ap = argparse.ArgumentParser()
-  ap.add_argument('--ref', default='/root/reference')
+  ap.add_argument('--ref', default=os.environ.get('SRDATALOG_REF', ''))
   ap.add_argument('--check', action='store_true', help='compare instead of writing')
   args = ap.parse_args()
+  if not args.ref:
+    ap.error('name the reference checkout with --ref or SRDATALOG_REF')
   sys.path.insert(0, os.path.join(args.ref, 'src'))
   sys.path.insert(0, os.path.join(REPO, 'srdatalog-python_b200'))
   sys.path.insert(0, HERE)

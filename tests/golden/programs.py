@@ -420,6 +420,37 @@ def galen_program() -> Program:
   ])
 
 
+def _live(index_type: str | None) -> Program:
+  '''Backward liveness and a later read of it in the other column order:
+  Live is stored in order (1, 0) (its recursive rule joins on column 1), so
+  the later stratum's read Live(v, p) & Derefs(v, o) needs FULL (0, 1),
+  which the recursive stratum never merges into: the planner inserts a
+  RebuildIndex(FULL) for it after the stratum (src/srdatalog/mir/passes.py:
+  104-145).  The shape of Polonius' var_live_on_entry and its ole_use read.'''
+  used = _bin('Used', 'Used.csv')
+  cfg = _bin('Cfg', 'Cfg.csv')
+  derefs = _bin('Derefs', 'Derefs.csv')
+  kw = {'column_types': (int, int), 'print_size': True}
+  if index_type:
+    kw['index_type'] = index_type
+  live = Relation('Live', 2, **kw)
+  out = Relation('Out', 2, column_types=(int, int), print_size=True)
+  v, p, q, o = Var('v'), Var('p'), Var('q'), Var('o')
+  return Program(rules=[
+    (live(v, p) <= used(v, p)).named('LiveUsed'),
+    (live(v, p) <= live(v, q) & cfg(p, q)).named('LiveStep'),
+    (out(o, p) <= live(v, p) & derefs(v, o)).named('OutUse'),
+  ])
+
+
+def live_program() -> Program:
+  return _live(None)
+
+
+def live_lsm_program() -> Program:
+  return _live('SRDatalog::GPU::Device2LevelIndex')
+
+
 def polonius_program() -> Program:
   '''examples/polonius_test.py (Polonius borrow checking: 38 relations,
   five of them ternary, binary negations, two-column filters).  The program
@@ -464,4 +495,6 @@ PROGRAMS = {
   'head_const': (head_const_program, 'HeadConstPlan', None),
   'galen': (galen_program, 'GalenPlan', 'integration/galen.mir.sexpr'),
   'polonius': (polonius_program, 'PoloniusPlan', 'integration/polonius_test.mir.sexpr'),
+  'live': (live_program, 'LivePlan', None),
+  'live_lsm': (live_lsm_program, 'LivePlan', None),
 }

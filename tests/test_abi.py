@@ -125,7 +125,10 @@ def test_generated_shim_abi(tmp_path):
   lib.srdatalog_size.restype = ctypes.c_ulonglong
   # reference status codes (main_file.py:690-753)
   assert lib.srdatalog_run(0) == 1              # nothing loaded yet
+  lib.srdatalog_init()                           # 0 on a GPU box, 1 without a device
+  assert lib.srdatalog_run(0) == 1              # init alone loads nothing
   assert lib.srdatalog_load_csv(None, b'x') == 1
+  assert lib.srdatalog_run(0) == 1              # a rejected (null) load loads nothing
   csv = write(tmp_path, 'Arc.csv', '0\t1\n1\t2\n')
   assert lib.srdatalog_load_csv(b'Nope', csv.encode()) == 2
   assert lib.srdatalog_load_csv(b'ArcInput', b'/nonexistent.csv') == 3
@@ -135,6 +138,7 @@ def test_generated_shim_abi(tmp_path):
   assert lib.srdatalog_size(b'Unknown') == 0
   assert rt.srdatalog_shutdown() == 0
   assert lib.srdatalog_size(b'Path') == 0
+  assert lib.srdatalog_run(0) == 1              # shutdown drops the loaded state
 
 
 @pytest.mark.parametrize('n', [0, 1, 3, 55, 56, 63, 64, 65, 119, 120, 1000, 1 << 20])

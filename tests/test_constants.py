@@ -98,3 +98,20 @@ def test_batch_refuses_constants():
 def test_shard_plan_accepts_constants():
   spec = shard_plan(load_plan('head_const'))
   assert '__const_7' in spec.replicated
+
+
+@pytest.mark.parametrize('name', ['live', 'live_lsm'])
+@pytest.mark.parametrize('seed', range(3))
+def test_live_interpreter_vs_sets(name, seed):
+  '''The live program (a relation stored in order (1, 0) by its recursive
+  stratum, read in order (0, 1) by a later one after a RebuildIndex(FULL)):
+  the plan interpreter agrees with the rules restated on sets.'''
+  plan = load_plan(name)
+  steps = [o for s in plan['steps'] for o in s['ops']]
+  assert {'op': 'rebuild_index', 'rel': 'Live', 'ver': 'FULL', 'index': [0, 1]}.items() <= \
+      next(o for o in steps if o['op'] == 'rebuild_index' and o['ver'] == 'FULL').items()
+  inp = W.plan_inputs(plan, 30, 60, seed)
+  got, _ = oracle.run_plan(plan, inp)
+  want = oracle.live(inp)
+  assert got['Live'] == want['Live'] and got['Out'] == want['Out']
+  assert len(want['Out']) > 0

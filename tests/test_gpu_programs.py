@@ -366,10 +366,24 @@ def test_galen_ternary_joins(n, m, seed):
     assert oracle.dump_hash(db.dump(rel)) == oracle.dump_hash(w), rel
 
 
-@pytest.mark.xfail(reason='known mismatch: on facts (10, 8, 0) the engine derives 63 '
-                   'origin_live_on_entry tuples, the interpreter (checked against the '
-                   'rules restated on sets) 67; the 4 missing ones come from the ole_drop '
-                   'and ole_use rules', strict=False)
+@pytest.mark.parametrize('name', ['live', 'live_lsm'])
+@pytest.mark.parametrize('n,m,seed', [(30, 60, 0), (30, 60, 1), (400, 1500, 2), (3000, 9000, 3)])
+def test_live_rebuilt_full_permutation(name, n, m, seed):
+  '''A relation stored in order (1, 0), merged only in that order by its
+  recursive stratum, then read in order (0, 1) by a later stratum after the
+  plan's RebuildIndex(FULL, (0, 1)): that permutation is rebuilt from the
+  up-to-date one (single array and Device2LevelIndex), bit-exact against the
+  rules restated on sets.'''
+  plan = load_plan(name)
+  inp = W.plan_inputs(plan, n, m, seed)
+  want = oracle.live(inp)
+  db = run(name, inp)
+  for rel in ('Live', 'Out'):
+    w = np.array(want[rel], np.uint32).reshape(-1, 2)
+    assert db.size(rel) == w.shape[0], rel
+    assert oracle.dump_hash(db.dump(rel)) == oracle.dump_hash(w), rel
+
+
 @pytest.mark.parametrize('n,m,seed', [(10, 8, 0), (24, 20, 2), (32, 30, 3)])
 def test_polonius_vs_interpreter(n, m, seed):
   '''Polonius (the reference's examples/polonius_test.py): every relation
