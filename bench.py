@@ -23,6 +23,8 @@ share a GPU, which exercises the N>1 path but times nothing meaningful).
 --workload served: the request server (8 workers, unions of at most 16
 requests: --serve-workers, --serve-max-batch) against the plain loop at
 --rate offered requests/s.
+--workload primitives: the sort / merge / set-difference primitives alone
+(--keys, --bits), one JSON line each.
 --impl reference: the CPU restatement of the reference's evaluation on
 the host cores, one full run of the same workload per step (the batched
 and served workloads: a seeded sample of their queries).
@@ -379,13 +381,115 @@ def run_served(args, rank, world):
   print(json.dumps(line), flush=True)
 
 
+def run_primitives(args, rank, world):
+  '''The sort + unique, merge and set-difference primitives of libsrdl on
+  --keys random (hi, lo) pairs with --bits-bit halves, built on the device.
+  Each primitive runs --warmup times untimed, then --steps times between
+  CUDA events on the current stream (median reported); one JSON line per
+  primitive gives its time and algorithmic bandwidth (the bytes the
+  operation must move at least) against the measured HBM peak:
+    sort + unique of n keys: read the input, write the packed keys, read and
+      write them once per counting pass, read them for the dedup and write
+      the distinct keys;
+    merge of two disjoint sorted arrays: 16 B per output key;
+    set difference a - b: 8 B per key of a, b and the result.
+  torch provides device buffers and the stream only.'''
+  import ctypes
+
+  import torch
+  from srdatalog_b200 import native
+  if rank != 0:
+    return
+  lib = native.lib()
+  n, bits = args.keys, args.bits
+  peak, peak_kind = hbm_peak()
+  st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+  g = torch.Generator(device='cuda').manual_seed(1)
+  hi = torch.randint(0, 1 << bits, (n,), device='cuda', dtype=torch.int64, generator=g)
+  lo = torch.randint(0, 1 << bits, (n,), device='cuda', dtype=torch.int64, generator=g)
+  keys = (hi << 32) | lo
+  del hi, lo
+  flush = torch.empty(64 << 20, dtype=torch.int32, device='cuda')  # 256 MB > 126 MB L2
+
+  def timed(fn):
+    for _ in range(args.warmup):
+      fn()
+    ms = []
+    for i in range(args.steps):
+      flush.fill_(i)
+      e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+      e0.record()
+      fn()
+      e1.record()
+      e1.synchronize()
+      ms.append(e0.elapsed_time(e1))
+    return statistics.median(ms)
+
+  def report(name, ms, alg_bytes, **extra):
+    gbs = alg_bytes / ms / 1e6
+    print(json.dumps({'primitive': name, 'ms': round(ms, 4), 'alg_gbs': round(gbs, 1),
+                      'frac_of_peak': round(gbs / peak, 3), 'peak_gbs': peak,
+                      'peak_source': peak_kind, 'steps': args.steps, **extra}), flush=True)
+
+  out = torch.empty_like(keys)
+  dn = torch.zeros(1, dtype=torch.int64, device='cuda')
+  sb = lib.srdl_sort_unique_scratch_bytes(n, bits)
+  scratch = torch.empty(sb, dtype=torch.uint8, device='cuda')
+
+  def sort():
+    rc = lib.srdl_sort_unique_u64(keys.data_ptr(), n, bits, out.data_ptr(), dn.data_ptr(),
+                                  scratch.data_ptr(), sb, st)
+    assert rc == 0, native.last_error()
+
+  ms = timed(sort)
+  u = int(dn.item())
+  # packed key width k and the passes the library runs: read the input
+  # (8 B), write packed keys (k), P passes reading and writing k each, read
+  # the sorted keys once more (k) and write the distinct ones (8 B)
+  k = 4 if 2 * bits <= 32 else 8
+  passes = (2 * bits + 7) // 8  # the library's default widest digit is 8 bits
+  alg = n * (8 + k + passes * 2 * k + k) + 8 * u
+  report('sort_unique', ms, alg, keys=n, unique=u, value_bits=bits, passes=passes,
+         io_gbs=round(16 * n / ms / 1e6, 1))
+  del scratch
+
+  a = out[0:u:2].contiguous()
+  b = out[1:u:2].contiguous()
+  m = torch.empty(a.numel() + b.numel(), dtype=torch.int64, device='cuda')
+
+  def merge():
+    rc = lib.srdl_merge_u64(a.data_ptr(), a.numel(), b.data_ptr(), b.numel(), m.data_ptr(), st)
+    assert rc == 0, native.last_error()
+
+  report('merge', timed(merge), 16 * m.numel(), keys=m.numel())
+  del a, b, m
+
+  sub = out[0:u:3].contiguous()
+  d = torch.empty(u, dtype=torch.int64, device='cuda')
+  dn2 = torch.zeros(1, dtype=torch.int64, device='cuda')
+  sb2 = lib.srdl_set_difference_scratch_bytes(u)
+  scratch2 = torch.empty(sb2, dtype=torch.uint8, device='cuda')
+
+  def diff():
+    rc = lib.srdl_set_difference_u64(out.data_ptr(), u, sub.data_ptr(), sub.numel(), d.data_ptr(),
+                                     dn2.data_ptr(), scratch2.data_ptr(), sb2, st)
+    assert rc == 0, native.last_error()
+
+  ms = timed(diff)
+  nd = int(dn2.item())
+  report('set_difference', ms, 8 * (u + sub.numel() + nd), a=u, b=sub.numel(), result=nd)
+
+
 def main():
   ap = argparse.ArgumentParser()
   ap.add_argument('--gpus', type=int, default=1)
   ap.add_argument('--steps', type=int, default=10)
   ap.add_argument('--warmup', type=int, default=3)
   ap.add_argument('--impl', default='srdl', choices=['srdl', 'reference'])
-  ap.add_argument('--workload', default='triangle', choices=sorted(WORKLOADS) + ['served'])
+  ap.add_argument('--workload', default='triangle',
+                  choices=sorted(WORKLOADS) + ['served', 'primitives'])
+  ap.add_argument('--keys', type=int, default=200_000_000, help='primitives: keys')
+  ap.add_argument('--bits', type=int, default=21, help='primitives: bits per key half')
   ap.add_argument('--rate', type=float, default=2000.0, help='served: offered load (req/s)')
   ap.add_argument('--serve-workers', type=int, default=8, help='served: concurrent workers')
   ap.add_argument('--batch-max-edges', type=int, default=1 << 20,
@@ -405,6 +509,8 @@ def main():
     return run_reference(args, rank, world)
   if args.workload == 'served':
     return run_served(args, rank, world)
+  if args.workload == 'primitives':
+    return run_primitives(args, rank, world)
 
   import torch
   dist = None
