@@ -26,6 +26,8 @@
 //            tables are written in input order (count pass + scan + write
 //            pass), so every binding table stays lexicographically sorted.
 
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace srdl {
@@ -335,19 +337,28 @@ __device__ __forceinline__ uint32_t lower_bound_bf(const uint32_t* __restrict__ 
 // Two-source column join without filters (the common leapfrog step): the
 // count pass stored, per row, the driver list begin and the other list's
 // range, so a candidate costs one coalesced load of its value plus a
-// branch-free binary search in the other list (or a directory check when
-// the other list is all roots of a dense index).
+// branch-free binary search in the other list (or one bitmap word, or a
+// directory check when the other list is all roots of a dense index).
+//
+// Work distribution: the candidates are cut into chunks of `chunk` (a
+// multiple of 32) and resident warps take chunks in increasing order from a
+// device-wide counter (block-level work stealing).  Rows are sorted by their
+// first column, so the warps in flight at any moment all work inside a
+// window of about (resident warps x chunk) candidates: the few first-column
+// values there, whose child lists and bitmaps the probes of the window reuse,
+// stay in L2 instead of every warp's slice touching a different part of the
+// index.  A skewed row spans as many chunks as its candidates fill.  The
+// table modes record each chunk's surviving count (count pass) and write the
+// chunk's survivors at the scanned offset (write pass), so the table stays
+// in input order.
 template <int MODE, bool SEG>
 __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
     LevelSpec lv, Table in, const uint64_t* __restrict__ offs, const uint8_t* __restrict__ drv,
     const uint32_t* __restrict__ beg, const uint2* __restrict__ orange,
-    const uint32_t* __restrict__ obm, uint64_t total, uint64_t chunk, Table out,
-    uint64_t* __restrict__ out_keys, unsigned long long* __restrict__ d_out_n,
-    uint64_t* __restrict__ warp_counts) {
+    const uint32_t* __restrict__ obm, uint64_t total, uint64_t chunk,
+    unsigned long long* __restrict__ queue, Table out, uint64_t* __restrict__ out_keys,
+    unsigned long long* __restrict__ d_out_n, uint64_t* __restrict__ chunk_counts) {
   const int lane = threadIdx.x & 31;
-  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t c0 = gw * chunk;
-  const uint64_t c1 = c0 + chunk < total ? c0 + chunk : total;
   const uint32_t* vals0 = lv.src[0].prefix_slot < 0 ? lv.src[0].t.roots : lv.src[0].t.lo;
   const uint32_t* vals1 = lv.src[1].prefix_slot < 0 ? lv.src[1].t.roots : lv.src[1].t.lo;
   // a roots-list side with a dense directory answers membership in O(1)
@@ -357,12 +368,22 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
   const uint32_t* bp0 = lv.src[0].t.bpool;
   const uint32_t* bp1 = lv.src[1].t.bpool;
   const uint32_t bw0 = lv.src[0].t.bwords, bw1 = lv.src[1].t.bwords;
-  unsigned long long running = 0;
-  if (MODE == kModeTableWrite) running = warp_counts[gw];
-  if (c0 < c1) {
+  const uint64_t nchunks = (total + chunk - 1) / chunk;
+  unsigned long long counted = 0;  // count mode: this warp's survivors over all its chunks
+  while (true) {
+    unsigned long long k = 0;
+    if (lane == 0) k = atomicAdd(queue, 1ull);
+    k = __shfl_sync(kAllLanes, k, 0);
+    if (k >= nchunks) break;
+    const uint64_t c0 = k * chunk;
+    const uint64_t c1 = c0 + chunk < total ? c0 + chunk : total;
+    unsigned long long running = MODE == kModeTableWrite ? chunk_counts[k] : 0ull;
     SegWalk<SEG> sw(lv, c0);
-    uint64_t r0 = gallop_row(offs, 0, in.n, sw.at());
-    // The row of the warp's first candidate and its metadata, kept while the
+    // the row holding the chunk's first candidate: the last row whose offset
+    // is <= it (a warp-wide search, log32 of the rows in load rounds)
+    const uint64_t first = sw.at();
+    uint64_t r0 = warp_partition_point(0, in.n, [&](uint64_t i) { return offs[i] <= first; }) - 1;
+    // The row of the round's first candidate and its metadata, kept while the
     // warp stays in it (r0 is warp-uniform): most candidates lie in rows
     // longer than a warp round, whose lanes then need no row search and no
     // per-lane metadata loads.
@@ -471,12 +492,10 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
       }
       r0 = __shfl_sync(kAllLanes, r, 31);
     }
+    if (MODE == kModeCount) counted += running;
+    else if (MODE == kModeTableCount && lane == 0) chunk_counts[k] = running;
   }
-  if (MODE == kModeCount) {
-    if (lane == 0 && running) atomicAdd(d_out_n, running);
-  } else if (MODE == kModeTableCount) {
-    if (lane == 0) warp_counts[gw] = running;
-  }
+  if (MODE == kModeCount && lane == 0 && counted) atomicAdd(d_out_n, counted);
 }
 
 template <int MODE, bool SEG>
@@ -705,9 +724,37 @@ static int jgrid(uint64_t n, const Launch& L) {
   return g ? (int)g : 1;
 }
 
+// Most per-chunk counts the two-source column join keeps in its table modes.
+constexpr uint64_t kCj2MaxTableChunks = 1ull << 18;
+
 size_t join_expand_scratch_bytes(const Launch& L) {
   const uint64_t warps = (uint64_t)L.num_sms * (L.join_bpsm > 0 ? L.join_bpsm : 16) * (kJThreads / 32);
-  return 2 * ((warps + 1) * 8 + 255) + scan_scratch_bytes(warps) + 1024;
+  const uint64_t n = std::max<uint64_t>(warps, kCj2MaxTableChunks);
+  return 2 * ((n + 1) * 8 + 255) + scan_scratch_bytes(n) + 4096;
+}
+
+// Resident blocks per SM of the two-source column-join kernel for a level
+// (its register count differs per mode), asked of the runtime once each.
+template <int MODE, bool SEG>
+static int cj2_occ() {
+  static int occ = [] {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, join_cj2_kernel<MODE, SEG>, kJThreads, 0) !=
+            cudaSuccess ||
+        b < 1) {
+      (void)cudaGetLastError();
+      b = 4;
+    }
+    return b;
+  }();
+  return occ;
+}
+
+static int cj2_blocks_per_sm(bool seg, int emit) {
+  if (emit == kEmitCount) return seg ? cj2_occ<kModeCount, true>() : cj2_occ<kModeCount, false>();
+  if (emit == kEmitKeys) return seg ? cj2_occ<kModeKeys, true>() : cj2_occ<kModeKeys, false>();
+  return std::min(seg ? cj2_occ<kModeTableCount, true>() : cj2_occ<kModeTableCount, false>(),
+                  seg ? cj2_occ<kModeTableWrite, true>() : cj2_occ<kModeTableWrite, false>());
 }
 
 JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scratch& s) {
@@ -739,25 +786,45 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
   const uint64_t chunk = ((total + warps - 1) / warps + 31) & ~uint64_t(31);
   Table out = out_table ? *out_table : Table{};
   if (lv.kind == kColumnJoin && lv.nsrc == 2 && lv.nfilt == 0 && !lv.wide) {
-#define SRDL_CJ2(MODE, WC)                                                                   \
-  (lv.seg ? join_cj2_kernel<MODE, true><<<g, kJThreads, 0, L.stream>>>(                       \
-                lv, in, w.offs, w.drv, w.beg, w.orange, w.obm, total, chunk, out, out_keys, cnt, WC) \
-          : join_cj2_kernel<MODE, false><<<g, kJThreads, 0, L.stream>>>(                      \
-                lv, in, w.offs, w.drv, w.beg, w.orange, w.obm, total, chunk, out, out_keys, cnt, WC))
+    // Persistent warps over a chunk queue: as many blocks as stay resident
+    // (at most join_bpsm per SM), about eight chunks per warp for balance,
+    // chunks of 64-4096 candidates (the table modes keep at most
+    // kCj2MaxTableChunks per-chunk counts).
+    const int occ = cj2_blocks_per_sm(lv.seg != 0, lv.emit);
+    const int bpsm = std::max(1, std::min(occ, L.join_bpsm > 0 ? L.join_bpsm : 16));
+    const uint64_t resident = (uint64_t)L.num_sms * bpsm * (kJThreads / 32);
+    uint64_t chunk = (total + resident * 8 - 1) / (resident * 8);
+    chunk = std::min<uint64_t>(std::max<uint64_t>(chunk, 64), 4096);
+    if (lv.emit == kEmitTable)
+      chunk = std::max<uint64_t>(chunk, (total + kCj2MaxTableChunks - 1) / kCj2MaxTableChunks);
+    chunk = (chunk + 31) & ~uint64_t(31);
+    const uint64_t nchunks = (total + chunk - 1) / chunk;
+    const uint64_t blocks = std::min<uint64_t>((uint64_t)L.num_sms * bpsm,
+                                               (nchunks + kJThreads / 32 - 1) / (kJThreads / 32));
+    const int gq = (int)std::max<uint64_t>(blocks, 1);
+    unsigned long long* q = s.take<unsigned long long>(2);
+    SRDL_CUDA(cudaMemsetAsync(q, 0, 2 * sizeof(unsigned long long), L.stream));
+#define SRDL_CJ2(MODE, Q, CC)                                                                     \
+  (lv.seg ? join_cj2_kernel<MODE, true><<<gq, kJThreads, 0, L.stream>>>(                           \
+                lv, in, w.offs, w.drv, w.beg, w.orange, w.obm, total, chunk, Q, out, out_keys, cnt, \
+                CC)                                                                               \
+          : join_cj2_kernel<MODE, false><<<gq, kJThreads, 0, L.stream>>>(                          \
+                lv, in, w.offs, w.drv, w.beg, w.orange, w.obm, total, chunk, Q, out, out_keys, cnt, \
+                CC))
     if (lv.emit == kEmitCount) {
-      SRDL_CJ2(kModeCount, nullptr);
+      SRDL_CJ2(kModeCount, q, nullptr);
       count_launches(1);
     } else if (lv.emit == kEmitKeys) {
-      SRDL_CJ2(kModeKeys, nullptr);
+      SRDL_CJ2(kModeKeys, q, nullptr);
       count_launches(1);
     } else {
-      uint64_t* wc = s.take<uint64_t>(warps + 1);
-      uint64_t* wo = s.take<uint64_t>(warps + 1);
-      SRDL_CJ2(kModeTableCount, wc);
+      uint64_t* cc = s.take<uint64_t>(nchunks + 1);
+      uint64_t* co = s.take<uint64_t>(nchunks + 1);
+      SRDL_CJ2(kModeTableCount, q, cc);
       SRDL_CUDA(cudaGetLastError());
-      exclusive_scan_u64(L, wc, warps, wo, s);
-      SRDL_CUDA(cudaMemcpyAsync(d_out_n, wo + warps, 8, cudaMemcpyDeviceToDevice, L.stream));
-      SRDL_CJ2(kModeTableWrite, wo);
+      exclusive_scan_u64(L, cc, nchunks, co, s);
+      SRDL_CUDA(cudaMemcpyAsync(d_out_n, co + nchunks, 8, cudaMemcpyDeviceToDevice, L.stream));
+      SRDL_CJ2(kModeTableWrite, q + 1, co);
       count_launches(2);
     }
 #undef SRDL_CJ2
