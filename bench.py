@@ -295,7 +295,8 @@ SERVE_POOL = 48          # distinct inputs per program; requests draw from them
 SERVE_REQUESTS = 512
 SERVE_DESC = ('served queries: Poisson arrivals, 50% TC / 30% SG / 20% triangle count, input '
               'edges log-uniform in [1e3, 4e6] (TC subcritical n=2m, SG forest n<=5,000, '
-              'triangle R-MAT), 120 GB admission budget, 4 workers, continuous batching')
+              'triangle R-MAT), 120 GB admission budget (runs held to their reservations), '
+              '8 workers, continuous batching')
 
 
 def serve_pool():
@@ -352,8 +353,14 @@ def run_served(args, rank, world):
       st = replay(srv, reqs, offs)
       got = [r.result for r in reqs]
       assert results is None or got == results  # same answers every replay
+      assert not any(r.error for r in reqs)
       results = got
       sums.append(st.summary())
+    memory = {'budget_bytes': srv.budget, 'peak_in_use_bytes': srv.peak_in_use,
+              'peak_reserved_bytes': srv.peak_reserved, 'runs_outgrowing_reservation': srv.retried,
+              'requests_held_back': len(srv.held_back),
+              'note': 'peak_in_use: device bytes all handles held and cached (libsrdl '
+                      'srdl_mem_stats), sampled after every run'}
   h2d = sum(int(list(r.inputs.values())[0].nbytes) for r in serve_requests(pool, SERVE_REQUESTS, 11))
   with Server(progs, workers=1, batching=False) as plain_srv:
     reqs = serve_requests(pool, SERVE_REQUESTS, seed=11)
@@ -373,6 +380,7 @@ def run_served(args, rank, world):
                    'p99': statistics.median(s['p99_ms'] for s in sums)},
     'mean_batch': statistics.median(s['mean_batch'] for s in sums),
     'plain_loop': pst, 'speedup_vs_plain_loop': qps / pst['queries_per_s'],
+    'memory': memory,
     'e2e': {'value': qps, 'unit': 'queries/s', 'h2d_bytes_per_step': h2d,
             'd2h_bytes_per_step': 8 * SERVE_REQUESTS,
             'note': 'every request is end to end: host rows in, its size/count read back'},

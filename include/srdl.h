@@ -75,9 +75,10 @@ int srdl_set_stream(srdl_db* db, void* stream);
  * device time and algorithmic bytes in srdl_stats_json ("kernels"). */
 int srdl_set_profiling(srdl_db* db, int enable);
 
-/* Per-handle tuning options (the autotuner's knobs; results never change):
+/* Per-handle options (the autotuner's knobs, which never change a result,
+ * and the run's memory limit):
  *   "bitmap_mb"        budget for bitmaps of long child lists (MB, 0 = none;
- *                      default SRDL_BITMAP_MB or 256)
+ *                      default SRDL_BITMAP_MB or 768)
  *   "hash_min"         hash child lists longer than this (0 = never; default
  *                      SRDL_HASH_MIN or 0)
  *   "lsm_compact_pct"  Device2LevelIndex: merge HEAD into FULL once HEAD
@@ -87,6 +88,9 @@ int srdl_set_profiling(srdl_db* db, int enable);
  *                      b-bit keys runs ceil(b / radix_bits) passes
  *   "join_blocks_per_sm"  join launches use at most this many blocks per
  *                      SM, 1..64 (default 16): the candidates per warp
+ *   "mem_limit_mb"     device memory a run may hold (MB, 0 = no limit,
+ *                      the default): past it the run stops with status 5
+ *                      (see srdl_mem_stats)
  *   "shard_world",     evaluate as shard "shard_rank" of "shard_world"
  *   "shard_rank"       (default 0 of 1): rules the plan marks
  *                      "shard": "key" keep only bindings whose "shard_var"
@@ -181,6 +185,20 @@ int64_t srdl_dump(srdl_db* db, const char* rel, uint32_t* out_rows, uint64_t cap
 
 /* JSON run statistics (iterations per step, timings, derived rows). */
 int srdl_stats_json(srdl_db* db, char* buf, uint64_t cap);
+
+/* Device memory of the database's stream, measured by its caching arena:
+ * out4[0] bytes held by live buffers now, out4[1] the most held during the
+ * last srdl_run (its peak, recorded whether it succeeded or not), out4[2]
+ * bytes cached for reuse, out4[3] the run limit set by the "mem_limit_mb"
+ * option (0: none).  A run that would hold more than the limit stops with
+ * status 5; its database keeps nothing of that run.  No reference
+ * counterpart (the reference runs one query and never limits it). */
+int srdl_mem_stats(srdl_db* db, uint64_t* out4);
+
+/* Give the blocks the database's stream caches for reuse back to the device
+ * (a server does this for idle handles when its memory budget is tight; the
+ * next run allocates afresh).  No reference counterpart. */
+int srdl_trim_cache(srdl_db* db);
 
 /* SHA-256 of FULL(rel) as srdl_dump returns it (rows sorted, declared
  * column order, row-major little-endian uint32) into out32[32]: the parity

@@ -372,6 +372,23 @@ int srdl_stats_json(srdl_db* h, char* buf, uint64_t cap) {
   return 0;
 }
 
+int srdl_mem_stats(srdl_db* h, uint64_t* out4) {
+  if (!h || !out4) return kErrArg;
+  SRDL_GUARD(0, {
+    const srdl::ArenaUse u = h->db->mem_stats();
+    out4[0] = u.in_use;
+    out4[1] = u.peak;
+    out4[2] = u.cached;
+    out4[3] = u.limit;
+    return 0;
+  })
+}
+
+int srdl_trim_cache(srdl_db* h) {
+  if (!h) return kErrArg;
+  SRDL_GUARD(0, h->db->trim_cache(); return 0;)
+}
+
 // ------------------------------------------------------ kernel primitives
 
 static Launch launch_for(void* stream) {

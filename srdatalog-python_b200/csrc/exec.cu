@@ -281,7 +281,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
   for (size_t li = 0; li < levels.size(); li++) {
     LevelSpec& lv = levels[li];
     const bool last = li + 1 == levels.size();
-    DevBuf wscr(join_work_scratch_bytes(cur.n) + join_expand_scratch_bytes(L_), L_.stream);
+    DevBuf wscr(join_work_scratch_bytes(cur.n), L_.stream);
     Scratch s{wscr.as<char>(), wscr.bytes(), 0};
     size_t pid = prof_begin("join_count");
     JoinWork w = join_count(L_, lv, cur, s);
@@ -300,6 +300,9 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
       lv.seg_rank = (uint32_t)shard_rank_;
       total = seg_owned(total, lv.seg, shard_world_, shard_rank_);
     }
+    // the expand pass's own scratch, sized for this level's candidates
+    DevBuf xscr(join_expand_scratch_bytes(L_, total), L_.stream);
+    Scratch xs{xscr.as<char>(), xscr.bytes(), 0};
     if (last) {
       if (op.count) {
         lv.emit = kEmitCount;
@@ -320,7 +323,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
           lv.grp_counts = gc.as<unsigned long long>();
         }
         pid = prof_begin("join_expand_count");
-        join_expand(L_, lv, cur, w, total, nullptr, nullptr, d_small_.as<uint64_t>() + 2, s);
+        join_expand(L_, lv, cur, w, total, nullptr, nullptr, d_small_.as<uint64_t>() + 2, xs);
         if (lv.grp_counts) {
           std::vector<uint64_t> h(lv.n_groups);
           SRDL_CUDA(cudaMemcpyAsync(h.data(), gc.as<void>(), h.size() * 8, cudaMemcpyDeviceToHost,
@@ -344,7 +347,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
         ch.keys = DevBuf(std::max<uint64_t>(total, 1) * 8, L_.stream);
         pid = prof_begin("join_expand_keys");
         join_expand(L_, lv, cur, w, total, nullptr, ch.keys.as<uint64_t>(),
-                    d_small_.as<uint64_t>() + 2, s);
+                    d_small_.as<uint64_t>() + 2, xs);
         // a filter-free two-source product emits exactly its candidates
         const bool exact = lv.kind == kCartesian && lv.nsrc == 2 && lv.src[0].out_slot >= 0 &&
                            lv.src[1].out_slot >= 0 && lv.nfilt == 0;
@@ -368,7 +371,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
       DevBuf count(8, L_.stream);
       SRDL_CUDA(cudaMemsetAsync(count.as<void>(), 0, 8, L_.stream));
       pid = prof_begin("join_expand_table");
-      join_expand(L_, lv, cur, w, total, &next, nullptr, count.as<uint64_t>(), s);
+      join_expand(L_, lv, cur, w, total, &next, nullptr, count.as<uint64_t>(), xs);
       prof_end(pid, 4.0 * total * std::max(1, lv.nsrc), (double)total);
       next.n = total;
       next.d_n = count.as<uint64_t>();
@@ -715,9 +718,37 @@ void Database::exec_ops(const Step& st, uint64_t it) {
 }
 
 void Database::run(uint64_t max_iters) {
+  try {
+    run_steps(max_iters);
+  } catch (...) {
+    // a failed run keeps none of its relations (their buffers go back to
+    // the arena); the staged inputs stay for the next run
+    cudaStreamSynchronize(L_.stream);
+    reset_device_state();
+    throw;
+  }
+}
+
+void Database::run_steps(uint64_t max_iters) {
   init_device();
   SRDL_REQUIRE(shard_rank_ < shard_world_, kErrArg, "shard_rank must be below shard_world");
   reset_device_state();
+  // the run's device-memory limit applies to every buffer the run holds,
+  // the staged inputs included; the peak is recorded whether it succeeds
+  arena_set_limit(L_.stream, 0);
+  arena_reset_peak(L_.stream);
+  struct MemRecord {
+    Database* db;
+    ~MemRecord() { db->mem_run_ = arena_use(db->L_.stream); }
+  } mem_record{this};
+  if (opt_mem_limit_) {
+    const ArenaUse u = arena_use(L_.stream);
+    SRDL_REQUIRE(u.in_use <= opt_mem_limit_, kErrCapacity,
+                 "device memory limit of the run exceeded: " + std::to_string(u.in_use) +
+                     " bytes held before it starts, limit " + std::to_string(opt_mem_limit_) +
+                     " (mem_limit_mb)");
+    arena_set_limit(L_.stream, opt_mem_limit_);
+  }
   const uint64_t launches0 = launches_total();
   auto t0 = std::chrono::steady_clock::now();
   opstats_.clear();
@@ -776,6 +807,13 @@ void Database::run(uint64_t max_iters) {
   }
   launches_ = launches_total() - launches0;
   prof_collect();
+}
+
+ArenaUse Database::mem_stats() const {
+  ArenaUse u = dev_ready_ ? arena_use(L_.stream) : ArenaUse{};
+  u.peak = mem_run_.peak;
+  u.limit = opt_mem_limit_;
+  return u;
 }
 
 uint64_t Database::size(const std::string& name) {
@@ -869,6 +907,7 @@ std::string Database::stats_json() const {
       << ",\"max_ms\":" << kv.second.max_ms << ",\"calls\":" << kv.second.calls << "}";
     ofirst = false;
   }
+  o << "},\"mem\":{\"peak_bytes\":" << mem_run_.peak << ",\"limit_bytes\":" << opt_mem_limit_;
   o << "},\"alloc\":{\"ms\":" << alloc_.ms << ",\"max_ms\":" << alloc_.max_ms
     << ",\"calls\":" << alloc_.calls << ",\"pool_reserved_gb\":" << pool_reserved_gb_;
   o << "},\"counts\":{";

@@ -112,32 +112,31 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
       continue;
     }
     if (lv.kind == kColumnJoin && lv.nsrc == 2) {
-      // Leapfrog seek: clip both sorted lists to their common value range
-      // [max(first), min(last)]; only that part can intersect.  The shorter
-      // clipped list drives, the other's clipped range is probed.
+      // Leapfrog seek: the shorter list drives; it is clipped to the other
+      // list's value range [first, last] (only that part can intersect),
+      // searching only at an end that lies outside it.  The other list's
+      // range is probed as it is.
       uint32_t b0, n0, b1, n1;
       src_list(lv.src[0], in, r, b0, n0);
       src_list(lv.src[1], in, r, b1, n1);
       const uint32_t* v0 = lv.src[0].prefix_slot < 0 ? lv.src[0].t.roots : lv.src[0].t.lo;
       const uint32_t* v1 = lv.src[1].prefix_slot < 0 ? lv.src[1].t.roots : lv.src[1].t.lo;
-      uint32_t e0 = b0 + n0, e1 = b1 + n1;
-      if (n0 && n1) {
-        const uint32_t lo = max(v0[b0], v1[b1]), hi = min(v0[e0 - 1], v1[e1 - 1]);
-        if (lo > hi) {
-          e0 = b0;
-        } else {
-          b0 = lower_bound_u32(v0, b0, e0, lo);
-          e0 = hi == 0xffffffffu ? e0 : lower_bound_u32(v0, b0, e0, hi + 1);
-          b1 = lower_bound_u32(v1, b1, e1, lo);
-          e1 = hi == 0xffffffffu ? e1 : lower_bound_u32(v1, b1, e1, hi + 1);
-        }
+      const int bd = n1 < n0 ? 1 : 0;
+      const uint32_t* dv = bd ? v1 : v0;
+      const uint32_t* ov = bd ? v0 : v1;
+      uint32_t db = bd ? b1 : b0, de = db + (bd ? n1 : n0);
+      const uint32_t ob = bd ? b0 : b1, oe = ob + (bd ? n0 : n1);
+      if (db < de && ob < oe) {
+        const uint32_t lo = ov[ob], hi = ov[oe - 1];
+        if (dv[db] < lo) db = lower_bound_u32(dv, db, de, lo);
+        if (db < de && dv[de - 1] > hi) de = lower_bound_u32(dv, db, de, hi + 1);
+      } else {
+        de = db;
       }
-      const uint32_t l0 = e0 - b0, l1 = e1 - b1;
-      const int bd = l1 < l0 ? 1 : 0;
-      work[r] = (l0 && l1) ? (bd ? l1 : l0) : 0;
+      work[r] = de - db;
       drv[r] = (uint8_t)bd;
-      beg[r] = bd ? b1 : b0;
-      orange[r] = bd ? make_uint2(b0, e0) : make_uint2(b1, e1);
+      beg[r] = db;
+      orange[r] = make_uint2(ob, oe);
       if (obm) {
         // the probed (other) list's bitmap, if its parent value has one
         const uint32_t* obd = bd ? lv.src[0].t.bdir : lv.src[1].t.bdir;
@@ -727,9 +726,12 @@ static int jgrid(uint64_t n, const Launch& L) {
 // Most per-chunk counts the two-source column join keeps in its table modes.
 constexpr uint64_t kCj2MaxTableChunks = 1ull << 18;
 
-size_t join_expand_scratch_bytes(const Launch& L) {
-  const uint64_t warps = (uint64_t)L.num_sms * (L.join_bpsm > 0 ? L.join_bpsm : 16) * (kJThreads / 32);
-  const uint64_t n = std::max<uint64_t>(warps, kCj2MaxTableChunks);
+size_t join_expand_scratch_bytes(const Launch& L, uint64_t total) {
+  // per-warp counts of the generic kernels' table modes, or per-chunk counts
+  // of the two-source column join's (chunks of at least 64 candidates)
+  const uint64_t warps = (uint64_t)jgrid(total, L) * (kJThreads / 32);
+  const uint64_t chunks = std::min<uint64_t>(kCj2MaxTableChunks, (total + 63) / 64);
+  const uint64_t n = std::max<uint64_t>(warps, chunks);
   return 2 * ((n + 1) * 8 + 255) + scan_scratch_bytes(n) + 4096;
 }
 

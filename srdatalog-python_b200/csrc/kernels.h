@@ -96,11 +96,12 @@ void build_roots(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* ro
 // slot or kNoHash; every child of a hashed list is inserted into `pool`,
 // which the caller pre-fills with 0xff bytes.
 // Bitmaps of long child lists.  bitmap_plan: cnt[k] = values whose child
-// list has at least (1024 << k) entries, k < kBitmapLevels.  bitmap_build:
+// list has at least (kBitmapMinLen << k) entries, k < kBitmapLevels.  bitmap_build:
 // bdir[v] = a fresh slot for lists of at least min_len entries (kNoBitmap
 // otherwise); every key (v, c) of such a list sets bit c of v's bitmap
 // (pool zeroed by the caller); *d_slots receives the slot count.
-constexpr int kBitmapLevels = 7;
+constexpr int kBitmapLevels = 10;
+constexpr uint32_t kBitmapMinLen = 128;
 void bitmap_plan(const Launch& L, const uint32_t* dir, uint32_t dir_n, unsigned long long* cnt);
 void bitmap_build(const Launch& L, const uint64_t* keys, uint64_t n, const uint32_t* dir,
                   uint32_t dir_n, uint32_t min_len, uint32_t* bdir, uint32_t* pool, uint32_t bwords,
@@ -238,8 +239,9 @@ JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scrat
 // surviving bindings are appended to `out_table` (emit table, in input
 // order: the table stays sorted), to `out_keys` (emit keys, any order) or
 // counted (emit count) via *d_out_n, which the caller zeroes.  Output
-// capacity = total.
-size_t join_expand_scratch_bytes(const Launch& L);
+// capacity = total.  The scratch for a level of `total` candidates comes
+// from join_expand_scratch_bytes(L, total).
+size_t join_expand_scratch_bytes(const Launch& L, uint64_t total);
 void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const JoinWork& w,
                  uint64_t total, Table* out_table, uint64_t* out_keys, uint64_t* d_out_n,
                  Scratch& s);

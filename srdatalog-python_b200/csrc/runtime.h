@@ -35,6 +35,20 @@ enum Ver { kFull = 0, kDelta = 1, kNew = 2 };
 class StreamArena;
 void arena_attach(cudaStream_t s);   // one reference per database using `s`
 void arena_detach(cudaStream_t s);   // last reference frees the cached blocks
+// Device bytes of the stream's arena: handed out to live buffers now, the
+// most handed out since the last reset_peak, cached for reuse, and the limit
+// on the bytes it holds, handed out plus cached (0: none).  Under a limit the
+// cache is dropped before a new block would pass it, and a request that
+// would take the handed-out bytes alone past it fails with status 5
+// (kErrCapacity) instead of allocating: a server admits work against a
+// device-memory budget and holds each run to its reservation this way.
+struct ArenaUse {
+  size_t in_use = 0, peak = 0, cached = 0, limit = 0;
+};
+ArenaUse arena_use(cudaStream_t s);
+void arena_set_limit(cudaStream_t s, size_t bytes);
+void arena_reset_peak(cudaStream_t s);
+void arena_trim(cudaStream_t s);  // frees the cached blocks (stream-ordered)
 
 // Owning device allocation: from the stream's arena when one is attached,
 // else straight from the stream-ordered pool.
@@ -247,6 +261,13 @@ class Database {
   // Rows of FULL in declared column order, lexicographically sorted.
   int64_t dump(const std::string& rel, uint32_t* out, uint64_t cap_rows);
   std::string stats_json() const;
+  // Arena bytes of this database's stream: in use now, the last run's peak,
+  // cached, and the limit.
+  ArenaUse mem_stats() const;
+  // Frees the blocks this database's stream arena caches for reuse.
+  void trim_cache() {
+    if (dev_ready_) arena_trim(L_.stream);
+  }
   bool any_loaded() const;
   void stage_facts(Relation& r);
   uint64_t staged_rows(const std::string& name) {
@@ -281,6 +302,8 @@ class Database {
   int64_t opt_bitmap_mb_ = -1;      // -1: SRDL_BITMAP_MB or the default
   int64_t opt_hash_min_ = -1;       // -1: SRDL_HASH_MIN or off
   int64_t opt_lsm_pct_ = 10;        // HEAD -> FULL merge threshold (% of FULL)
+  uint64_t opt_mem_limit_ = 0;      // bytes a run may hold on the device (0: no limit)
+  ArenaUse mem_run_{};              // the last run's arena use (peak: its most held)
   int64_t shard_rank_ = 0, shard_world_ = 1;  // this database's shard among shard_world_
   srdl_exchange_fn xfn_ = nullptr;  // moves tuples between shards (exchange ops)
   void* xuser_ = nullptr;
@@ -323,6 +346,7 @@ class Database {
   void ensure_bitmaps(Index& ix);
   void sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full,
                  const Index* head = nullptr, int key_bits = 0);
+  void run_steps(uint64_t max_iters);
   void exec_ops(const Step& st, uint64_t iteration);
   void exec_pipeline(const Op& op, bool recursive, uint64_t iteration);
   void op_rebuild(const Step& st, size_t pos, const Op& op);

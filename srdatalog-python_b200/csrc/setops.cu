@@ -369,7 +369,7 @@ __global__ void bitmap_plan_kernel(const uint32_t* __restrict__ dir, uint32_t nv
     const uint32_t len = dir[v + 1] - dir[v];
 #pragma unroll
     for (int k = 0; k < kBitmapLevels; k++)
-      if (len >= (1024u << k)) atomicAdd(&cnt[k], 1ull);
+      if (len >= (kBitmapMinLen << k)) atomicAdd(&cnt[k], 1ull);
   }
 }
 

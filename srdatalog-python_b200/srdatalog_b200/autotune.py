@@ -37,14 +37,14 @@ import numpy as np
 LSM = 'SRDatalog::GPU::Device2LevelIndex'
 
 DEFAULT_SPACE = {
-  'bitmap_mb': [0, 64, 256, 1024],
+  'bitmap_mb': [0, 64, 256, 768, 2048],
   'lsm_compact_pct': [5, 10, 25],
   'radix_bits': [6, 7, 8],
   'join_blocks_per_sm': [8, 16, 32],
 }
 
 # library defaults: the tuner's starting point
-DEFAULTS = {'bitmap_mb': 256, 'lsm_compact_pct': 10, 'radix_bits': 8, 'join_blocks_per_sm': 16}
+DEFAULTS = {'bitmap_mb': 768, 'lsm_compact_pct': 10, 'radix_bits': 8, 'join_blocks_per_sm': 16}
 
 
 @dataclass

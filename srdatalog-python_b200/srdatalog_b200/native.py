@@ -50,6 +50,8 @@ SIGNATURES = {
   'srdl_count': (_u64, [_vp, _cp]),
   'srdl_dump': (_i64, [_vp, _cp, _u32p, _u64]),
   'srdl_stats_json': (ctypes.c_int, [_vp, ctypes.c_char_p, _u64]),
+  'srdl_mem_stats': (ctypes.c_int, [_vp, ctypes.POINTER(_u64)]),
+  'srdl_trim_cache': (ctypes.c_int, [_vp]),
   'srdl_sort_unique_scratch_bytes': (_u64, [_u64, ctypes.c_int]),
   'srdl_sort_unique_u64': (ctypes.c_int, [_vp, _u64, ctypes.c_int, _vp, _vp, _vp, _u64, _vp]),
   'srdl_set_difference_scratch_bytes': (_u64, [_u64]),
@@ -182,7 +184,8 @@ class Database:
     check(lib().srdl_set_exchange(self._h, self._xfn, None), 'srdl_set_exchange')
 
   def set_option(self, name: str, value: int) -> None:
-    '''Tuning option (srdl_set_option): bitmap_mb, hash_min, lsm_compact_pct.'''
+    '''Option (srdl_set_option): bitmap_mb, hash_min, lsm_compact_pct,
+    radix_bits, join_blocks_per_sm, shard_world, shard_rank, mem_limit_mb.'''
     check(lib().srdl_set_option(self._h, name.encode(), int(value)), 'srdl_set_option')
 
   def set_count_groups(self, rule: str, bounds) -> None:
@@ -246,6 +249,18 @@ class Database:
       if m != n:
         raise SrdlError(f'srdl_dump({rel})', -1, 'size changed')
     return out
+
+  def mem_stats(self) -> dict:
+    '''Device bytes of this handle's stream (srdl_mem_stats): held now, the
+    last run's peak, cached for reuse, and the run limit (0: none).'''
+    out = (_u64 * 4)()
+    check(lib().srdl_mem_stats(self._h, out), 'srdl_mem_stats')
+    return {'in_use': int(out[0]), 'peak': int(out[1]), 'cached': int(out[2]),
+            'limit': int(out[3])}
+
+  def trim_cache(self) -> None:
+    '''Return the blocks this handle's stream caches to the device.'''
+    check(lib().srdl_trim_cache(self._h), 'srdl_trim_cache')
 
   def stats(self) -> dict:
     buf = ctypes.create_string_buffer(1 << 16)

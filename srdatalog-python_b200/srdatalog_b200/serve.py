@@ -1,10 +1,21 @@
 '''Serving: a request loop that admits Datalog queries of mixed programs and
 sizes against a device-memory budget and batches them continuously.
 
-* Admission: every request carries an estimate of the device memory its
-  evaluation needs (`footprint`); it is admitted when the sum over admitted,
-  unfinished requests stays within the budget, in arrival order (a large
-  request waits; later small ones do not overtake it).
+* Admission: every request holds a reservation of device memory
+  (`footprint`, first an estimate from its input size); it is admitted when
+  the reservations of the admitted, unfinished requests plus the blocks idle
+  handles cache stay within the budget, in arrival order (a large request
+  waits; later small ones do not overtake it).
+* Estimates: a request's first reservation comes from its program's measured
+  runs: the largest peak per input edge of runs in its size class (input
+  edges to a power of two; the nearest class seen), times 1.25, with a 1 MB
+  floor; before any run, from the spec's bytes_per_edge.
+* Enforcement: a run may hold at most its batch's reservations on the device
+  (libsrdl's per-run limit, option mem_limit_mb, measured by the handle's
+  caching arena).  A run that outgrows it stops with status 5; its requests
+  go back to the head of the queue with twice the reservation and are
+  admitted again when memory frees up.  A request that outgrows the whole
+  budget fails cleanly (`error` set, result -1) while the others proceed.
 * Continuous batching: a dispatcher hands work to whichever of the `workers`
   is idle.  A worker takes the oldest admitted request and, with it, every
   admitted request of the same program (up to `max_batch`), and evaluates
@@ -14,6 +25,10 @@ sizes against a device-memory budget and batches them continuously.
 * Workers own their database handles, so each has its own CUDA stream and
   the runs of different workers overlap on the GPU; relations stay on the
   device until the request's result (its size or count) has been read.
+* Measured memory: after every run the server reads, from the library, the
+  device bytes every handle holds and caches (srdl_mem_stats); `peak_in_use`
+  is the largest such total seen, `peak_reserved` the largest sum of
+  reservations.
 
 A request's result is identical alone and in any mix: instances of a union
 cannot interact (see batch.py), and runs on different handles share nothing.
@@ -29,7 +44,9 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from .batch import make_union
-from .native import Database
+from .native import Database, SrdlError
+
+_MB = 1 << 20
 
 
 @dataclass
@@ -38,7 +55,10 @@ class Request:
   program: str                 # key into the server's plans
   inputs: dict                 # relation -> (m, 2) uint32 rows
   arrival: float = 0.0         # seconds (perf_counter clock)
-  footprint: int = 0           # estimated device bytes
+  footprint: int = 0           # reserved device bytes (estimate; doubled when outgrown)
+  retries: int = 0             # runs that outgrew the reservation
+  peak_bytes: int = 0          # measured peak of the run that answered it (its union's)
+  error: str = ''              # set when the request failed (result stays -1)
   admitted: float = -1.0
   started: float = -1.0
   finished: float = -1.0
@@ -88,8 +108,14 @@ class Server:
   def __init__(self, programs: dict, device: int = 0, workers: int = 8,
                budget_bytes: int = 120 << 30, max_batch: int = 16, batching: bool = True,
                keep_rows: bool = False, batch_max_edges: int = 1 << 20,
-               batch_max_span: int = 1 << 23):
+               batch_max_span: int = 1 << 23, learn: bool = True):
     self.programs = programs
+    # Reservation estimates learned from measured peaks: per program and
+    # size class (input edges to a power of two), the largest peak per input
+    # edge seen.  Without learning (or before the program's first run) the
+    # spec's bytes_per_edge with a 1 MB floor.
+    self.learn = learn
+    self.est_ratio: dict = {}
     self.device = device
     self.budget = budget_bytes
     self.max_batch = max_batch if batching else 1
@@ -103,8 +129,13 @@ class Server:
     self.cv = threading.Condition()
     self.pending: list[Request] = []   # arrived, waiting for admission (FIFO)
     self.ready: list[Request] = []     # admitted, not started
-    self.in_use = 0
-    self.peak_in_use = 0
+    self.in_use = 0                    # reservations of admitted, unfinished requests
+    self.peak_reserved = 0
+    self.idle_cache: dict = {}         # handle id -> (handle, bytes it caches while idle)
+    self.handles: list = []            # every handle of every worker (measured usage)
+    self.peak_in_use = 0               # largest measured device bytes of all handles
+    self.retried = 0                   # runs that outgrew their reservation
+    self.held_back: set = set()        # ids of requests that waited for the budget
     self.submitted = 0
     self.done: list[Request] = []
     self.errors: list[BaseException] = []
@@ -117,9 +148,10 @@ class Server:
   # ------------------------------------------------------------ client side
   def submit(self, req: Request) -> None:
     spec = self.programs[req.program]
-    if not req.footprint:
-      req.footprint = default_footprint(spec, req)
     with self.cv:
+      if not req.footprint:
+        req.footprint = self._estimate(spec, req)
+      req.footprint = min(req.footprint, self.budget)
       self.pending.append(req)
       self.submitted += 1
       self._admit()
@@ -155,18 +187,56 @@ class Server:
     now = time.perf_counter()
     while self.pending:
       r = self.pending[0]
-      # a request larger than the whole budget runs alone
-      if self.in_use + r.footprint > self.budget and self.in_use > 0:
+      cached = sum(b for _, b in self.idle_cache.values())
+      # a request as large as the whole budget runs alone
+      if self.in_use + cached + r.footprint > self.budget and self.in_use + cached > 0:
+        if cached:
+          self._trim_idle()
+          continue
+        self.held_back.add(r.rid)
         break
       self.pending.pop(0)
       self.in_use += r.footprint
-      self.peak_in_use = max(self.peak_in_use, self.in_use)
+      self.peak_reserved = max(self.peak_reserved, self.in_use)
       r.admitted = now
       self.ready.append(r)
 
+  def _trim_idle(self) -> None:
+    '''Idle handles give their cached blocks back (called with cv held: a
+    worker takes its handle out of idle_cache under cv before running it).'''
+    for key, (db, _) in list(self.idle_cache.items()):
+      db.trim_cache()
+      self.idle_cache[key] = (db, 0)
+
+  def _estimate(self, spec: ProgramSpec, req: Request) -> int:
+    m = _edges(req)
+    known = self.est_ratio.get(req.program)
+    if not known:
+      return default_footprint(spec, req)
+    b = m.bit_length()
+    nearest = min(known, key=lambda k: (abs(k - b), -k))   # ties: the larger size class
+    return max(1 << 20, int(m * known[nearest] * 1.25))
+
+  def _observe(self, batch: list, peak: int) -> None:
+    '''Learn from a successful run's measured peak (cv held): the largest
+    peak per input edge of the program's runs with as many edges, to a
+    power of two.'''
+    if not self.learn or peak <= 0:
+      return
+    m = max(1, sum(_edges(r) for r in batch))
+    ratios = self.est_ratio.setdefault(batch[0].program, {})
+    b = m.bit_length()
+    ratios[b] = max(ratios.get(b, 0.0), peak / m)
+
+  def _requeue(self, r: Request) -> None:
+    '''Back into the pending queue in arrival order (ahead of later arrivals).'''
+    i = 0
+    while i < len(self.pending) and (self.pending[i].arrival, self.pending[i].rid) <= (r.arrival, r.rid):
+      i += 1
+    self.pending.insert(i, r)
+
   def _take_batch(self) -> list:
     first = self.ready[0]
-    spec = self.programs[first.program]
     if self.max_batch == 1 or _edges(first) > self.batch_max_edges:
       batch = [first]
     else:
@@ -183,6 +253,14 @@ class Server:
     self.ready = [r for r in self.ready if id(r) not in ids]
     return batch
 
+  def _measure(self) -> None:
+    '''Device bytes all handles hold and cache now, read from the library.'''
+    total = 0
+    for db in list(self.handles):
+      m = db.mem_stats()
+      total += m['in_use'] + m['cached']
+    self.peak_in_use = max(self.peak_in_use, total)
+
   def _worker(self, wid: int) -> None:
     dbs: dict = {}
     try:
@@ -197,13 +275,43 @@ class Server:
         for r in batch:
           r.started = t0
           r.batch_size = len(batch)
-        self._run(dbs, batch)
+        db = self._handle(dbs, batch[0].program)
+        with self.cv:
+          self.idle_cache.pop(id(db), None)
+        # the run may hold at most its requests' reservations
+        db.set_option('mem_limit_mb', max(1, sum(r.footprint for r in batch) // _MB))
+        outgrown = ''
+        try:
+          self._run(db, batch)
+        except SrdlError as e:
+          if e.code != 5:
+            raise
+          outgrown = str(e)
+        mem = db.mem_stats()
         t1 = time.perf_counter()
         with self.cv:
+          self._measure()
           for r in batch:
-            r.finished = t1
             self.in_use -= r.footprint
-          self.done.extend(batch)
+            r.peak_bytes = mem['peak']
+          if outgrown:
+            self.retried += 1
+            for r in batch:
+              if r.footprint >= self.budget:
+                r.error = outgrown
+                r.result = -1
+                r.finished = t1
+                self.done.append(r)
+              else:
+                r.retries += 1
+                r.footprint = min(self.budget, 2 * r.footprint)
+                self._requeue(r)
+          else:
+            self._observe(batch, mem['peak'])
+            for r in batch:
+              r.finished = t1
+            self.done.extend(batch)
+          self.idle_cache[id(db)] = (db, mem['cached'])
           self._admit()
           self.cv.notify_all()
     except BaseException as e:  # surface to drain()
@@ -211,14 +319,25 @@ class Server:
         self.errors.append(e)
         self.cv.notify_all()
     finally:
+      with self.cv:
+        for db in dbs.values():
+          self.idle_cache.pop(id(db), None)
+          if db in self.handles:
+            self.handles.remove(db)
       for db in dbs.values():
         db.close()
 
-  def _run(self, dbs: dict, batch: list) -> None:
-    spec = self.programs[batch[0].program]
-    db = dbs.get(batch[0].program)
+  def _handle(self, dbs: dict, program: str) -> Database:
+    db = dbs.get(program)
     if db is None:
-      db = dbs[batch[0].program] = Database(spec.plan, device=self.device)
+      db = dbs[program] = Database(self.programs[program].plan, device=self.device)
+      db.init_device()
+      with self.cv:
+        self.handles.append(db)
+    return db
+
+  def _run(self, db: Database, batch: list) -> None:
+    spec = self.programs[batch[0].program]
     db.clear_inputs()
     if spec.count_only:
       db.set_count_groups(spec.out, [])

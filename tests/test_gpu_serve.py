@@ -59,12 +59,62 @@ def test_mixed_requests_same_alone_and_in_the_mix():
       assert r.result == oracle.triangle_count(e)
 
 
+def peak_alone(req):
+  '''Device bytes a fresh handle holds at the peak of the request's run.'''
+  db = native.Database(load_plan(req.program))
+  for rel, rows in req.inputs.items():
+    db.load_rows(rel, rows)
+  db.run()
+  return db.mem_stats()['peak']
+
+
 def test_budget_is_never_exceeded():
+  '''Runs are held to their reservations and admitted within the budget;
+  the peak is the device bytes the library measured, not an estimate.'''
   reqs = make_requests(24, seed=8)
-  fps = [max(1 << 20, 512 * sum(v.shape[0] for v in r.inputs.values())) for r in reqs]
-  budget = max(fps)
+  budget = 4 * max(peak_alone(r) for r in reqs)
   with Server(programs(), workers=3, budget_bytes=budget) as srv:
     replay(srv, reqs, np.zeros(len(reqs)))
-    assert srv.peak_in_use <= budget
+    assert 0 < srv.peak_in_use <= budget
+    assert srv.peak_reserved <= budget
   for r in reqs:
+    assert not r.error
     assert r.result == alone(r)[0]
+    assert 0 < r.peak_bytes <= budget
+
+
+def test_outgrown_reservation_is_requeued_and_held_back():
+  '''Estimates far below the real need (1 MB): every run that outgrows its
+  reservation stops with status 5 and goes back to the queue with twice the
+  reservation; once reservations are large, only one run fits the budget at
+  a time and the others wait.  Every result still equals the request run
+  alone, and the measured device bytes never pass the budget.'''
+  progs = {'tc': ProgramSpec(load_plan('tc'), 'Path', bytes_per_edge=1)}
+  reqs = [Request(i, 'tc', {'ArcInput': W.uniform_edges(2000, 6000, 40 + i)}) for i in range(3)]
+  peak = max(peak_alone(r) for r in reqs)
+  mb = 1 << 20
+  grown = mb << max(0, (peak - 1) // mb).bit_length()    # the doubling's first reservation >= peak
+  budget = grown + grown // 2                            # room for one such run at a time
+  with Server(progs, workers=3, budget_bytes=budget, learn=False) as srv:
+    replay(srv, reqs, np.zeros(len(reqs)))
+    assert srv.retried >= len(reqs)
+    assert srv.held_back                                 # a grown request waited for the budget
+    assert 0 < srv.peak_in_use <= budget
+  for r in reqs:
+    assert not r.error and r.retries > 0
+    assert r.footprint <= budget and r.peak_bytes <= r.footprint
+    assert r.result == alone(r)[0]
+
+
+def test_request_beyond_the_budget_fails_cleanly():
+  '''A request whose run outgrows the whole budget fails (error set, result
+  -1) without stopping the server; the other request is answered.'''
+  progs = {'tc': ProgramSpec(load_plan('tc'), 'Path', bytes_per_edge=1)}
+  big = Request(0, 'tc', {'ArcInput': W.uniform_edges(2000, 6000, 40)})
+  small = Request(1, 'tc', {'ArcInput': W.uniform_edges(50, 80, 41)})
+  budget = max(8 << 20, 4 * peak_alone(small))
+  assert peak_alone(big) > budget
+  with Server(progs, workers=2, budget_bytes=budget, learn=False) as srv:
+    replay(srv, [big, small], np.zeros(2))
+  assert big.result == -1 and 'memory limit' in big.error
+  assert not small.error and small.result == alone(small)[0]

@@ -21,13 +21,15 @@ def test_admission_respects_budget_in_arrival_order():
     s.submit(req(i, 'tc', fp))
   assert [r.rid for r in s.ready] == [0, 1]       # 120 > 100: request 2 waits
   assert [r.rid for r in s.pending] == [2, 3]     # and 3 does not overtake it
-  assert s.peak_in_use == 80
+  assert s.peak_reserved == 80
+  assert s.held_back == {2}
 
 
 def test_oversized_request_runs_alone():
   s = Server(programs(), workers=0, budget_bytes=100)
   s.submit(req(0, 'tc', 500))
   assert [r.rid for r in s.ready] == [0]
+  assert s.ready[0].footprint == 100              # reserved: the whole budget, no more
   s.submit(req(1, 'tc', 10))
   assert [r.rid for r in s.pending] == [1]
 
@@ -63,3 +65,51 @@ def test_large_requests_run_alone_and_span_is_capped():
   assert [r.rid for r in s._take_batch()] == [0]          # over the edge limit: alone
   assert [r.rid for r in s._take_batch()] == [1, 2]       # spans 8 + 8 <= 20 < 24
   assert [r.rid for r in s._take_batch()] == [3, 4]
+
+
+def test_requeue_keeps_arrival_order():
+  s = Server(programs(), workers=0, budget_bytes=10)
+  for i in range(4):
+    r = req(i, 'tc', 10)
+    r.arrival = float(i)
+    s.submit(r)
+  assert [r.rid for r in s.ready] == [0] and [r.rid for r in s.pending] == [1, 2, 3]
+  back = s.ready.pop(0)                           # its run outgrew the reservation
+  s.in_use -= back.footprint
+  s._requeue(back)
+  assert [r.rid for r in s.pending] == [0, 1, 2, 3]
+  s._admit()
+  assert [r.rid for r in s.ready] == [0]
+
+
+class FakeHandle:
+  def __init__(self):
+    self.trimmed = 0
+
+  def trim_cache(self):
+    self.trimmed += 1
+
+
+def test_idle_caches_count_against_the_budget_and_are_trimmed():
+  s = Server(programs(), workers=0, budget_bytes=100)
+  h = FakeHandle()
+  s.idle_cache[id(h)] = (h, 70)                   # an idle handle caches 70 bytes
+  s.submit(req(0, 'tc', 50))                      # 70 + 50 > 100: its cache is given back
+  assert h.trimmed == 1 and s.idle_cache[id(h)] == (h, 0)
+  assert [r.rid for r in s.ready] == [0]
+
+
+def test_estimates_learn_from_measured_peaks():
+  s = Server(programs(), workers=0, budget_bytes=1 << 40)
+  small = req(0, 'tc', 0)                                      # 1 edge
+  assert s._estimate(s.programs['tc'], small) == 1 << 20       # spec default before any run
+  s._observe([small], 5 << 20)                                 # a 1-edge run peaked at 5 MB
+  assert s._estimate(s.programs['tc'], small) == int((5 << 20) * 1.25)
+  big = Request(1, 'tc', {'ArcInput': np.zeros((1 << 17, 2), np.uint32)})
+  assert s._estimate(s.programs['tc'], big) == int((1 << 17) * (5 << 20) * 1.25)  # nearest class
+  s._observe([big], 300 << 20)                                 # 2400 B per edge in its class
+  assert s._estimate(s.programs['tc'], big) == int((300 << 20) * 1.25)
+  assert s._estimate(s.programs['tc'], small) == int((5 << 20) * 1.25)
+  off = Server(programs(), workers=0, learn=False)
+  off._observe([small], 5 << 20)
+  assert off._estimate(off.programs['tc'], small) == 1 << 20
