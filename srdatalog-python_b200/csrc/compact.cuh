@@ -13,7 +13,9 @@
 // No block waits on another, so nothing can spin.  Selectors provide
 //   __device__ void block_setup(uint64_t begin, uint64_t end);  (all threads)
 //   __device__ bool select(uint64_t i);
-//   __device__ void emit(uint64_t i, uint64_t pos);
+//   using value_type = ...;
+//   __device__ value_type value(uint64_t i);        (what element i emits)
+//   __device__ void store(uint64_t pos, value_type v);
 #pragma once
 
 #include "common.cuh"
@@ -93,6 +95,14 @@ __global__ void __launch_bounds__(kCpThreads) cp_write_kernel(Sel sel, uint64_t 
     const uint64_t w0 = tile + (uint64_t)wid * (kCpItems * 32);
     const uint64_t wi = w0 + (uint64_t)lane * 32;
     const uint32_t my_word = (lane < kCpItems && wi < end) ? flags[wi / 32] : 0u;
+    // the eight rounds' element loads are all issued before the first
+    // store (coalesced either way; this keeps eight loads in flight)
+    typename Sel::value_type v[kCpItems];
+#pragma unroll
+    for (int r = 0; r < kCpItems; r++) {
+      const uint64_t i = w0 + (uint64_t)r * 32 + lane;
+      if (i < end) v[r] = sel.value(i);
+    }
     const uint32_t wcount = warp_sum((uint32_t)__popc(my_word));
     if (lane == 0) wtot[par][wid] = wcount;
     __syncthreads();
@@ -107,7 +117,7 @@ __global__ void __launch_bounds__(kCpThreads) cp_write_kernel(Sel sel, uint64_t 
 #pragma unroll
     for (int r = 0; r < kCpItems; r++) {
       const uint32_t m = __shfl_sync(kAllLanes, my_word, r);
-      if ((m >> lane) & 1u) sel.emit(w0 + (uint64_t)r * 32 + lane, pos + __popc(m & lt));
+      if ((m >> lane) & 1u) sel.store(pos + __popc(m & lt), v[r]);
       pos += __popc(m);
     }
     base += tile_total;
@@ -178,7 +188,9 @@ struct DedupDiffSel {
     }
     return true;
   }
-  __device__ void emit(uint64_t i, uint64_t pos) const { out[pos] = expand(a[i]); }
+  using value_type = uint64_t;
+  __device__ uint64_t value(uint64_t i) const { return expand(a[i]); }
+  __device__ void store(uint64_t pos, uint64_t v) const { out[pos] = v; }
 };
 
 // FULL position of every tile boundary: fpos[t] = lower_bound(FULL, first key
@@ -574,7 +586,9 @@ struct RootSel {
   __device__ bool select(uint64_t i) const {
     return i == 0 || (keys[i] >> 32) != (keys[i - 1] >> 32);
   }
-  __device__ void emit(uint64_t i, uint64_t pos) const { roots[pos] = (uint32_t)(keys[i] >> 32); }
+  using value_type = uint32_t;
+  __device__ uint32_t value(uint64_t i) const { return (uint32_t)(keys[i] >> 32); }
+  __device__ void store(uint64_t pos, uint32_t v) const { roots[pos] = v; }
 };
 
 }  // namespace srdl

@@ -289,7 +289,9 @@ struct OwnerSel {
     const uint64_t k = keys[i];
     return shard_owner(col0_lo ? (uint32_t)k : (uint32_t)(k >> 32), world) == dest;
   }
-  __device__ void emit(uint64_t i, uint64_t pos) const { out[pos] = keys[i]; }
+  using value_type = uint64_t;
+  __device__ uint64_t value(uint64_t i) const { return keys[i]; }
+  __device__ void store(uint64_t pos, uint64_t v) const { out[pos] = v; }
 };
 
 size_t shard_select_scratch_bytes(uint64_t n) { return cp_scratch_bytes(n); }

@@ -151,8 +151,10 @@ __device__ __forceinline__ void rs_prefetch(K* buf, const K* in, uint64_t tile, 
 // match instruction; the lowest such lane adds the group's size to the warp's
 // counter for the digit and passes the old value on.  The staged
 // (digit-ordered) tile reuses the buffer the current keys were read from.
+// Five resident blocks per SM (their shared memory fits; the register cap
+// that needs costs no spills).
 template <typename K, int DB>
-__global__ void __launch_bounds__(kRsThreads) rs_scatter(const K* __restrict__ in,
+__global__ void __launch_bounds__(kRsThreads, 5) rs_scatter(const K* __restrict__ in,
                                                          K* __restrict__ out, uint64_t n,
                                                          uint64_t chunk, int shift,
                                                          const uint32_t* __restrict__ offs,
@@ -193,7 +195,7 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter(const K* __restrict__ i
     __syncthreads();
     const uint32_t cnt = (uint32_t)((end - tile) < kRsTile ? (end - tile) : kRsTile);
     K key[kRsPerWarp / 32];
-    uint32_t rank[kRsPerWarp / 32];
+    uint32_t rank[kRsPerWarp / 32];  // rank in the warp's digit run | digit << 16
     // Warp `wid` owns keys [wid*256, +256) of the tile in rounds of 32, so the
     // (round, lane) order is the input order.  Each round's counter update
     // precedes the next round's (__syncwarp orders them): ranks are stable.
@@ -216,7 +218,7 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter(const K* __restrict__ i
       uint32_t old = 0;
       if (valid && lane == leader) old = atomicAdd(&wofs[wid][d], (uint32_t)__popc(peers));
       old = __shfl_sync(kAllLanes, old, leader);
-      rank[r] = valid ? old + __popc(peers & lt) : 0xffffffffu;
+      rank[r] = valid ? (old + __popc(peers & lt)) | (d << 16) : 0xffffffffu;
       __syncwarp();
     }
     __syncthreads();
@@ -243,10 +245,7 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter(const K* __restrict__ i
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kRsPerWarp / 32; r++) {
-      if (rank[r] != 0xffffffffu) {
-        const uint32_t d = (uint32_t)(key[r] >> shift) & mask;
-        buf[cur][wofs[wid][d] + rank[r]] = key[r];
-      }
+      if (rank[r] != 0xffffffffu) buf[cur][wofs[wid][rank[r] >> 16] + (rank[r] & 0xffffu)] = key[r];
     }
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < cnt; j += kRsThreads) {
