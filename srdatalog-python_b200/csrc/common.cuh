@@ -259,4 +259,23 @@ __device__ __forceinline__ uint64_t warp_partition_point(uint64_t lo, uint64_t h
 
 inline int div_up(uint64_t a, uint64_t b) { return (int)((a + b - 1) / b); }
 
+// Device-resident sizes (the device loop): a kernel given a capacity `cap`
+// and a count d_n on the device works on min(cap, *d_n) items; without d_n,
+// on cap.  Grids are sized for the capacity on the host.
+__device__ __forceinline__ uint64_t dev_size(uint64_t cap, const uint64_t* d_n) {
+  if (!d_n) return cap;
+  const uint64_t n = *d_n;
+  return n < cap ? n : cap;
+}
+
+// Items per block when `gridDim.x` blocks share n items in whole tiles: the
+// host's value, or, when it passes 0 (n known on the device only), the same
+// even split derived on the device.
+__device__ __forceinline__ uint64_t dev_chunk(uint64_t chunk, uint64_t n, uint64_t tile) {
+  if (chunk) return chunk;
+  const uint64_t tiles = (n + tile - 1) / tile;
+  const uint64_t per = (tiles + gridDim.x - 1) / gridDim.x;
+  return (per ? per : 1) * tile;
+}
+
 }  // namespace srdl

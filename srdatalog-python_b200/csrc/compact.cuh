@@ -53,10 +53,15 @@ inline size_t cp_scratch_bytes(uint64_t n) {
          2 * ((tiles * 8 + 255) & ~uint64_t(255)) + 2 * ((mtiles * 8 + 255) & ~uint64_t(255)) + 256;
 }
 
+// With d_n (device loop), n is a capacity and the count is *d_n; chunk 0
+// then means the even split of the true count over the grid.
 template <class Sel>
 __global__ void __launch_bounds__(kCpThreads) cp_flag_kernel(Sel sel, uint64_t n, uint64_t chunk,
-                                                             uint32_t* flags, uint32_t* blk_counts) {
+                                                             uint32_t* flags, uint32_t* blk_counts,
+                                                             const uint64_t* d_n) {
   __shared__ uint32_t sh[kCpThreads / 32 + 1];
+  n = dev_size(n, d_n);
+  chunk = dev_chunk(chunk, n, kCpTile);
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = begin + chunk < n ? begin + chunk : n;
   const int lane = threadIdx.x & 31;
@@ -82,8 +87,11 @@ __global__ void cp_scan_kernel(const uint32_t* blk_counts, int nb, uint64_t* off
 template <class Sel>
 __global__ void __launch_bounds__(kCpThreads) cp_write_kernel(Sel sel, uint64_t n, uint64_t chunk,
                                                               const uint32_t* __restrict__ flags,
-                                                              const uint64_t* offs) {
+                                                              const uint64_t* offs,
+                                                              const uint64_t* d_n) {
   __shared__ uint32_t wtot[2][kCpWarps];
+  n = dev_size(n, d_n);
+  chunk = dev_chunk(chunk, n, kCpTile);
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = begin + chunk < n ? begin + chunk : n;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -124,21 +132,24 @@ __global__ void __launch_bounds__(kCpThreads) cp_write_kernel(Sel sel, uint64_t 
   }
 }
 
-// Runs the three launches; the selected count lands in *d_total.
+// Runs the three launches; the selected count lands in *d_total.  With d_n,
+// n is a capacity and the element count is *d_n (device loop).
 template <class Sel>
-void compact(const Launch& L, Sel sel, uint64_t n, uint64_t* d_total, Scratch& s) {
+void compact(const Launch& L, Sel sel, uint64_t n, uint64_t* d_total, Scratch& s,
+             const uint64_t* d_n = nullptr) {
   if (n == 0) {
     SRDL_CUDA(cudaMemsetAsync(d_total, 0, sizeof(uint64_t), L.stream));
     return;
   }
   const uint64_t chunk = cp_chunk(n, L.num_sms);
   const int nb = cp_blocks(n, chunk);
+  const uint64_t kchunk = d_n ? 0 : chunk;
   uint32_t* flags = s.take<uint32_t>(cp_words(n));
   uint32_t* counts = s.take<uint32_t>(nb);
   uint64_t* offs = s.take<uint64_t>(nb + 1);
-  cp_flag_kernel<Sel><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, counts);
+  cp_flag_kernel<Sel><<<nb, kCpThreads, 0, L.stream>>>(sel, n, kchunk, flags, counts, d_n);
   cp_scan_kernel<<<1, 1024, 0, L.stream>>>(counts, nb, offs, d_total);
-  cp_write_kernel<Sel><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, offs);
+  cp_write_kernel<Sel><<<nb, kCpThreads, 0, L.stream>>>(sel, n, kchunk, flags, offs, d_n);
   SRDL_CUDA(cudaGetLastError());
   count_launches(3);
 }
@@ -157,6 +168,7 @@ struct DedupDiffSel {
   uint64_t* out;
   const uint64_t* head = nullptr;
   uint64_t n_head = 0;
+  const uint64_t* d_n_full = nullptr;  // device loop: FULL's count on the device (n_full = capacity)
 
   __device__ __forceinline__ uint64_t expand(K c) const {
     if (sizeof(K) == 8 && bits == 32) return (uint64_t)c;
@@ -200,11 +212,15 @@ struct DedupDiffSel {
 // hpos (when a HEAD is given) holds the same positions in HEAD.
 template <typename K>
 __global__ void dd_bounds_kernel(DedupDiffSel<K> sel, uint64_t n, uint64_t tiles,
-                                 uint64_t* __restrict__ fpos, uint64_t* __restrict__ hpos) {
+                                 uint64_t* __restrict__ fpos, uint64_t* __restrict__ hpos,
+                                 const uint64_t* d_n) {
   const uint64_t t = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / 32;
   if (t > tiles) return;
+  sel.n_full = dev_size(sel.n_full, sel.d_n_full);
+  n = dev_size(n, d_n);
+  const uint64_t real = (n + kCpTile - 1) / kCpTile;  // tiles holding keys
   uint64_t p = sel.n_full, q = sel.n_head;
-  if (t < tiles) {
+  if (t < real) {
     const uint64_t first = sel.expand(sel.a[t * kCpTile]);
     p = warp_partition_point(0, sel.n_full, [&](uint64_t i) { return sel.full[i] < first; });
     if (hpos)
@@ -234,10 +250,14 @@ __global__ void __launch_bounds__(kCpThreads) dd_flag_kernel(DedupDiffSel<K> sel
                                                              const uint64_t* __restrict__ fpos,
                                                              const uint64_t* __restrict__ hpos,
                                                              uint32_t* flags,
-                                                             uint32_t* blk_counts) {
+                                                             uint32_t* blk_counts,
+                                                             const uint64_t* d_n) {
   __shared__ uint64_t stage[kDdStage];
   __shared__ K skey[kCpTile + 1];  // skey[j + 1] = tile key j, skey[0] = the key before the tile
   __shared__ uint32_t sh[kCpThreads / 32 + 1];
+  sel.n_full = dev_size(sel.n_full, sel.d_n_full);
+  n = dev_size(n, d_n);
+  chunk = dev_chunk(chunk, n, kCpTile);
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = begin + chunk < n ? begin + chunk : n;
   const int lane = threadIdx.x & 31;
@@ -560,7 +580,8 @@ void compact_diff(const Launch& L, DedupDiffSel<K> sel, uint64_t n, uint64_t* d_
     dm_mark_kernel<K><<<mgrid, kCpThreads, 0, L.stream>>>(sel, n, mtiles, split, mhpos, flags);
     cp_count_kernel<<<nb, kCpThreads, 0, L.stream>>>(flags, n, chunk, counts);
     cp_scan_kernel<<<1, 1024, 0, L.stream>>>(counts, nb, offs, d_total);
-    cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, offs);
+    cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, offs,
+                                                                       nullptr);
     SRDL_CUDA(cudaGetLastError());
     count_launches(5);
     return;
@@ -570,10 +591,47 @@ void compact_diff(const Launch& L, DedupDiffSel<K> sel, uint64_t n, uint64_t* d_
   prefer_shared(dd_flag_kernel<K>);
   const uint64_t bthreads = (tiles + 1) * 32;
   dd_bounds_kernel<K><<<(unsigned)((bthreads + 255) / 256), 256, 0, L.stream>>>(sel, n, tiles, fpos,
-                                                                                hpos);
-  dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, fpos, hpos, flags, counts);
+                                                                                hpos, nullptr);
+  dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, fpos, hpos, flags, counts,
+                                                     nullptr);
   cp_scan_kernel<<<1, 1024, 0, L.stream>>>(counts, nb, offs, d_total);
-  cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, offs);
+  cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, offs,
+                                                                     nullptr);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(4);
+}
+
+// compact_diff with the key count on the device (device loop): `cap` keys
+// of room, *d_n of them present, FULL's count at sel.d_n_full (n_full its
+// capacity).  The per-tile probe path serves every size ratio, so no host
+// decision depends on the counts; the grids are sized for the capacities
+// and each block derives its share of the true counts.
+template <typename K>
+void compact_diff_dev(const Launch& L, DedupDiffSel<K> sel, uint64_t cap, const uint64_t* d_n,
+                      uint64_t* d_total, Scratch& s) {
+  sel.head = nullptr;
+  sel.n_head = 0;
+  if (!sel.full || !sel.d_n_full) {
+    sel.full = nullptr;
+    sel.n_full = 0;
+    sel.d_n_full = nullptr;
+    compact(L, sel, cap, d_total, s, d_n);
+    return;
+  }
+  const uint64_t chunk = cp_chunk(cap, L.num_sms);
+  const int nb = cp_blocks(cap, chunk);
+  const uint64_t tiles = (cap + kCpTile - 1) / kCpTile;
+  uint32_t* flags = s.take<uint32_t>(cp_words(cap));
+  uint32_t* counts = s.take<uint32_t>(nb);
+  uint64_t* offs = s.take<uint64_t>(nb + 1);
+  uint64_t* fpos = s.take<uint64_t>(tiles + 1);
+  prefer_shared(dd_flag_kernel<K>);
+  const uint64_t bthreads = (tiles + 1) * 32;
+  dd_bounds_kernel<K><<<(unsigned)((bthreads + 255) / 256), 256, 0, L.stream>>>(sel, cap, tiles,
+                                                                                fpos, nullptr, d_n);
+  dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, cap, 0, fpos, nullptr, flags, counts, d_n);
+  cp_scan_kernel<<<1, 1024, 0, L.stream>>>(counts, nb, offs, d_total);
+  cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, cap, 0, flags, offs, d_n);
   SRDL_CUDA(cudaGetLastError());
   count_launches(4);
 }

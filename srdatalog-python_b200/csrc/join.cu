@@ -274,6 +274,42 @@ __device__ __forceinline__ uint64_t emit_key(const LevelSpec& lv, const uint32_t
 
 enum ExpandMode : int { kModeCount = 0, kModeKeys = 1, kModeTableCount = 2, kModeTableWrite = 3 };
 
+// Device loop: the true candidate count (clamped to the capacity `total`;
+// a larger count raises the overflow flag once, from the first thread).
+__device__ __forceinline__ uint64_t dev_total(const JoinDev& jd, uint64_t total) {
+  if (!jd.d_total) return total;
+  const uint64_t t = *jd.d_total;
+  if (t > total) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && jd.d_overflow) atomicExch(jd.d_overflow, 1u);
+    return total;
+  }
+  return t;
+}
+
+// A warp's share of the candidates when the count is only known on the
+// device: whole rounds of 32, spread evenly over the grid's warps.
+__device__ __forceinline__ uint64_t dev_warp_chunk(const JoinDev& jd, uint64_t chunk, uint64_t total) {
+  if (!jd.d_total) return chunk;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32);
+  return (((total + warps - 1) / warps) + 31) & ~uint64_t(31);
+}
+
+// Warp-aggregated append of the m-set lanes' keys at *d_out_n; with an
+// output capacity, positions past it are dropped and raise the flag.
+__device__ __forceinline__ void append_key(const JoinDev& jd, unsigned m, bool ok, int lane,
+                                           unsigned long long* d_out_n, uint64_t* out_keys,
+                                           uint64_t key) {
+  if (!m) return;
+  const int leader = __ffs(m) - 1;
+  unsigned long long pos0 = 0;
+  if (lane == leader) pos0 = atomicAdd(d_out_n, (unsigned long long)__popc(m));
+  pos0 = __shfl_sync(kAllLanes, pos0, leader);
+  const uint64_t pos = pos0 + __popc(m & lanemask_lt());
+  if (jd.out_cap && pos0 + __popc(m) > jd.out_cap && lane == leader && jd.d_overflow)
+    atomicExch(jd.d_overflow, 1u);
+  if (ok && (!jd.out_cap || pos < jd.out_cap)) out_keys[pos] = key;
+}
+
 // in.col[k][r] with a compile-time slot index, so the Table parameter is
 // never copied to local memory for a runtime subscript.
 __device__ __forceinline__ uint32_t slot_value(const Table& t, int k, uint64_t r) {
@@ -356,8 +392,9 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
     const uint32_t* __restrict__ beg, const uint2* __restrict__ orange,
     const uint32_t* __restrict__ obm, uint64_t total, uint64_t chunk,
     unsigned long long* __restrict__ queue, Table out, uint64_t* __restrict__ out_keys,
-    unsigned long long* __restrict__ d_out_n, uint64_t* __restrict__ chunk_counts) {
+    unsigned long long* __restrict__ d_out_n, uint64_t* __restrict__ chunk_counts, JoinDev jd) {
   const int lane = threadIdx.x & 31;
+  total = dev_total(jd, total);
   const uint32_t* vals0 = lv.src[0].prefix_slot < 0 ? lv.src[0].t.roots : lv.src[0].t.lo;
   const uint32_t* vals1 = lv.src[1].prefix_slot < 0 ? lv.src[1].t.roots : lv.src[1].t.lo;
   // a roots-list side with a dense directory answers membership in O(1)
@@ -464,21 +501,17 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
       if (MODE == kModeCount || MODE == kModeTableCount) {
         running += __popc(m);
       } else if (MODE == kModeKeys) {
-        if (m) {
-          const int leader = __ffs(m) - 1;
-          unsigned long long pos0 = 0;
-          if (lane == leader) pos0 = atomicAdd(d_out_n, (unsigned long long)__popc(m));
-          pos0 = __shfl_sync(kAllLanes, pos0, leader);
-          if (ok) {
-            uint32_t kc[4];
+        uint64_t key = 0;
+        if (ok) {
+          uint32_t kc[4];
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-              const int ks = lv.key_slot[i];
-              kc[i] = i < lv.key_arity ? (ks < lv.n_in_slots ? slot_value(in, ks, r) : v) : 0u;
-            }
-            out_keys[pos0 + __popc(m & lanemask_lt())] = emit_key(lv, kc);
+          for (int i = 0; i < 4; i++) {
+            const int ks = lv.key_slot[i];
+            kc[i] = i < lv.key_arity ? (ks < lv.n_in_slots ? slot_value(in, ks, r) : v) : 0u;
           }
+          key = emit_key(lv, kc);
         }
+        append_key(jd, m, ok, lane, d_out_n, out_keys, key);
       } else {
         if (ok) {
           const uint64_t pos = running + __popc(m & lanemask_lt());
@@ -502,8 +535,10 @@ __global__ void __launch_bounds__(kJThreads) join_expand_kernel(
     LevelSpec lv, Table in, const uint64_t* __restrict__ offs, const uint8_t* __restrict__ drv,
     const uint32_t* __restrict__ beg, uint64_t total, uint64_t chunk, Table out,
     uint64_t* __restrict__ out_keys, unsigned long long* __restrict__ d_out_n,
-    uint64_t* __restrict__ warp_counts) {
+    uint64_t* __restrict__ warp_counts, JoinDev jd) {
   const int lane = threadIdx.x & 31;
+  total = dev_total(jd, total);
+  chunk = dev_warp_chunk(jd, chunk, total);
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t c0 = gw * chunk;
   const uint64_t c1 = c0 + chunk < total ? c0 + chunk : total;
@@ -581,18 +616,14 @@ __global__ void __launch_bounds__(kJThreads) join_expand_kernel(
       if (MODE == kModeCount || MODE == kModeTableCount) {
         running += __popc(m);
       } else if (MODE == kModeKeys) {
-        if (m) {
-          const int leader = __ffs(m) - 1;
-          unsigned long long pos0 = 0;
-          if (lane == leader) pos0 = atomicAdd(d_out_n, (unsigned long long)__popc(m));
-          pos0 = __shfl_sync(kAllLanes, pos0, leader);
-          if (ok) {
-            uint32_t kc[4];
+        uint64_t key = 0;
+        if (ok) {
+          uint32_t kc[4];
 #pragma unroll
-            for (int i = 0; i < 4; i++) kc[i] = i < lv.key_arity ? val(lv.key_slot[i]) : 0u;
-            out_keys[pos0 + __popc(m & lanemask_lt())] = emit_key(lv, kc);
-          }
+          for (int i = 0; i < 4; i++) kc[i] = i < lv.key_arity ? val(lv.key_slot[i]) : 0u;
+          key = emit_key(lv, kc);
         }
+        append_key(jd, m, ok, lane, d_out_n, out_keys, key);
       } else {  // ordered table write
         if (ok) {
           const uint64_t pos = running + __popc(m & lanemask_lt());
@@ -619,8 +650,13 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
     LevelSpec lv, Table in, const uint64_t* __restrict__ offs, const uint32_t* __restrict__ beg,
     const uint2* __restrict__ orange, uint64_t total, uint64_t chunk, Table out,
     uint64_t* __restrict__ out_keys, unsigned long long* __restrict__ d_out_n,
-    uint64_t* __restrict__ warp_counts) {
+    uint64_t* __restrict__ warp_counts, JoinDev jd) {
   const int lane = threadIdx.x & 31;
+  total = dev_total(jd, total);
+  chunk = dev_warp_chunk(jd, chunk, total);
+  // every candidate a result (no filter) and the output private to this
+  // launch: each is written at its own index
+  const bool exact = MODE == kModeKeys && lv.nfilt == 0 && !jd.d_total;
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t c0 = gw * chunk;
   const uint64_t c1 = c0 + chunk < total ? c0 + chunk : total;
@@ -629,8 +665,7 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
   const int s0 = lv.src[0].out_slot, s1 = lv.src[1].out_slot;
   unsigned long long running = 0;
   if (MODE == kModeTableWrite) running = warp_counts[gw];
-  // without filters every candidate is written at its own index
-  if (MODE == kModeKeys && lv.nfilt == 0 && gw == 0 && lane == 0) *d_out_n = total;
+  if (exact && gw == 0 && lane == 0) *d_out_n = total;
   if (c0 < c1) {
     SegWalk<SEG> sw(lv, c0);
     uint64_t r0 = gallop_row(offs, 0, in.n, sw.at());
@@ -655,7 +690,7 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
         v1 = vals1[rg.x + i1];
         if (lv.nfilt) ok = level_filters(lv, in, r, s0, v0, s1, v1);
       }
-      if (MODE == kModeKeys && lv.nfilt == 0) {
+      if (exact) {
         // every candidate is a result: candidate index = output position
         if (ok) {
           uint32_t kc[4];
@@ -673,21 +708,17 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
       if (MODE == kModeCount || MODE == kModeTableCount) {
         running += __popc(m);
       } else if (MODE == kModeKeys) {
-        if (m) {
-          const int leader = __ffs(m) - 1;
-          unsigned long long pos0 = 0;
-          if (lane == leader) pos0 = atomicAdd(d_out_n, (unsigned long long)__popc(m));
-          pos0 = __shfl_sync(kAllLanes, pos0, leader);
-          if (ok) {
-            uint32_t kc[4];
+        uint64_t key = 0;
+        if (ok) {
+          uint32_t kc[4];
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-              const int ks = lv.key_slot[i];
-              kc[i] = i >= lv.key_arity ? 0u : ks == s0 ? v0 : ks == s1 ? v1 : slot_value(in, ks, r);
-            }
-            out_keys[pos0 + __popc(m & lanemask_lt())] = emit_key(lv, kc);
+          for (int i = 0; i < 4; i++) {
+            const int ks = lv.key_slot[i];
+            kc[i] = i >= lv.key_arity ? 0u : ks == s0 ? v0 : ks == s1 ? v1 : slot_value(in, ks, r);
           }
+          key = emit_key(lv, kc);
         }
+        append_key(jd, m, ok, lane, d_out_n, out_keys, key);
       } else {
         if (ok) {
           const uint64_t pos = running + __popc(m & lanemask_lt());
@@ -780,8 +811,9 @@ JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scrat
 
 void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const JoinWork& w,
                  uint64_t total, Table* out_table, uint64_t* out_keys, uint64_t* d_out_n,
-                 Scratch& s) {
+                 Scratch& s, const JoinDev* dev) {
   if (total == 0) return;
+  const JoinDev jd = dev ? *dev : JoinDev{};
   auto* cnt = reinterpret_cast<unsigned long long*>(d_out_n);
   const int g = jgrid(total, L);
   const uint64_t warps = (uint64_t)g * (kJThreads / 32);
@@ -809,10 +841,10 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
 #define SRDL_CJ2(MODE, Q, CC)                                                                     \
   (lv.seg ? join_cj2_kernel<MODE, true><<<gq, kJThreads, 0, L.stream>>>(                           \
                 lv, in, w.offs, w.drv, w.beg, w.orange, w.obm, total, chunk, Q, out, out_keys, cnt, \
-                CC)                                                                               \
+                CC, jd)                                                                           \
           : join_cj2_kernel<MODE, false><<<gq, kJThreads, 0, L.stream>>>(                          \
                 lv, in, w.offs, w.drv, w.beg, w.orange, w.obm, total, chunk, Q, out, out_keys, cnt, \
-                CC))
+                CC, jd))
     if (lv.emit == kEmitCount) {
       SRDL_CJ2(kModeCount, q, nullptr);
       count_launches(1);
@@ -822,6 +854,9 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
     } else {
       uint64_t* cc = s.take<uint64_t>(nchunks + 1);
       uint64_t* co = s.take<uint64_t>(nchunks + 1);
+      // with the count on the device, chunks past it are never taken: zero
+      // their counts so the scan over the capacity's chunks stays exact
+      if (jd.d_total) SRDL_CUDA(cudaMemsetAsync(cc, 0, (nchunks + 1) * 8, L.stream));
       SRDL_CJ2(kModeTableCount, q, cc);
       SRDL_CUDA(cudaGetLastError());
       exclusive_scan_u64(L, cc, nchunks, co, s);
@@ -837,9 +872,9 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
       !lv.wide) {
 #define SRDL_CART2(MODE, WC)                                                                 \
   (lv.seg ? join_cart2_kernel<MODE, true><<<g, kJThreads, 0, L.stream>>>(                     \
-                lv, in, w.offs, w.beg, w.orange, total, chunk, out, out_keys, cnt, WC)          \
+                lv, in, w.offs, w.beg, w.orange, total, chunk, out, out_keys, cnt, WC, jd)      \
           : join_cart2_kernel<MODE, false><<<g, kJThreads, 0, L.stream>>>(                    \
-                lv, in, w.offs, w.beg, w.orange, total, chunk, out, out_keys, cnt, WC))
+                lv, in, w.offs, w.beg, w.orange, total, chunk, out, out_keys, cnt, WC, jd))
     if (lv.emit == kEmitCount) {
       SRDL_CART2(kModeCount, nullptr);
       count_launches(1);
@@ -862,9 +897,9 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
   }
 #define SRDL_EXP(MODE, WC)                                                                    \
   (lv.seg ? join_expand_kernel<MODE, true><<<g, kJThreads, 0, L.stream>>>(                       \
-                lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, WC)              \
+                lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, WC, jd)          \
           : join_expand_kernel<MODE, false><<<g, kJThreads, 0, L.stream>>>(                      \
-                lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, WC))
+                lv, in, w.offs, w.drv, w.beg, total, chunk, out, out_keys, cnt, WC, jd))
   if (lv.emit == kEmitCount) {
     SRDL_EXP(kModeCount, nullptr);
     count_launches(1);

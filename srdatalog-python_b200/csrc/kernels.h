@@ -83,12 +83,29 @@ void set_difference(const Launch& L, const uint64_t* a, uint64_t na, const uint6
 void merge_disjoint(const Launch& L, const uint64_t* a, uint64_t na, const uint64_t* b,
                     uint64_t nb, uint64_t* out);
 
-// Trie view pieces for a sorted unique key array.
+// Device loop: out = a U b with the counts on the device (*d_na, *d_nb; na_cap
+// and nb_cap are capacities); *d_nout = the merged count; a merged count
+// above out_cap sets *d_overflow and writes nothing.
+void merge_disjoint_dev(const Launch& L, const uint64_t* a, uint64_t na_cap, const uint64_t* d_na,
+                        const uint64_t* b, uint64_t nb_cap, const uint64_t* d_nb, uint64_t* out,
+                        uint64_t out_cap, uint64_t* d_nout, unsigned int* d_overflow);
+
+// sort_dedup with the input count on the device (device loop): `cap` keys of
+// room in `in`, *d_n present; FULL (room full_cap, count *d_n_full, may be
+// null) is subtracted.  No host decision depends on the counts.
+void sort_dedup_dev(const Launch& L, const uint64_t* in, uint64_t cap, const uint64_t* d_n,
+                    int bits, const uint64_t* full, uint64_t full_cap, const uint64_t* d_n_full,
+                    uint64_t* out, uint64_t* d_nout, Scratch& s);
+
+// Trie view pieces for a sorted unique key array (with d_n: n is a capacity
+// and the count is on the device).
 size_t roots_scratch_bytes(uint64_t n);
-void build_lo(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* lo);
-void build_dir(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* dir, uint32_t dir_n);
+void build_lo(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* lo,
+              const uint64_t* d_n = nullptr);
+void build_dir(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* dir, uint32_t dir_n,
+               const uint64_t* d_n = nullptr);
 void build_roots(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* roots,
-                 uint64_t* d_nroots, Scratch& s);
+                 uint64_t* d_nroots, Scratch& s, const uint64_t* d_n = nullptr);
 
 // Hash tables for the child lists longer than `min_len` of a dense-directory
 // trie.  Plan: sizes[v] = slots for value v (0 = no table), offs = exclusive
@@ -242,9 +259,21 @@ JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scrat
 // capacity = total.  The scratch for a level of `total` candidates comes
 // from join_expand_scratch_bytes(L, total).
 size_t join_expand_scratch_bytes(const Launch& L, uint64_t total);
+
+// Device loop: the candidate count is on the device (d_total, the count
+// pass's offs[rows]); `total` is then its capacity.  A count above the
+// capacity, or emitted keys beyond out_cap (emit keys: appended after the
+// keys already at *d_out_n), set *d_overflow; nothing is written out of
+// bounds.
+struct JoinDev {
+  const uint64_t* d_total = nullptr;
+  uint64_t out_cap = 0;
+  unsigned int* d_overflow = nullptr;
+};
+
 void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const JoinWork& w,
                  uint64_t total, Table* out_table, uint64_t* out_keys, uint64_t* d_out_n,
-                 Scratch& s);
+                 Scratch& s, const JoinDev* dev = nullptr);
 
 // Work items of shard `rank` among `world` when `total` items are dealt out
 // in segments of `seg` (segment i goes to shard i mod world).

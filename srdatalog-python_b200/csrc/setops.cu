@@ -13,6 +13,7 @@
 // (.ipp:1104-1107) and the binary-probe variant (.ipp:933-1041): every
 // element of `a` is probed in the slice of `b` that its block's key range
 // can reach, then the survivors are compacted in order.
+#include <algorithm>
 #include <atomic>
 
 #include "compact.cuh"
@@ -48,12 +49,35 @@ __device__ __forceinline__ uint64_t merge_path(const uint64_t* a, uint64_t na, c
 // split is na and is not stored).  Only tile t's block reads or writes tile
 // t's slots, and it reads them before writing its outputs, so no scratch
 // buffer is needed.
+// Device loop: na / nb are capacities and the counts are *d_na / *d_nb;
+// tiles past the merged count do nothing (the last real tile ends at na).
+// A merged count above out_cap raises *d_overflow and merges nothing.
+struct MergeDev {
+  const uint64_t* d_na = nullptr;
+  const uint64_t* d_nb = nullptr;
+  uint64_t out_cap = 0;
+  uint64_t* d_nout = nullptr;        // receives na + nb
+  unsigned int* d_overflow = nullptr;
+};
+
+__device__ __forceinline__ bool merge_dev_sizes(const MergeDev& md, uint64_t& na, uint64_t& nb) {
+  na = dev_size(na, md.d_na);
+  nb = dev_size(nb, md.d_nb);
+  return !(md.out_cap && na + nb > md.out_cap);
+}
+
 __global__ void merge_split_kernel(const uint64_t* __restrict__ a, uint64_t na,
                                    const uint64_t* __restrict__ b, uint64_t nb, uint64_t tiles,
-                                   uint64_t* __restrict__ out) {
+                                   uint64_t* __restrict__ out, MergeDev md) {
   const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (t >= tiles) return;
+  if (!merge_dev_sizes(md, na, nb)) {
+    if (t == 0 && md.d_overflow) atomicExch(md.d_overflow, 1u);
+    return;
+  }
+  if (t == 0 && md.d_nout) *md.d_nout = na + nb;
   const uint64_t diag = t * kMgTile;
+  if (diag >= na + nb) return;
   const uint64_t s = merge_path(a, na, b, nb, diag);
   out[diag] = s;
   if (t > 0) out[diag - kMgTile + 1] = s;
@@ -68,14 +92,16 @@ __global__ void __launch_bounds__(kMgThreads) merge_kernel(const uint64_t* __res
                                                            uint64_t na,
                                                            const uint64_t* __restrict__ b,
                                                            uint64_t nb,
-                                                           uint64_t* __restrict__ out) {
+                                                           uint64_t* __restrict__ out, MergeDev md) {
   __shared__ uint64_t sin[kMgPadded];
   __shared__ uint64_t sout[kMgPadded];
   __shared__ uint64_t split[2];
+  if (!merge_dev_sizes(md, na, nb)) return;
   const uint64_t total = na + nb;
   const uint64_t d0 = (uint64_t)blockIdx.x * kMgTile;
+  if (d0 >= total) return;
   const uint64_t d1 = d0 + kMgTile < total ? d0 + kMgTile : total;
-  const bool last = blockIdx.x + 1 == gridDim.x;
+  const bool last = d1 == total;
   if (threadIdx.x == 0) split[0] = out[d0];
   if (threadIdx.x == 1) split[1] = last ? na : out[d0 + 1];
   __syncthreads();
@@ -121,8 +147,22 @@ void merge_disjoint(const Launch& L, const uint64_t* a, uint64_t na, const uint6
   SRDL_REQUIRE(blocks < (1ull << 31), kErrCapacity, "merge: too many rows");
   prefer_shared(merge_kernel);
   merge_split_kernel<<<(unsigned)((blocks + 255) / 256), 256, 0, L.stream>>>(a, na, b, nb, blocks,
-                                                                             out);
-  merge_kernel<<<(unsigned)blocks, kMgThreads, 0, L.stream>>>(a, na, b, nb, out);
+                                                                             out, MergeDev{});
+  merge_kernel<<<(unsigned)blocks, kMgThreads, 0, L.stream>>>(a, na, b, nb, out, MergeDev{});
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(2);
+}
+
+void merge_disjoint_dev(const Launch& L, const uint64_t* a, uint64_t na_cap, const uint64_t* d_na,
+                        const uint64_t* b, uint64_t nb_cap, const uint64_t* d_nb, uint64_t* out,
+                        uint64_t out_cap, uint64_t* d_nout, unsigned int* d_overflow) {
+  const uint64_t blocks = std::max<uint64_t>(1, (na_cap + nb_cap + kMgTile - 1) / kMgTile);
+  SRDL_REQUIRE(blocks < (1ull << 31), kErrCapacity, "merge: too many rows");
+  MergeDev md{d_na, d_nb, out_cap, d_nout, d_overflow};
+  prefer_shared(merge_kernel);
+  merge_split_kernel<<<(unsigned)((blocks + 255) / 256), 256, 0, L.stream>>>(a, na_cap, b, nb_cap,
+                                                                             blocks, out, md);
+  merge_kernel<<<(unsigned)blocks, kMgThreads, 0, L.stream>>>(a, na_cap, b, nb_cap, out, md);
   SRDL_CUDA(cudaGetLastError());
   count_launches(2);
 }
@@ -135,14 +175,17 @@ void set_difference(const Launch& L, const uint64_t* a, uint64_t na, const uint6
   compact_diff(L, sel, na, d_nout, s);
 }
 
-__global__ void lo_kernel(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ lo) {
+__global__ void lo_kernel(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ lo,
+                          const uint64_t* d_n) {
+  n = dev_size(n, d_n);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x)
     lo[i] = (uint32_t)keys[i];
 }
 
 __global__ void dir_kernel(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ dir,
-                           uint32_t dir_n) {
+                           uint32_t dir_n, const uint64_t* d_n) {
+  n = dev_size(n, d_n);
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < dir_n;
        v += (uint64_t)gridDim.x * blockDim.x)
     dir[v] = (uint32_t)lower_bound_u64(keys, 0, n, v << 32);
@@ -163,16 +206,17 @@ static int grid_for(uint64_t n, int sms) {
   return g ? (int)g : 1;
 }
 
-void build_lo(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* lo) {
+void build_lo(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* lo, const uint64_t* d_n) {
   if (!n) return;
-  lo_kernel<<<grid_for(n, L.num_sms), 256, 0, L.stream>>>(keys, n, lo);
+  lo_kernel<<<grid_for(n, L.num_sms), 256, 0, L.stream>>>(keys, n, lo, d_n);
   SRDL_CUDA(cudaGetLastError());
   count_launches(1);
 }
 
-void build_dir(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* dir, uint32_t dir_n) {
+void build_dir(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* dir, uint32_t dir_n,
+               const uint64_t* d_n) {
   if (!dir_n) return;
-  dir_kernel<<<grid_for(dir_n, L.num_sms), 256, 0, L.stream>>>(keys, n, dir, dir_n);
+  dir_kernel<<<grid_for(dir_n, L.num_sms), 256, 0, L.stream>>>(keys, n, dir, dir_n, d_n);
   SRDL_CUDA(cudaGetLastError());
   count_launches(1);
 }
@@ -180,9 +224,9 @@ void build_dir(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* dir,
 size_t roots_scratch_bytes(uint64_t n) { return cp_scratch_bytes(n); }
 
 void build_roots(const Launch& L, const uint64_t* keys, uint64_t n, uint32_t* roots,
-                 uint64_t* d_nroots, Scratch& s) {
+                 uint64_t* d_nroots, Scratch& s, const uint64_t* d_n) {
   RootSel sel{keys, roots};
-  compact(L, sel, n, d_nroots, s);
+  compact(L, sel, n, d_nroots, s, d_n);
 }
 
 void swap_halves(const Launch& L, const uint64_t* in, uint64_t n, uint64_t* out) {

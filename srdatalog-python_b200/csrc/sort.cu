@@ -57,7 +57,8 @@ __global__ void cp_scan_kernel(const uint32_t* blk_counts, int nb, uint64_t* off
 
 template <typename K>
 __global__ void rs_pack(const uint64_t* __restrict__ in, uint64_t n, int bits, bool swap,
-                        K* __restrict__ out) {
+                        K* __restrict__ out, const uint64_t* d_n) {
+  n = dev_size(n, d_n);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     uint64_t k = in[i];
@@ -74,8 +75,11 @@ __global__ void rs_pack(const uint64_t* __restrict__ in, uint64_t n, int bits, b
 template <typename K>
 __global__ void __launch_bounds__(kRsThreads) rs_hist(const K* __restrict__ keys, uint64_t n,
                                                       uint64_t chunk, int shift, int nbins,
-                                                      uint32_t* __restrict__ counts) {
+                                                      uint32_t* __restrict__ counts,
+                                                      const uint64_t* d_n) {
   __shared__ uint32_t h[kRsBins];
+  n = dev_size(n, d_n);
+  chunk = dev_chunk(chunk, n, kRsTile);
   for (int d = threadIdx.x; d < nbins; d += kRsThreads) h[d] = 0;
   __syncthreads();
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
@@ -158,7 +162,8 @@ __global__ void __launch_bounds__(kRsThreads, 5) rs_scatter(const K* __restrict_
                                                          K* __restrict__ out, uint64_t n,
                                                          uint64_t chunk, int shift,
                                                          const uint32_t* __restrict__ offs,
-                                                         const uint32_t* __restrict__ digit_tot) {
+                                                         const uint32_t* __restrict__ digit_tot,
+                                                         const uint64_t* d_n) {
   constexpr int nbins = 1 << DB;
   constexpr uint32_t mask = nbins - 1;
   __shared__ uint32_t base[kRsBins];             // next global output position per digit
@@ -168,6 +173,8 @@ __global__ void __launch_bounds__(kRsThreads, 5) rs_scatter(const K* __restrict_
   __shared__ __align__(16) K buf[2][kRsTile];
 
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  n = dev_size(n, d_n);
+  chunk = dev_chunk(chunk, n, kRsTile);
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = begin + chunk < n ? begin + chunk : n;
   if (begin < end) rs_prefetch(buf[0], in, begin, end);
@@ -259,12 +266,12 @@ __global__ void __launch_bounds__(kRsThreads, 5) rs_scatter(const K* __restrict_
 template <typename K>
 static void launch_scatter(const Launch& L, int nb, int w, const K* in, K* out, uint64_t n,
                            uint64_t chunk, int shift, const uint32_t* offs,
-                           const uint32_t* digit_tot) {
+                           const uint32_t* digit_tot, const uint64_t* d_n) {
 #define SRDL_SCATTER_CASE(DB)                                                          \
   case DB:                                                                             \
     prefer_shared(rs_scatter<K, DB>);                                                  \
     rs_scatter<K, DB><<<nb, kRsThreads, 0, L.stream>>>(in, out, n, chunk, shift, offs, \
-                                                       digit_tot);                     \
+                                                       digit_tot, d_n);                \
     break;
   switch (w) {
     SRDL_SCATTER_CASE(1)
@@ -292,21 +299,24 @@ size_t sort_scratch_bytes(uint64_t n, int bits) {
 template <typename K>
 static void sort_dedup_t(const Launch& L, const uint64_t* in, uint64_t n, int bits, bool swap,
                          const uint64_t* full, uint64_t n_full, uint64_t* out,
-                         uint64_t* d_nout, Scratch& s, const uint64_t* head, uint64_t n_head) {
+                         uint64_t* d_nout, Scratch& s, const uint64_t* head, uint64_t n_head,
+                         const uint64_t* d_n, const uint64_t* d_n_full) {
   SRDL_REQUIRE(n < (1ull << 32), kErrCapacity, "sort: more than 2^32-1 rows in one index");
   K* a = s.take<K>(n);
   K* b = s.take<K>(n);
   const int pgrid = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)L.num_sms * 16);
-  rs_pack<K><<<pgrid ? pgrid : 1, 256, 0, L.stream>>>(in, n, bits, swap, a);
+  rs_pack<K><<<pgrid ? pgrid : 1, 256, 0, L.stream>>>(in, n, bits, swap, a, d_n);
   SRDL_CUDA(cudaGetLastError());
   count_launches(1);
 
-  // Tile partition shared by the histogram and scatter launches.
+  // Tile partition shared by the histogram and scatter launches (with the
+  // count on the device, the blocks derive the same even split from it).
   const uint64_t tiles = (n + kRsTile - 1) / kRsTile;
   const uint64_t cap = (uint64_t)L.num_sms * 8;
   const uint64_t per = (tiles + cap - 1) / cap;
   const uint64_t chunk = (per ? per : 1) * kRsTile;
   const int nb = (int)((n + chunk - 1) / chunk);
+  const uint64_t kchunk = d_n ? 0 : chunk;
   uint32_t* counts = s.take<uint32_t>((size_t)kRsBins * nb);
   uint32_t* digit_tot = s.take<uint32_t>(kRsBins);
 
@@ -314,19 +324,21 @@ static void sort_dedup_t(const Launch& L, const uint64_t* in, uint64_t n, int bi
   const int maxw = L.radix_bits >= 1 && L.radix_bits <= 8 ? L.radix_bits : 8;
   const int passes = (total_bits + maxw - 1) / maxw;
   int shift = 0;
-  for (int p = 0; p < passes && n > 1; p++) {
+  for (int p = 0; p < passes && (n > 1 || d_n); p++) {
     const int w = total_bits / passes + (p < total_bits % passes ? 1 : 0);
     const int nbins = 1 << w;
-    rs_hist<K><<<nb, kRsThreads, 0, L.stream>>>(a, n, chunk, shift, nbins, counts);
+    rs_hist<K><<<nb, kRsThreads, 0, L.stream>>>(a, n, kchunk, shift, nbins, counts, d_n);
     rs_rowscan<<<nbins, kRsThreads, 0, L.stream>>>(counts, nb, digit_tot);
-    launch_scatter<K>(L, nb, w, a, b, n, chunk, shift, counts, digit_tot);
+    launch_scatter<K>(L, nb, w, a, b, n, kchunk, shift, counts, digit_tot, d_n);
     SRDL_CUDA(cudaGetLastError());
     count_launches(3);
     std::swap(a, b);
     shift += w;
   }
   DedupDiffSel<K> sel{a, bits, true, full, n_full, out, head, n_head};
-  compact_diff(L, sel, n, d_nout, s);
+  sel.d_n_full = d_n_full;
+  if (d_n) compact_diff_dev(L, sel, n, d_n, d_nout, s);
+  else compact_diff(L, sel, n, d_nout, s);
 }
 
 void sort_dedup(const Launch& L, const uint64_t* in, uint64_t n, int bits, bool swap,
@@ -337,8 +349,21 @@ void sort_dedup(const Launch& L, const uint64_t* in, uint64_t n, int bits, bool 
     return;
   }
   if (use32(bits))
-    sort_dedup_t<uint32_t>(L, in, n, bits, swap, full, n_full, out, d_nout, s, head, n_head);
-  else sort_dedup_t<uint64_t>(L, in, n, bits, swap, full, n_full, out, d_nout, s, head, n_head);
+    sort_dedup_t<uint32_t>(L, in, n, bits, swap, full, n_full, out, d_nout, s, head, n_head,
+                           nullptr, nullptr);
+  else sort_dedup_t<uint64_t>(L, in, n, bits, swap, full, n_full, out, d_nout, s, head, n_head,
+                              nullptr, nullptr);
+}
+
+void sort_dedup_dev(const Launch& L, const uint64_t* in, uint64_t cap, const uint64_t* d_n,
+                    int bits, const uint64_t* full, uint64_t full_cap, const uint64_t* d_n_full,
+                    uint64_t* out, uint64_t* d_nout, Scratch& s) {
+  cap = cap ? cap : 1;
+  if (use32(bits))
+    sort_dedup_t<uint32_t>(L, in, cap, bits, false, full, full_cap, out, d_nout, s, nullptr, 0, d_n,
+                           d_n_full);
+  else sort_dedup_t<uint64_t>(L, in, cap, bits, false, full, full_cap, out, d_nout, s, nullptr, 0,
+                              d_n, d_n_full);
 }
 
 }  // namespace srdl
