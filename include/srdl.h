@@ -88,6 +88,15 @@ int srdl_set_profiling(srdl_db* db, int enable);
  *                      b-bit keys runs ceil(b / radix_bits) passes
  *   "join_blocks_per_sm"  join launches use at most this many blocks per
  *                      SM, 1..64 (default 16): the candidates per warp
+ *   "device_loop"      1 (default; SRDL_DEVICE_LOOP=0 changes it) runs the
+ *                      iterations of a qualifying recursive step after the
+ *                      first as one CUDA graph that loops on the device
+ *                      until the delta is empty; 0 keeps every iteration on
+ *                      the host path.  Results are the same either way
+ *   "device_loop_cap_limit"  largest buffer capacity (rows) the device loop
+ *                      may choose, 0 = none (default); small values force
+ *                      its overflow path, which hands iterations back to the
+ *                      host path (for tests)
  *   "mem_limit_mb"     device memory a run may hold (MB, 0 = no limit,
  *                      the default): past it the run stops with status 5
  *                      (see srdl_mem_stats)

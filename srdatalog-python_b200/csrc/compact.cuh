@@ -213,11 +213,12 @@ struct DedupDiffSel {
 template <typename K>
 __global__ void dd_bounds_kernel(DedupDiffSel<K> sel, uint64_t n, uint64_t tiles,
                                  uint64_t* __restrict__ fpos, uint64_t* __restrict__ hpos,
-                                 const uint64_t* d_n) {
+                                 const uint64_t* d_n, int path) {
   const uint64_t t = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / 32;
   if (t > tiles) return;
   sel.n_full = dev_size(sel.n_full, sel.d_n_full);
   n = dev_size(n, d_n);
+  if (!diff_path_runs(path, sel, n)) return;
   const uint64_t real = (n + kCpTile - 1) / kCpTile;  // tiles holding keys
   uint64_t p = sel.n_full, q = sel.n_head;
   if (t < real) {
@@ -251,12 +252,13 @@ __global__ void __launch_bounds__(kCpThreads) dd_flag_kernel(DedupDiffSel<K> sel
                                                              const uint64_t* __restrict__ hpos,
                                                              uint32_t* flags,
                                                              uint32_t* blk_counts,
-                                                             const uint64_t* d_n) {
+                                                             const uint64_t* d_n, int path) {
   __shared__ uint64_t stage[kDdStage];
   __shared__ K skey[kCpTile + 1];  // skey[j + 1] = tile key j, skey[0] = the key before the tile
   __shared__ uint32_t sh[kCpThreads / 32 + 1];
   sel.n_full = dev_size(sel.n_full, sel.d_n_full);
   n = dev_size(n, d_n);
+  if (!diff_path_runs(path, sel, n)) return;
   chunk = dev_chunk(chunk, n, kCpTile);
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = begin + chunk < n ? begin + chunk : n;
@@ -392,10 +394,28 @@ __device__ __forceinline__ uint64_t dm_path(const DedupDiffSel<K>& sel, uint64_t
 
 // split[t] = a-keys among the first t*kCpTile merged elements; hpos[t] = the
 // HEAD position of a[split[t]] (n_head past the last key).
+// Device loop (d_n set): the merge path and the probe path are both in the
+// graph and each kernel runs only when the counts on the device select its
+// path (FULL at most kDmMaxFullRatio times the keys: merge path).
+constexpr uint64_t kDmMaxFullRatio = 16;
+enum DiffPath : int { kPathAny = 0, kPathMerge = 1, kPathProbe = 2 };
+
+template <typename K>
+__device__ __forceinline__ bool diff_path_runs(int path, const DedupDiffSel<K>& sel, uint64_t n) {
+  if (path == kPathAny) return true;
+  const bool merge = sel.n_full <= kDmMaxFullRatio * n;
+  return (path == kPathMerge) == merge;
+}
+
 template <typename K>
 __global__ void dm_split_kernel(DedupDiffSel<K> sel, uint64_t na, uint64_t tiles,
-                                uint64_t* __restrict__ split, uint64_t* __restrict__ hpos) {
+                                uint64_t* __restrict__ split, uint64_t* __restrict__ hpos,
+                                const uint64_t* d_n, int path) {
   const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  sel.n_full = dev_size(sel.n_full, sel.d_n_full);
+  na = dev_size(na, d_n);
+  if (!diff_path_runs(path, sel, na)) return;
+  if (d_n) tiles = (na + sel.n_full + kCpTile - 1) / kCpTile;
   if (t > tiles) return;
   const uint64_t total = na + sel.n_full;
   const uint64_t diag = t * kCpTile < total ? t * kCpTile : total;
@@ -429,9 +449,14 @@ __global__ void __launch_bounds__(kCpThreads) dm_mark_kernel(DedupDiffSel<K> sel
                                                              uint64_t tiles,
                                                              const uint64_t* __restrict__ split,
                                                              const uint64_t* __restrict__ hpos,
-                                                             uint32_t* __restrict__ flags) {
+                                                             uint32_t* __restrict__ flags,
+                                                             const uint64_t* d_n, int path) {
   __shared__ __align__(16) unsigned char buf[2][kCpTile * 8];
   __shared__ uint32_t sbits[kCpTile / 32 + 2];
+  sel.n_full = dev_size(sel.n_full, sel.d_n_full);
+  na = dev_size(na, d_n);
+  if (!diff_path_runs(path, sel, na)) return;
+  if (d_n) tiles = (na + sel.n_full + kCpTile - 1) / kCpTile;
   const uint64_t total = na + sel.n_full;
   auto bounds = [&](uint64_t t, uint64_t& i0, uint64_t& i1, uint64_t& j0, uint64_t& j1) {
     const uint64_t d0 = t * kCpTile;
@@ -527,10 +552,17 @@ __global__ void __launch_bounds__(kCpThreads) dm_mark_kernel(DedupDiffSel<K> sel
 }
 
 // Per-block selected counts of a flag-word array (blocks own `chunk` keys).
+template <typename K>
 static __global__ void __launch_bounds__(kCpThreads) cp_count_kernel(const uint32_t* __restrict__ flags,
                                                               uint64_t n, uint64_t chunk,
-                                                              uint32_t* blk_counts) {
+                                                              uint32_t* blk_counts,
+                                                              DedupDiffSel<K> sel,
+                                                              const uint64_t* d_n, int path) {
   __shared__ uint32_t sh[kCpThreads / 32 + 1];
+  sel.n_full = dev_size(sel.n_full, sel.d_n_full);
+  n = dev_size(n, d_n);
+  if (!diff_path_runs(path, sel, n)) return;
+  chunk = dev_chunk(chunk, n, kCpTile);
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = begin + chunk < n ? begin + chunk : n;
   uint32_t c = 0;
@@ -541,9 +573,8 @@ static __global__ void __launch_bounds__(kCpThreads) cp_count_kernel(const uint3
   if (threadIdx.x == 0) blk_counts[blockIdx.x] = tot;
 }
 
-// The merge-path pass streams all of FULL; past this ratio the per-tile
+// The merge-path pass streams all of FULL; past kDmMaxFullRatio the per-tile
 // probes of dd_flag_kernel read less.
-constexpr uint64_t kDmMaxFullRatio = 16;
 
 // compact() for DedupDiffSel with a FULL array: merge path when FULL is not
 // much larger than the keys, tiled shared-memory probes otherwise.
@@ -575,10 +606,12 @@ void compact_diff(const Launch& L, DedupDiffSel<K> sel, uint64_t n, uint64_t* d_
     uint64_t* mhpos = sel.head ? s.take<uint64_t>(mtiles + 1) : nullptr;
     SRDL_CUDA(cudaMemsetAsync(flags, 0, cp_words(n) * 4, L.stream));
     dm_split_kernel<K><<<(unsigned)((mtiles + 1 + 255) / 256), 256, 0, L.stream>>>(sel, n, mtiles,
-                                                                                  split, mhpos);
+                                                                                  split, mhpos, nullptr,
+                                                                                  kPathAny);
     const unsigned mgrid = (unsigned)std::min<uint64_t>(mtiles, (uint64_t)L.num_sms * 4);
-    dm_mark_kernel<K><<<mgrid, kCpThreads, 0, L.stream>>>(sel, n, mtiles, split, mhpos, flags);
-    cp_count_kernel<<<nb, kCpThreads, 0, L.stream>>>(flags, n, chunk, counts);
+    dm_mark_kernel<K><<<mgrid, kCpThreads, 0, L.stream>>>(sel, n, mtiles, split, mhpos, flags, nullptr,
+                                                          kPathAny);
+    cp_count_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(flags, n, chunk, counts, sel, nullptr, kPathAny);
     cp_scan_kernel<<<1, 1024, 0, L.stream>>>(counts, nb, offs, d_total);
     cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, offs,
                                                                        nullptr);
@@ -591,9 +624,9 @@ void compact_diff(const Launch& L, DedupDiffSel<K> sel, uint64_t n, uint64_t* d_
   prefer_shared(dd_flag_kernel<K>);
   const uint64_t bthreads = (tiles + 1) * 32;
   dd_bounds_kernel<K><<<(unsigned)((bthreads + 255) / 256), 256, 0, L.stream>>>(sel, n, tiles, fpos,
-                                                                                hpos, nullptr);
+                                                                                hpos, nullptr, kPathAny);
   dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, fpos, hpos, flags, counts,
-                                                     nullptr);
+                                                     nullptr, kPathAny);
   cp_scan_kernel<<<1, 1024, 0, L.stream>>>(counts, nb, offs, d_total);
   cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, n, chunk, flags, offs,
                                                                      nullptr);
@@ -603,9 +636,15 @@ void compact_diff(const Launch& L, DedupDiffSel<K> sel, uint64_t n, uint64_t* d_
 
 // compact_diff with the key count on the device (device loop): `cap` keys
 // of room, *d_n of them present, FULL's count at sel.d_n_full (n_full its
-// capacity).  The per-tile probe path serves every size ratio, so no host
-// decision depends on the counts; the grids are sized for the capacities
-// and each block derives its share of the true counts.
+// capacity).  Both the merge path and the per-tile probe path are launched;
+// each kernel runs only when the counts on the device select its path (the
+// host's rule: merge while FULL is at most kDmMaxFullRatio times the keys),
+// so no host decision depends on the counts.  Grids are sized for the
+// capacities and each block derives its share of the true counts.
+inline size_t diff_dev_extra_bytes(uint64_t cap, uint64_t full_cap) {
+  return ((cap + full_cap) / kCpTile + 2) * 8 + 512;
+}
+
 template <typename K>
 void compact_diff_dev(const Launch& L, DedupDiffSel<K> sel, uint64_t cap, const uint64_t* d_n,
                       uint64_t* d_total, Scratch& s) {
@@ -621,19 +660,33 @@ void compact_diff_dev(const Launch& L, DedupDiffSel<K> sel, uint64_t cap, const 
   const uint64_t chunk = cp_chunk(cap, L.num_sms);
   const int nb = cp_blocks(cap, chunk);
   const uint64_t tiles = (cap + kCpTile - 1) / kCpTile;
+  const uint64_t mtiles = (cap + sel.n_full + kCpTile - 1) / kCpTile;
   uint32_t* flags = s.take<uint32_t>(cp_words(cap));
   uint32_t* counts = s.take<uint32_t>(nb);
   uint64_t* offs = s.take<uint64_t>(nb + 1);
   uint64_t* fpos = s.take<uint64_t>(tiles + 1);
+  uint64_t* split = s.take<uint64_t>(mtiles + 1);
   prefer_shared(dd_flag_kernel<K>);
+  // merge path: the mark pass ORs its bits into zeroed flag words
+  SRDL_CUDA(cudaMemsetAsync(flags, 0, cp_words(cap) * 4, L.stream));
+  dm_split_kernel<K><<<(unsigned)((mtiles + 1 + 255) / 256), 256, 0, L.stream>>>(sel, cap, mtiles, split,
+                                                                                nullptr, d_n, kPathMerge);
+  const unsigned mgrid = (unsigned)std::min<uint64_t>(mtiles, (uint64_t)L.num_sms * 4);
+  dm_mark_kernel<K><<<mgrid, kCpThreads, 0, L.stream>>>(sel, cap, mtiles, split, nullptr, flags, d_n,
+                                                        kPathMerge);
+  cp_count_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(flags, cap, 0, counts, sel, d_n, kPathMerge);
+  // probe path
   const uint64_t bthreads = (tiles + 1) * 32;
   dd_bounds_kernel<K><<<(unsigned)((bthreads + 255) / 256), 256, 0, L.stream>>>(sel, cap, tiles,
-                                                                                fpos, nullptr, d_n);
-  dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, cap, 0, fpos, nullptr, flags, counts, d_n);
+                                                                                fpos, nullptr, d_n,
+                                                                                kPathProbe);
+  dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, cap, 0, fpos, nullptr, flags, counts, d_n,
+                                                     kPathProbe);
+  // either way: offsets and the ordered write of the kept keys
   cp_scan_kernel<<<1, 1024, 0, L.stream>>>(counts, nb, offs, d_total);
   cp_write_kernel<DedupDiffSel<K>><<<nb, kCpThreads, 0, L.stream>>>(sel, cap, 0, flags, offs, d_n);
   SRDL_CUDA(cudaGetLastError());
-  count_launches(4);
+  count_launches(7);
 }
 
 // Distinct first-column values of a sorted key array.

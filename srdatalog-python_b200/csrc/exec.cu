@@ -69,11 +69,33 @@ std::vector<FilterTerm> parse_filter(const std::string& code) {
   return out;
 }
 
+// A message as a JSON string body: quotes and backslashes escaped, control
+// characters dropped.
+std::string json_escape(const std::string& m) {
+  std::string o;
+  for (char c : m) {
+    if (c == '"' || c == '\\') o += '\\';
+    if ((unsigned char)c >= 0x20) o += c;
+  }
+  return o;
+}
+
+// The device loop runs unless SRDL_DEVICE_LOOP=0 (or the device_loop option)
+// turns it off.
+bool device_loop_default() {
+  static const bool on = [] {
+    const char* e = std::getenv("SRDL_DEVICE_LOOP");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 }  // namespace
 
 constexpr uint64_t kSegsPerShard = 256;
 
-void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
+PipePlan Database::plan_pipeline(const Op& op, bool recursive, uint64_t iteration,
+                                 const std::map<std::string, TrieView>* dviews) {
   std::map<std::string, int> slot;
   int nslots = 0;
   auto bind = [&](const std::string& v) {
@@ -135,6 +157,16 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
     SRDL_REQUIRE(r.arity <= 2, kErrUnsupported, "join over relation " + r.name + " of arity > 2");
     SRDL_REQUIRE(d.prefix.size() < (size_t)std::max(r.arity, 2), kErrUnsupported,
                  "rule " + op.rule + ": prefix too long on " + r.name);
+    if (v == kDelta && dviews) {
+      // the device loop's DELTA of this relation (its canonical order)
+      auto dv = dviews->find(d.rel);
+      if (dv != dviews->end()) {
+        SrcSpec s;
+        s.t = dv->second;
+        s.prefix_slot = d.prefix.empty() ? -1 : slot_of(d.prefix[0]);
+        return s;
+      }
+    }
     Index& ix = ensure_index(r, v, d.index);
     // Hash long child lists of probed FULL indexes; a delta is rebuilt every
     // iteration and is usually the short (driving) side anyway.
@@ -273,6 +305,28 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
                  "rule " + op.rule + ": " + target->name + " is written in its canonical order only");
   }
 
+  PipePlan pp;
+  pp.levels = std::move(levels);
+  pp.insert = insert;
+  pp.target = target;
+  pp.nslots = nslots;
+  pp.sharded = sharded;
+  pp.work_split = work_split;
+  if (!op.count)
+    for (int c = 0; c < target->arity && c < 4; c++)
+      pp.key_slot[c] = slot_of(insert->vars[insert->index[c]]);
+  return pp;
+}
+
+void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
+  PipePlan pp = plan_pipeline(op, recursive, iteration, nullptr);
+  std::vector<LevelSpec>& levels = pp.levels;
+  Relation* target = pp.target;
+  const int nslots = pp.nslots;
+  const bool sharded = pp.sharded;
+  const size_t work_split = pp.work_split;
+  std::vector<uint64_t>& seen = level_max_[&op];
+  seen.resize(levels.size(), 0);
   // Walk the levels over a table of partial bindings.
   Table cur;
   cur.n = 1;
@@ -290,6 +344,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
     SRDL_CUDA(cudaMemsetAsync(d_small_.as<uint64_t>() + 2, 0, 8, L_.stream));
     SRDL_CUDA(cudaStreamSynchronize(L_.stream));
     uint64_t total = h_small_[3];
+    seen[li] = std::max(seen[li], total);
     if (sharded && op.shard == Op::Work && li == work_split) {
       // Deal this level's work items out in segments, kSegsPerShard per
       // shard, interleaved so every shard gets a share of each key range
@@ -341,9 +396,9 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
         lv.key_arity = target->arity;
         lv.pack_bits = target->pack_bits;
         lv.pack_half = target->pack_half;
-        for (int c = 0; c < target->arity; c++) lv.key_slot[c] = slot_of(insert->vars[insert->index[c]]);
+        for (int c = 0; c < target->arity; c++) lv.key_slot[c] = pp.key_slot[c];
         Chunk ch;
-        ch.order = insert->index;
+        ch.order = pp.insert->index;
         ch.keys = DevBuf(std::max<uint64_t>(total, 1) * 8, L_.stream);
         pid = prof_begin("join_expand_keys");
         join_expand(L_, lv, cur, w, total, nullptr, ch.keys.as<uint64_t>(),
@@ -403,6 +458,7 @@ void Database::op_rebuild(const Step& st, size_t pos, const Op& op) {
                    "relation " + r.name + " of arity > 2 rebuilt in another order");
   uint64_t total = 0;
   for (auto& c : rv.chunks) total += c.n;
+  if (op.ver == kNew) new_max_[r.name] = std::max(new_max_[r.name], total);
   // Gather the chunks into one buffer packed in the target order.
   DevBuf gathered;
   const uint64_t* in = nullptr;
@@ -461,6 +517,7 @@ void Database::op_compute_delta(const Op& op) {
   r.v[kDelta].clear();
   r.delta_epoch++;
   if (r.pending_delta) {
+    delta_max_[r.name] = std::max(delta_max_[r.name], r.pending.n);
     r.v[kDelta].idx[op.index] = std::move(r.pending);
     r.pending = Index{};
     r.pending_delta = false;
@@ -492,6 +549,7 @@ void Database::op_compute_delta(const Op& op) {
   d.n = read_scalar(0);
   prof_end(pid, 8.0 * (nw.n + f.n + d.n), (double)nw.n);
   if (r.lsm) subtract_head(r, op.index, d);
+  delta_max_[r.name] = std::max(delta_max_[r.name], d.n);
 }
 
 void Database::op_merge(const Op& op) {
@@ -771,6 +829,13 @@ void Database::run_steps(uint64_t max_iters) {
       std::vector<std::string> computed;
       for (auto& op : st.ops)
         if (op.kind == Op::ComputeDelta) computed.push_back(op.rel);
+      // From iteration 1 on, a qualifying step runs on the device loop
+      // (loop.cu); an overflow hands one iteration back to the host path,
+      // after which the loop is entered again (at most three times a step).
+      std::string why;
+      const bool loop_on =
+          (opt_device_loop_ < 0 ? device_loop_default() : opt_device_loop_ != 0) && loop_eligible(st, why);
+      int entries = 0;
       for (uint64_t it = 0; it < max_iters; it++) {
         if (it > 0) {
           uint64_t total = 0;
@@ -782,6 +847,16 @@ void Database::run_steps(uint64_t max_iters) {
           // sharded with exchanges: stop only when every shard's delta is empty
           if (xfn_ && shard_world_ > 1) total = shards_sum(total);
           if (total == 0) break;
+          if (loop_on && entries < 3) {
+            entries++;
+            uint64_t done = 0;
+            const int rc = run_device_loop(st, it, max_iters, &done);
+            step_stats_[si].iterations += done;
+            it += done;
+            if (rc == kLoopDone) break;
+            if (rc == kLoopSkipped) entries = 3;
+            if (it >= max_iters) break;
+          }
         }
         exec_ops(st, it);
         step_stats_[si].iterations++;
@@ -907,6 +982,10 @@ std::string Database::stats_json() const {
       << ",\"max_ms\":" << kv.second.max_ms << ",\"calls\":" << kv.second.calls << "}";
     ofirst = false;
   }
+  o << "},\"device_loop\":{\"entries\":" << loop_stats_.entries << ",\"iterations\":"
+    << loop_stats_.iterations << ",\"overflows\":" << loop_stats_.overflows << ",\"skipped\":"
+    << loop_stats_.skipped << ",\"capture_ms\":" << loop_stats_.capture_ms << ",\"run_ms\":"
+    << loop_stats_.run_ms << ",\"last_error\":\"" << json_escape(loop_stats_.last_error) << "\"";
   o << "},\"mem\":{\"peak_bytes\":" << mem_run_.peak << ",\"limit_bytes\":" << opt_mem_limit_;
   o << "},\"alloc\":{\"ms\":" << alloc_.ms << ",\"max_ms\":" << alloc_.max_ms
     << ",\"calls\":" << alloc_.calls << ",\"pool_reserved_gb\":" << pool_reserved_gb_;

@@ -394,7 +394,9 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
     unsigned long long* __restrict__ queue, Table out, uint64_t* __restrict__ out_keys,
     unsigned long long* __restrict__ d_out_n, uint64_t* __restrict__ chunk_counts, JoinDev jd) {
   const int lane = threadIdx.x & 31;
-  total = dev_total(jd, total);
+  // (count-only rules never run in the device loop: the count instance
+  // keeps the registers of the hot triangle level free of it)
+  if (MODE != kModeCount) total = dev_total(jd, total);
   const uint32_t* vals0 = lv.src[0].prefix_slot < 0 ? lv.src[0].t.roots : lv.src[0].t.lo;
   const uint32_t* vals1 = lv.src[1].prefix_slot < 0 ? lv.src[1].t.roots : lv.src[1].t.lo;
   // a roots-list side with a dense directory answers membership in O(1)
@@ -656,7 +658,7 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
   chunk = dev_warp_chunk(jd, chunk, total);
   // every candidate a result (no filter) and the output private to this
   // launch: each is written at its own index
-  const bool exact = MODE == kModeKeys && lv.nfilt == 0 && !jd.d_total;
+  const bool exact = MODE == kModeKeys && lv.nfilt == 0 && (!jd.d_total || jd.exact_ok);
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t c0 = gw * chunk;
   const uint64_t c1 = c0 + chunk < total ? c0 + chunk : total;
@@ -665,7 +667,10 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
   const int s0 = lv.src[0].out_slot, s1 = lv.src[1].out_slot;
   unsigned long long running = 0;
   if (MODE == kModeTableWrite) running = warp_counts[gw];
-  if (exact && gw == 0 && lane == 0) *d_out_n = total;
+  if (exact && gw == 0 && lane == 0) {
+    *d_out_n = total;
+    if (jd.out_cap && total > jd.out_cap && jd.d_overflow) atomicExch(jd.d_overflow, 1u);
+  }
   if (c0 < c1) {
     SegWalk<SEG> sw(lv, c0);
     uint64_t r0 = gallop_row(offs, 0, in.n, sw.at());
@@ -699,7 +704,7 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
             const int ks = lv.key_slot[i];
             kc[i] = i >= lv.key_arity ? 0u : ks == s0 ? v0 : ks == s1 ? v1 : slot_value(in, ks, r);
           }
-          out_keys[base + lane] = emit_key(lv, kc);
+          if (!jd.out_cap || base + lane < jd.out_cap) out_keys[base + lane] = emit_key(lv, kc);
         }
         r0 = __shfl_sync(kAllLanes, r, 31);
         continue;

@@ -90,6 +90,14 @@ void merge_disjoint_dev(const Launch& L, const uint64_t* a, uint64_t na_cap, con
                         const uint64_t* b, uint64_t nb_cap, const uint64_t* d_nb, uint64_t* out,
                         uint64_t out_cap, uint64_t* d_nout, unsigned int* d_overflow);
 
+// Scratch sort_dedup_dev needs for `cap` keys against a FULL of full_cap.
+size_t sort_dev_scratch_bytes(uint64_t cap, uint64_t full_cap, int bits);
+
+// Sets, once, the kernel attributes the device loop's kernels use (a graph
+// capture must not be the first to set them).
+void warm_device_loop_kernels(int bits);
+void warm_merge_kernels();
+
 // sort_dedup with the input count on the device (device loop): `cap` keys of
 // room in `in`, *d_n present; FULL (room full_cap, count *d_n_full, may be
 // null) is subtracted.  No host decision depends on the counts.
@@ -269,6 +277,10 @@ struct JoinDev {
   const uint64_t* d_total = nullptr;
   uint64_t out_cap = 0;
   unsigned int* d_overflow = nullptr;
+  // emit keys: the output buffer is this launch's alone (one rule fills the
+  // relation's NEW), so a filter-free product may write each key at its
+  // candidate index and set *d_out_n to the count
+  bool exact_ok = false;
 };
 
 void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const JoinWork& w,

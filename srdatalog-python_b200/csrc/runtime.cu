@@ -565,6 +565,7 @@ void Database::reset_device_state() {
   counts_.clear();
   group_counts_.clear();
   kstats_.clear();
+  loop_stats_ = LoopStats{};
   derived_ = 0;
   for (auto& s : step_stats_) s = StepStats{};
 }
@@ -901,6 +902,8 @@ void Database::set_option(const std::string& name, int64_t value) {
   else if (name == "hash_min") opt_hash_min_ = value;
   else if (name == "lsm_compact_pct") opt_lsm_pct_ = value;
   else if (name == "mem_limit_mb") opt_mem_limit_ = (uint64_t)value << 20;
+  else if (name == "device_loop") opt_device_loop_ = value ? 1 : 0;
+  else if (name == "device_loop_cap_limit") opt_loop_cap_limit_ = (uint64_t)value;
   else if (name == "shard_world") {
     SRDL_REQUIRE(value >= 1 && value <= 65536, kErrArg, "set_option: shard_world out of [1, 65536]");
     shard_world_ = value;

@@ -230,6 +230,18 @@ struct OpStats {
   uint64_t calls = 0;
 };
 
+// A pipeline's join levels, built from the plan (sources resolved to
+// index views), before any is run.
+struct PipePlan {
+  std::vector<LevelSpec> levels;
+  const PipeOp* insert = nullptr;
+  Relation* target = nullptr;
+  int nslots = 0;
+  int key_slot[4] = {-1, -1, -1, -1};  // emitted key columns (materialising rules)
+  bool sharded = false;
+  size_t work_split = 0;
+};
+
 class Database {
  public:
   Database(const std::string& plan_json, int device);
@@ -319,6 +331,20 @@ class Database {
   AllocStats alloc_{0, 0, 0};
   double pool_reserved_gb_ = 0;
   uint64_t launches_ = 0;
+  // The device loop (loop.cu): statistics of the last run, on/off.
+  struct LoopStats {
+    uint64_t entries = 0, iterations = 0, overflows = 0, skipped = 0;
+    double capture_ms = 0, run_ms = 0;
+    std::string last_error;
+  };
+  LoopStats loop_stats_;
+  int64_t opt_device_loop_ = -1;     // -1: SRDL_DEVICE_LOOP (0 turns it off) or on
+  uint64_t opt_loop_cap_limit_ = 0;  // largest capacity the loop may choose (0: none; tests force overflows)
+  // Largest candidate count seen per join level of each execute op, and the
+  // largest NEW (before dedup), DELTA and final FULL sizes per relation, kept
+  // across runs: the device loop sizes its buffers from them.
+  std::map<const Op*, std::vector<uint64_t>> level_max_;
+  std::map<std::string, uint64_t> new_max_, delta_max_, full_max_;
   size_t prof_begin(const std::string& name);
   void prof_end(size_t id, double bytes, double units);
   void prof_collect();
@@ -347,7 +373,18 @@ class Database {
   void sort_into(Index& out, const uint64_t* in, uint64_t n, bool swap, const Index* full,
                  const Index* head = nullptr, int key_bits = 0);
   void run_steps(uint64_t max_iters);
+  // Device loop: whether a recursive step qualifies (why not, when it does
+  // not), and running its iterations from it0 on the device; returns
+  // kLoopDone (fixpoint or iteration limit reached), kLoopOverflow (a
+  // capacity was too small: iteration it0 + *done is to be redone on the
+  // host) or kLoopSkipped (nothing done).
+  enum { kLoopDone = 0, kLoopOverflow = 1, kLoopSkipped = 2 };
+  bool loop_eligible(const Step& st, std::string& why);
+  int run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, uint64_t* done);
   void exec_ops(const Step& st, uint64_t iteration);
+  // dviews: DELTA views that replace the relation's DELTA index (device loop)
+  PipePlan plan_pipeline(const Op& op, bool recursive, uint64_t iteration,
+                         const std::map<std::string, TrieView>* dviews);
   void exec_pipeline(const Op& op, bool recursive, uint64_t iteration);
   void op_rebuild(const Step& st, size_t pos, const Op& op);
   void op_compute_delta(const Op& op);

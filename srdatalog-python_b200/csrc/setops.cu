@@ -153,6 +153,8 @@ void merge_disjoint(const Launch& L, const uint64_t* a, uint64_t na, const uint6
   count_launches(2);
 }
 
+void warm_merge_kernels() { prefer_shared(merge_kernel); }
+
 void merge_disjoint_dev(const Launch& L, const uint64_t* a, uint64_t na_cap, const uint64_t* d_na,
                         const uint64_t* b, uint64_t nb_cap, const uint64_t* d_nb, uint64_t* out,
                         uint64_t out_cap, uint64_t* d_nout, unsigned int* d_overflow) {

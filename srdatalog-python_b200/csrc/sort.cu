@@ -290,6 +290,10 @@ static void launch_scatter(const Launch& L, int nb, int w, const K* in, K* out, 
 
 static inline bool use32(int bits) { return 2 * bits <= 32; }
 
+size_t sort_dev_scratch_bytes(uint64_t cap, uint64_t full_cap, int bits) {
+  return sort_scratch_bytes(cap, bits) + diff_dev_extra_bytes(cap, full_cap);
+}
+
 size_t sort_scratch_bytes(uint64_t n, int bits) {
   const size_t ks = use32(bits) ? 4 : 8;
   const size_t counts = (size_t)kRsBins * 256 * 8 * 4;  // <= 8 blocks per SM, 256 SMs
@@ -353,6 +357,25 @@ void sort_dedup(const Launch& L, const uint64_t* in, uint64_t n, int bits, bool 
                            nullptr, nullptr);
   else sort_dedup_t<uint64_t>(L, in, n, bits, swap, full, n_full, out, d_nout, s, head, n_head,
                               nullptr, nullptr);
+}
+
+template <typename K>
+static void warm_sort_kernels() {
+  prefer_shared(rs_scatter<K, 1>);
+  prefer_shared(rs_scatter<K, 2>);
+  prefer_shared(rs_scatter<K, 3>);
+  prefer_shared(rs_scatter<K, 4>);
+  prefer_shared(rs_scatter<K, 5>);
+  prefer_shared(rs_scatter<K, 6>);
+  prefer_shared(rs_scatter<K, 7>);
+  prefer_shared(rs_scatter<K, 8>);
+  prefer_shared(dd_flag_kernel<K>);
+}
+
+void warm_device_loop_kernels(int bits) {
+  if (use32(bits)) warm_sort_kernels<uint32_t>();
+  else warm_sort_kernels<uint64_t>();
+  warm_merge_kernels();
 }
 
 void sort_dedup_dev(const Launch& L, const uint64_t* in, uint64_t cap, const uint64_t* d_n,

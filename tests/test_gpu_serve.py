@@ -59,9 +59,12 @@ def test_mixed_requests_same_alone_and_in_the_mix():
       assert r.result == oracle.triangle_count(e)
 
 
-def peak_alone(req):
-  '''Device bytes a fresh handle holds at the peak of the request's run.'''
+def peak_alone(req, loop=True):
+  '''Device bytes a fresh handle holds at the peak of the request's run
+  (loop=False: on the host path, the least a run needs -- under a tighter
+  memory limit the device loop declines its buffers and runs there).'''
   db = native.Database(load_plan(req.program))
+  db.set_option('device_loop', 1 if loop else 0)
   for rel, rows in req.inputs.items():
     db.load_rows(rel, rows)
   db.run()
@@ -91,7 +94,7 @@ def test_outgrown_reservation_is_requeued_and_held_back():
   alone, and the measured device bytes never pass the budget.'''
   progs = {'tc': ProgramSpec(load_plan('tc'), 'Path', bytes_per_edge=1)}
   reqs = [Request(i, 'tc', {'ArcInput': W.uniform_edges(2000, 6000, 40 + i)}) for i in range(3)]
-  peak = max(peak_alone(r) for r in reqs)
+  peak = max(peak_alone(r, loop=False) for r in reqs)
   mb = 1 << 20
   grown = mb << max(0, (peak - 1) // mb).bit_length()    # the doubling's first reservation >= peak
   budget = grown + grown // 2                            # room for one such run at a time
