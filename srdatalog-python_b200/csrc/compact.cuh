@@ -214,22 +214,25 @@ template <typename K>
 __global__ void dd_bounds_kernel(DedupDiffSel<K> sel, uint64_t n, uint64_t tiles,
                                  uint64_t* __restrict__ fpos, uint64_t* __restrict__ hpos,
                                  const uint64_t* d_n, int path) {
-  const uint64_t t = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / 32;
-  if (t > tiles) return;
   sel.n_full = dev_size(sel.n_full, sel.d_n_full);
   n = dev_size(n, d_n);
   if (!diff_path_runs(path, sel, n)) return;
   const uint64_t real = (n + kCpTile - 1) / kCpTile;  // tiles holding keys
-  uint64_t p = sel.n_full, q = sel.n_head;
-  if (t < real) {
-    const uint64_t first = sel.expand(sel.a[t * kCpTile]);
-    p = warp_partition_point(0, sel.n_full, [&](uint64_t i) { return sel.full[i] < first; });
-    if (hpos)
-      q = warp_partition_point(0, sel.n_head, [&](uint64_t i) { return sel.head[i] < first; });
-  }
-  if ((threadIdx.x & 31) == 0) {
-    fpos[t] = p;
-    if (hpos) hpos[t] = q;
+  // one warp per boundary; warps walk the boundaries when the grid is capped
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) / 32;
+  for (uint64_t t = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / 32; t <= tiles; t += warps) {
+    uint64_t p = sel.n_full, q = sel.n_head;
+    if (t < real) {
+      const uint64_t first = sel.expand(sel.a[t * kCpTile]);
+      p = warp_partition_point(0, sel.n_full, [&](uint64_t i) { return sel.full[i] < first; });
+      if (hpos)
+        q = warp_partition_point(0, sel.n_head, [&](uint64_t i) { return sel.head[i] < first; });
+    }
+    if ((threadIdx.x & 31) == 0) {
+      fpos[t] = p;
+      if (hpos) hpos[t] = q;
+    }
+    if (d_n && t > real) break;  // past the true tiles every entry is n_full
   }
 }
 
@@ -675,11 +678,11 @@ void compact_diff_dev(const Launch& L, DedupDiffSel<K> sel, uint64_t cap, const 
   dm_mark_kernel<K><<<mgrid, kCpThreads, 0, L.stream>>>(sel, cap, mtiles, split, nullptr, flags, d_n,
                                                         kPathMerge);
   cp_count_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(flags, cap, 0, counts, sel, d_n, kPathMerge);
-  // probe path
+  // probe path (a capped grid of warps walks the tile boundaries)
   const uint64_t bthreads = (tiles + 1) * 32;
-  dd_bounds_kernel<K><<<(unsigned)((bthreads + 255) / 256), 256, 0, L.stream>>>(sel, cap, tiles,
-                                                                                fpos, nullptr, d_n,
-                                                                                kPathProbe);
+  const uint64_t bblocks = std::min<uint64_t>((bthreads + 255) / 256, (uint64_t)L.num_sms * 8);
+  dd_bounds_kernel<K><<<(unsigned)bblocks, 256, 0, L.stream>>>(sel, cap, tiles, fpos, nullptr, d_n,
+                                                              kPathProbe);
   dd_flag_kernel<K><<<nb, kCpThreads, 0, L.stream>>>(sel, cap, 0, fpos, nullptr, flags, counts, d_n,
                                                      kPathProbe);
   // either way: offsets and the ordered write of the kept keys

@@ -98,45 +98,50 @@ __global__ void __launch_bounds__(kMgThreads) merge_kernel(const uint64_t* __res
   __shared__ uint64_t split[2];
   if (!merge_dev_sizes(md, na, nb)) return;
   const uint64_t total = na + nb;
-  const uint64_t d0 = (uint64_t)blockIdx.x * kMgTile;
-  if (d0 >= total) return;
-  const uint64_t d1 = d0 + kMgTile < total ? d0 + kMgTile : total;
-  const bool last = d1 == total;
-  if (threadIdx.x == 0) split[0] = out[d0];
-  if (threadIdx.x == 1) split[1] = last ? na : out[d0 + 1];
-  __syncthreads();
-  const uint64_t i0 = split[0], i1 = split[1];
-  const uint64_t j0 = d0 - i0, j1 = d1 - i1;
-  const int la = (int)(i1 - i0), lb = (int)(j1 - j0), lt = la + lb;
-  for (int k = threadIdx.x; k < lt; k += kMgThreads)
-    sin[mg_pad(k)] = k < la ? a[i0 + k] : b[j0 + k - la];
-  __syncthreads();
-  const int ld = threadIdx.x * kMgItems;
-  if (ld < lt) {
-    int lo = ld > lb ? ld - lb : 0, hi = ld < la ? ld : la;
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (sin[mg_pad(mid)] <= sin[mg_pad(la + ld - 1 - mid)]) lo = mid + 1;
-      else hi = mid;
-    }
-    int i = lo, j = ld - lo;
-    uint64_t va = i < la ? sin[mg_pad(i)] : 0, vb = j < lb ? sin[mg_pad(la + j)] : 0;
+  // one output tile per block (host sizes); with the counts on the device
+  // the capped grid walks the tiles
+  for (uint64_t tile = blockIdx.x;; tile += gridDim.x) {
+    const uint64_t d0 = tile * kMgTile;
+    if (d0 >= total) return;
+    const uint64_t d1 = d0 + kMgTile < total ? d0 + kMgTile : total;
+    const bool last = d1 == total;
+    if (threadIdx.x == 0) split[0] = out[d0];
+    if (threadIdx.x == 1) split[1] = last ? na : out[d0 + 1];
+    __syncthreads();
+    const uint64_t i0 = split[0], i1 = split[1];
+    const uint64_t j0 = d0 - i0, j1 = d1 - i1;
+    const int la = (int)(i1 - i0), lb = (int)(j1 - j0), lt = la + lb;
+    for (int k = threadIdx.x; k < lt; k += kMgThreads)
+      sin[mg_pad(k)] = k < la ? a[i0 + k] : b[j0 + k - la];
+    __syncthreads();
+    const int ld = threadIdx.x * kMgItems;
+    if (ld < lt) {
+      int lo = ld > lb ? ld - lb : 0, hi = ld < la ? ld : la;
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (sin[mg_pad(mid)] <= sin[mg_pad(la + ld - 1 - mid)]) lo = mid + 1;
+        else hi = mid;
+      }
+      int i = lo, j = ld - lo;
+      uint64_t va = i < la ? sin[mg_pad(i)] : 0, vb = j < lb ? sin[mg_pad(la + j)] : 0;
 #pragma unroll
-    for (int k = 0; k < kMgItems; k++) {
-      if (ld + k >= lt) break;
-      const bool take_a = (j >= lb) || (i < la && va <= vb);
-      sout[mg_pad(ld + k)] = take_a ? va : vb;
-      if (take_a) {
-        i++;
-        va = i < la ? sin[mg_pad(i)] : 0;
-      } else {
-        j++;
-        vb = j < lb ? sin[mg_pad(la + j)] : 0;
+      for (int k = 0; k < kMgItems; k++) {
+        if (ld + k >= lt) break;
+        const bool take_a = (j >= lb) || (i < la && va <= vb);
+        sout[mg_pad(ld + k)] = take_a ? va : vb;
+        if (take_a) {
+          i++;
+          va = i < la ? sin[mg_pad(i)] : 0;
+        } else {
+          j++;
+          vb = j < lb ? sin[mg_pad(la + j)] : 0;
+        }
       }
     }
+    __syncthreads();
+    for (int k = threadIdx.x; k < lt; k += kMgThreads) out[d0 + k] = sout[mg_pad(k)];
+    __syncthreads();  // the shared tiles are refilled for the next tile
   }
-  __syncthreads();
-  for (int k = threadIdx.x; k < lt; k += kMgThreads) out[d0 + k] = sout[mg_pad(k)];
 }
 
 void merge_disjoint(const Launch& L, const uint64_t* a, uint64_t na, const uint64_t* b,
@@ -164,7 +169,10 @@ void merge_disjoint_dev(const Launch& L, const uint64_t* a, uint64_t na_cap, con
   prefer_shared(merge_kernel);
   merge_split_kernel<<<(unsigned)((blocks + 255) / 256), 256, 0, L.stream>>>(a, na_cap, b, nb_cap,
                                                                              blocks, out, md);
-  merge_kernel<<<(unsigned)blocks, kMgThreads, 0, L.stream>>>(a, na_cap, b, nb_cap, out, md);
+  // a capped grid (the tiles are walked): blocks beyond the true count would
+  // only be scheduled to exit
+  const uint64_t mgrid = std::min<uint64_t>(blocks, (uint64_t)L.num_sms * 8);
+  merge_kernel<<<(unsigned)mgrid, kMgThreads, 0, L.stream>>>(a, na_cap, b, nb_cap, out, md);
   SRDL_CUDA(cudaGetLastError());
   count_launches(2);
 }
