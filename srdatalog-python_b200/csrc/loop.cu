@@ -78,10 +78,13 @@ __global__ void loop_ctrl_kernel(LoopCtl* ctl, LoopCounts* cnt, int nrel, int p,
 
 constexpr uint64_t kLoopMaxIters = 20000;  // iterations one graph launch may run
 
+// n rounded up to a quarter step of its power of two (at least 1024).
 uint64_t round_cap(uint64_t n) {
-  uint64_t c = 1024;
-  while (c < n) c <<= 1;
-  return c;
+  if (n <= 1024) return 1024;
+  uint64_t p = 1024;
+  while (p * 2 <= n) p <<= 1;
+  const uint64_t q = p / 4;
+  return (n + q - 1) / q * q;
 }
 
 }  // namespace
@@ -218,10 +221,11 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
       Index& f = ensure_index(r, kFull, r.canonical);  // merges a Device2LevelIndex HEAD
       auto dit = r.v[kDelta].idx.find(r.canonical);
       const uint64_t dn = dit == r.v[kDelta].idx.end() ? 0 : dit->second.n;
+      // room: twice the largest NEW seen; FULL's final size seen before plus
+      // an eighth, or the current FULL plus two NEW rooms
       const uint64_t seen_new = std::max(new_max_[name], dn);
-      lr.cap_new = round_cap(std::max<uint64_t>(4 * seen_new, 1 << 16));
-      lr.cap_full = round_cap(std::max<uint64_t>(std::max(2 * f.n, full_max_[name] + full_max_[name] / 4),
-                                                 f.n + 4 * lr.cap_new));
+      lr.cap_new = round_cap(std::max<uint64_t>(2 * seen_new, 1 << 16));
+      lr.cap_full = round_cap(std::max<uint64_t>(full_max_[name] + full_max_[name] / 8, f.n + 2 * lr.cap_new));
       if (opt_loop_cap_limit_) {
         // smaller capacities than the counts seen (tests of the overflow path)
         lr.cap_new = std::max<uint64_t>(std::min(lr.cap_new, opt_loop_cap_limit_), dn + 1);
@@ -230,6 +234,18 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
       for (const Op* op : execs)
         for (auto& po : op->pipeline)
           if (po.kind == PipeOp::Insert && po.rel == name) lr.producers++;
+      {
+        // the buffers below; leave the step to the host path rather than
+        // take most of the free memory (the host path needs far less)
+        const uint64_t need = lr.cap_new * (8 + 16 + 16) + sort_dev_scratch_bytes(lr.cap_new, lr.cap_full, bits_) +
+                              lr.cap_full * 16;
+        size_t free_b = 0, total_b = 0;
+        SRDL_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const ArenaUse au = arena_use(L_.stream);
+        if ((double)need > 0.7 * (double)(free_b + au.cached))
+          throw Error{kErrCapacity, "device loop buffers (" + std::to_string(need >> 20) +
+                                        " MB) would take most of the free device memory"};
+      }
       lr.newk = DevBuf(lr.cap_new * 8, L_.stream);
       lr.sort_scr = DevBuf(sort_dev_scratch_bytes(lr.cap_new, lr.cap_full, bits_), L_.stream);
       lr.trie_scr = DevBuf(roots_scratch_bytes(lr.cap_new) + 1024, L_.stream);
@@ -249,7 +265,7 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
       for (size_t li = 0; li < seen.size(); li++) {
         LoopLevel ll;
         ll.cap_rows = rows;
-        ll.cap_total = round_cap(std::max<uint64_t>(4 * seen[li], 4096));
+        ll.cap_total = round_cap(std::max<uint64_t>(2 * seen[li], 4096));
         if (opt_loop_cap_limit_) ll.cap_total = std::min(ll.cap_total, opt_loop_cap_limit_);
         ll.wscr = DevBuf(join_work_scratch_bytes(ll.cap_rows), L_.stream);
         ll.xscr = DevBuf(join_expand_scratch_bytes(L_, ll.cap_total), L_.stream);
@@ -433,9 +449,24 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
     count_launches(1);
   };
 
-  // ---- capture: WHILE (go) { body(0); IF (go) { body(1) } }
+  // ---- capture: WHILE (go) { body(0); IF (go) { body(1) } }, on the loop's
+  // own stream, after everything queued on the database's stream
   // (kernel attributes are set before the capture, not inside it)
   warm_device_loop_kernels(bits_);
+  if (!loop_stream_) {
+    SRDL_CUDA(cudaStreamCreateWithFlags(&loop_stream_, cudaStreamNonBlocking));
+    SRDL_CUDA(cudaEventCreateWithFlags(&loop_ev_[0], cudaEventDisableTiming));
+    SRDL_CUDA(cudaEventCreateWithFlags(&loop_ev_[1], cudaEventDisableTiming));
+  }
+  SRDL_CUDA(cudaEventRecord(loop_ev_[0], L_.stream));
+  SRDL_CUDA(cudaStreamWaitEvent(loop_stream_, loop_ev_[0], 0));
+  const cudaStream_t db_stream = L_.stream;
+  struct StreamSwap {
+    Launch& L;
+    cudaStream_t keep;
+    ~StreamSwap() { L.stream = keep; }
+  } swap{L_, db_stream};
+  L_.stream = loop_stream_;
   const bool prof = profile_;
   profile_ = false;
   const uint64_t l0 = launches_total();
@@ -502,7 +533,7 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
     profile_ = prof;
     count_launches(-(int)(launches_total() - l0));
     (void)cudaGetLastError();
-    SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+    SRDL_CUDA(cudaStreamSynchronize(loop_stream_));
     loop_stats_.skipped++;
     loop_stats_.last_error = e.msg;
     return kLoopSkipped;
@@ -511,16 +542,19 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
   count_launches(-(int)(launches_total() - l0));  // counted again per executed iteration below
   const auto t1 = std::chrono::steady_clock::now();
 
-  // ---- run
+  // ---- run (events on the database's stream time the launch)
+  L_.stream = db_stream;
   size_t pid = prof_begin("device_loop");
-  SRDL_CUDA(cudaGraphLaunch(ge, L_.stream));
+  SRDL_CUDA(cudaGraphLaunch(ge, loop_stream_));
   LoopCtl ctl{};
   std::vector<LoopCounts> cnt(X.rels.size());
-  SRDL_CUDA(cudaMemcpyAsync(&ctl, X.ctl.as<void>(), sizeof(ctl), cudaMemcpyDeviceToHost, L_.stream));
+  SRDL_CUDA(cudaMemcpyAsync(&ctl, X.ctl.as<void>(), sizeof(ctl), cudaMemcpyDeviceToHost, loop_stream_));
   SRDL_CUDA(cudaMemcpyAsync(cnt.data(), X.cnt.as<void>(), cnt.size() * sizeof(LoopCounts),
-                            cudaMemcpyDeviceToHost, L_.stream));
+                            cudaMemcpyDeviceToHost, loop_stream_));
+  SRDL_CUDA(cudaEventRecord(loop_ev_[1], loop_stream_));
+  SRDL_CUDA(cudaStreamWaitEvent(db_stream, loop_ev_[1], 0));
   prof_end(pid, 0, (double)X.rels.size());
-  SRDL_CUDA(cudaStreamSynchronize(L_.stream));
+  SRDL_CUDA(cudaStreamSynchronize(loop_stream_));
   count_launches((int)(per_body * ctl.bodies));
   const auto t2 = std::chrono::steady_clock::now();
 

@@ -290,6 +290,9 @@ Database::~Database() {
       cudaEventDestroy(e.b);
     }
     for (auto e : ev_pool_) cudaEventDestroy(e);
+    if (loop_stream_) cudaStreamDestroy(loop_stream_);
+    for (auto e : loop_ev_)
+      if (e) cudaEventDestroy(e);
     if (own_stream_) cudaStreamDestroy(L_.stream);
   }
 }

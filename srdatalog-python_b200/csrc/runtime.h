@@ -339,6 +339,11 @@ class Database {
   };
   LoopStats loop_stats_;
   int64_t opt_device_loop_ = -1;     // -1: SRDL_DEVICE_LOOP (0 turns it off) or on
+  // The loop's graph is captured and launched on a stream of its own (the
+  // database's stream may be a default stream, which cannot be captured),
+  // ordered after and before the database's stream by two events.
+  cudaStream_t loop_stream_ = nullptr;
+  cudaEvent_t loop_ev_[2] = {nullptr, nullptr};
   uint64_t opt_loop_cap_limit_ = 0;  // largest capacity the loop may choose (0: none; tests force overflows)
   // Largest candidate count seen per join level of each execute op, and the
   // largest NEW (before dedup), DELTA and final FULL sizes per relation, kept

@@ -9,7 +9,8 @@ sizes against a device-memory budget and batches them continuously.
 * Estimates: a request's first reservation comes from its program's measured
   runs: the largest peak per input edge of runs in its size class (input
   edges to a power of two; the nearest class seen), times 1.25, with a 1 MB
-  floor; before any run, from the spec's bytes_per_edge.
+  floor; before any run, from the spec's bytes_per_edge.  A run that
+  outgrows its reservation raises its class to twice that reservation.
 * Enforcement: a run may hold at most its batch's reservations on the device
   (libsrdl's per-run limit, option mem_limit_mb, measured by the handle's
   caching arena).  A run that outgrows it stops with status 5; its requests
@@ -108,8 +109,9 @@ class Server:
   def __init__(self, programs: dict, device: int = 0, workers: int = 8,
                budget_bytes: int = 120 << 30, max_batch: int = 16, batching: bool = True,
                keep_rows: bool = False, batch_max_edges: int = 1 << 20,
-               batch_max_span: int = 1 << 23, learn: bool = True):
+               batch_max_span: int = 1 << 23, learn: bool = True, device_loop: bool = False):
     self.programs = programs
+    self.device_loop = device_loop
     # Reservation estimates learned from measured peaks: per program and
     # size class (input edges to a power of two), the largest peak per input
     # edge seen.  Without learning (or before the program's first run) the
@@ -228,6 +230,16 @@ class Server:
     b = m.bit_length()
     ratios[b] = max(ratios.get(b, 0.0), peak / m)
 
+  def _observe_outgrown(self, batch: list) -> None:
+    '''A run that outgrew its reservation needs more than it: its size
+    class starts at twice that from now on (cv held).'''
+    if not self.learn:
+      return
+    m = max(1, sum(_edges(r) for r in batch))
+    ratios = self.est_ratio.setdefault(batch[0].program, {})
+    b = m.bit_length()
+    ratios[b] = max(ratios.get(b, 0.0), 2.0 * sum(r.footprint for r in batch) / m)
+
   def _requeue(self, r: Request) -> None:
     '''Back into the pending queue in arrival order (ahead of later arrivals).'''
     i = 0
@@ -296,6 +308,7 @@ class Server:
             r.peak_bytes = mem['peak']
           if outgrown:
             self.retried += 1
+            self._observe_outgrown(batch)
             for r in batch:
               if r.footprint >= self.budget:
                 r.error = outgrown
@@ -332,6 +345,10 @@ class Server:
     if db is None:
       db = dbs[program] = Database(self.programs[program].plan, device=self.device)
       db.init_device()
+      # The served requests are small and their unions short-lived: the
+      # device loop's graph capture and capacity buffers cost them more than
+      # its saved host round trips (and inflate the learned reservations).
+      db.set_option('device_loop', 1 if self.device_loop else 0)
       with self.cv:
         self.handles.append(db)
     return db

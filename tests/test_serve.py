@@ -113,3 +113,10 @@ def test_estimates_learn_from_measured_peaks():
   off = Server(programs(), workers=0, learn=False)
   off._observe([small], 5 << 20)
   assert off._estimate(off.programs['tc'], small) == 1 << 20
+
+
+def test_outgrown_runs_raise_their_size_class():
+  s = Server(programs(), workers=0, budget_bytes=1 << 40)
+  r = Request(0, 'tc', {'ArcInput': np.zeros((1 << 12, 2), np.uint32)}, footprint=8 << 20)
+  s._observe_outgrown([r])                     # 8 MB was not enough for 4,096 edges
+  assert s._estimate(s.programs['tc'], r) == int(2 * (8 << 20) * 1.25)
