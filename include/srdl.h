@@ -88,6 +88,9 @@ int srdl_set_profiling(srdl_db* db, int enable);
  *                      b-bit keys runs ceil(b / radix_bits) passes
  *   "join_blocks_per_sm"  join launches use at most this many blocks per
  *                      SM, 1..64 (default 16): the candidates per warp
+ *   "join_chunk"       largest chunk of candidates a warp of the two-source
+ *                      column join takes from its queue, 64..2^20 (default
+ *                      4096): smaller chunks keep the rows in flight closer
  *   "device_loop"      1 (default; SRDL_DEVICE_LOOP=0 changes it) runs the
  *                      iterations of a qualifying recursive step after the
  *                      first as one CUDA graph that loops on the device

@@ -833,7 +833,7 @@ void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const Jo
     const int bpsm = std::max(1, std::min(occ, L.join_bpsm > 0 ? L.join_bpsm : 16));
     const uint64_t resident = (uint64_t)L.num_sms * bpsm * (kJThreads / 32);
     uint64_t chunk = (total + resident * 8 - 1) / (resident * 8);
-    chunk = std::min<uint64_t>(std::max<uint64_t>(chunk, 64), 4096);
+    chunk = std::min<uint64_t>(std::max<uint64_t>(chunk, 64), (uint64_t)std::max(64, L.join_chunk));
     if (lv.emit == kEmitTable)
       chunk = std::max<uint64_t>(chunk, (total + kCj2MaxTableChunks - 1) / kCj2MaxTableChunks);
     chunk = (chunk + 31) & ~uint64_t(31);

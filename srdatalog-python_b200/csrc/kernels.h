@@ -17,6 +17,7 @@ struct Launch {
   uint32_t* d_err = nullptr;  // device error word (bounded-wait failures etc.)
   int radix_bits = 8;         // widest radix-sort digit (1..8): passes = ceil(key bits / this)
   int join_bpsm = 16;         // join launches: at most this many blocks per SM (work per warp)
+  int join_chunk = 4096;      // two-source column join: largest chunk of candidates a warp takes
 };
 
 // Bump allocator over a caller-provided scratch region.  Every piece starts

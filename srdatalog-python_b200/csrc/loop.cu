@@ -54,9 +54,11 @@ struct LoopCtl {
   unsigned long long done;       // complete iterations
   unsigned long long remaining;  // iterations this launch may still do
   unsigned long long bodies;     // iterations started (complete or not)
+  double alg_bytes;              // algorithmic bytes of the complete iterations (as the host path counts them)
 };
 
-__global__ void loop_ctrl_kernel(LoopCtl* ctl, LoopCounts* cnt, int nrel, int p,
+// ks: packed key bytes of the sort, passes: its counting passes.
+__global__ void loop_ctrl_kernel(LoopCtl* ctl, LoopCounts* cnt, int nrel, int p, int ks, int passes,
                                  cudaGraphConditionalHandle hw, cudaGraphConditionalHandle hi,
                                  int set_if) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
@@ -67,8 +69,14 @@ __global__ void loop_ctrl_kernel(LoopCtl* ctl, LoopCounts* cnt, int nrel, int p,
     ctl->parity = 1 - p;
     uint64_t delta = 0;
     for (int r = 0; r < nrel; r++) {
+      const double nn = (double)cnt[r].n_new, nd = (double)cnt[r].n_delta[1 - p];
+      const double nf = (double)cnt[r].n_full[p];
       delta += cnt[r].n_delta[1 - p];
       cnt[r].derived += cnt[r].n_new;
+      // emitted keys, the sort with its fused difference, the merge and
+      // the delta's trie view -- the bytes the host path charges for them
+      ctl->alg_bytes += 8.0 * nn + passes * 2.0 * ks * nn + 8.0 * nn + 2.0 * ks * nn + 8.0 * nd +
+                        8.0 * nn + 16.0 * (nf + nd) + 16.0 * nd;
     }
     go = delta > 0 && ctl->done < ctl->remaining;
   }
@@ -444,7 +452,11 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
       build_dir(L_, lr.delta[1 - p].as<uint64_t>(), lr.cap_new, lr.dir[1 - p].as<uint32_t>(), X.dir_n,
                 &c->n_delta[1 - p]);
     }
-    loop_ctrl_kernel<<<1, 32, 0, L_.stream>>>(X.ctl_d(), cnt, (int)X.rels.size(), p, hw, hi, set_if);
+    const int ks = 2 * bits_ <= 32 ? 4 : 8;
+    const int maxw = L_.radix_bits >= 1 && L_.radix_bits <= 8 ? L_.radix_bits : 8;
+    const int passes = (2 * bits_ + maxw - 1) / maxw;
+    loop_ctrl_kernel<<<1, 32, 0, L_.stream>>>(X.ctl_d(), cnt, (int)X.rels.size(), p, ks, passes, hw, hi,
+                                              set_if);
     SRDL_CUDA(cudaGetLastError());
     count_launches(1);
   };
@@ -555,6 +567,7 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
   SRDL_CUDA(cudaStreamWaitEvent(db_stream, loop_ev_[1], 0));
   prof_end(pid, 0, (double)X.rels.size());
   SRDL_CUDA(cudaStreamSynchronize(loop_stream_));
+  if (pid != (size_t)-1) kev_[pid].bytes = ctl.alg_bytes;
   count_launches((int)(per_body * ctl.bodies));
   const auto t2 = std::chrono::steady_clock::now();
 

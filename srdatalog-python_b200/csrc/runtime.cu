@@ -914,6 +914,9 @@ void Database::set_option(const std::string& name, int64_t value) {
   else if (name == "radix_bits") {
     SRDL_REQUIRE(value >= 1 && value <= 8, kErrArg, "set_option: radix_bits out of [1, 8]");
     L_.radix_bits = (int)value;
+  } else if (name == "join_chunk") {
+    SRDL_REQUIRE(value >= 64 && value <= (1 << 20), kErrArg, "set_option: join_chunk out of [64, 2^20]");
+    L_.join_chunk = (int)value;
   } else if (name == "join_blocks_per_sm") {
     SRDL_REQUIRE(value >= 1 && value <= 64, kErrArg, "set_option: join_blocks_per_sm out of [1, 64]");
     L_.join_bpsm = (int)value;
