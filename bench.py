@@ -62,31 +62,37 @@ WORKLOADS = {
                   desc='4,096 independent TC instances, directed Erdos-Renyi, n log-uniform in '
                        '[64, 1024], mean out-degree U[2,8], seed 1000+j; evaluated as one '
                        'disjoint union; index policy and options picked by the autotuner'),
+  'batched-wide': dict(plan='tc', rel='ArcInput', out='Path', kind='batched', tune=True,
+                       desc='the batched config\'s own 4,096 draws (n log-uniform in [64, 65,536], '
+                            'mean out-degree U[2,8], seed 1000+j), the instances with n <= '
+                            '{n_max}; evaluated in disjoint-union waves under a device-memory '
+                            'budget; options picked by the autotuner'),
 }
 
 BATCH_COUNT = 4096
 BATCH_N_HI = 1024
 PLAIN_SAMPLE_STRIDE = 16
+WIDE_N_MAX = 8192
 
 
 _BATCH = None
 
 
-def make_batch():
-  '''(instances, union) of the batched workload (generated once per process).'''
+def make_batch(name: str = 'batched', n_max: int = WIDE_N_MAX) -> list:
+  """Instances of a batched workload (generated once per process)."""
   global _BATCH
-  if _BATCH is None:
+  if _BATCH is None or _BATCH[0] != (name, n_max):
     from srdatalog_b200 import workloads as W
-    from srdatalog_b200.batch import make_union
-    insts = [{'ArcInput': e} for e in W.batched_instances(count=BATCH_COUNT, n_hi=BATCH_N_HI)]
-    _BATCH = (insts, make_union(insts))
-  return _BATCH
+    if name == 'batched':
+      es = W.batched_instances(count=BATCH_COUNT, n_hi=BATCH_N_HI)
+    else:
+      es = W.batched_instances(count=BATCH_COUNT, n_hi=65536, n_max=n_max)
+    _BATCH = ((name, n_max), [{'ArcInput': e} for e in es])
+  return _BATCH[1]
 
 
 def make_edges(name: str) -> np.ndarray:
   from srdatalog_b200 import workloads as W
-  if name == 'batched':
-    return make_batch()[1].inputs['ArcInput']
   cache = os.path.join('/tmp', f'srdl_bench_{name}.npy')
   if os.path.exists(cache):
     return np.load(cache)
@@ -110,8 +116,9 @@ def result_units(db, wl) -> int:
 
 
 def plain_loop(plan, insts, stride, stream_ptr, device):
-  '''The one-query-at-a-time loop: every sampled instance through its own
-  srdl_run on one handle (host rows, result size read back).'''
+  """The one-query-at-a-time loop: every sampled instance through its own
+  srdl_run on one handle (host rows, result size read back).  Returns the
+  rate, and per sampled instance its Path size and recursive iterations."""
   import torch
   from srdatalog_b200 import Database
   db = Database(plan, device=device)
@@ -123,16 +130,17 @@ def plain_loop(plan, insts, stride, stream_ptr, device):
     db.run()
   torch.cuda.synchronize()
   t0 = time.perf_counter()
-  sizes = []
+  sizes, iters = [], []
   for inst in sample:
     db.clear_inputs()
     db.load_rows('ArcInput', inst['ArcInput'])
     db.run()
     sizes.append(db.size('Path'))
+    iters.append([st['iterations'] for st in db.stats()['steps'] if st['recursive']])
   dt = time.perf_counter() - t0
   db.close()
   return {'queries_per_s': len(sample) / dt, 'ms_per_query': 1e3 * dt / len(sample),
-          'sample': f'every {stride}th of {len(insts)} instances ({len(sample)})'}, sizes
+          'sample': f'every {stride}th of {len(insts)} instances ({len(sample)})'}, sizes, iters
 
 
 class ClockSampler:
@@ -222,7 +230,7 @@ def hbm_peak():
     return FALLBACK_HBM_GBS, 'fallback'
 
 
-def cpu_baseline(wl_name: str, edges: np.ndarray) -> dict:
+def cpu_baseline(wl_name: str, edges, n_max: int = WIDE_N_MAX) -> dict:
   '''The oracle (CPU restatement of the reference's evaluation) on the host
   cores, on a bounded sample; returns tuples/s for the same metric.'''
   import oracle
@@ -240,15 +248,22 @@ def cpu_baseline(wl_name: str, edges: np.ndarray) -> dict:
     dt = time.perf_counter() - t0
     return {'value': len(reqs) / dt, 'unit': 'queries/s', 'cores': cores, 'kind': 'port',
             'sample': f'first 64 requests of the served stream, one at a time ({dt:.2f} s)'}
-  if wl_name == 'batched':
-    insts, _ = make_batch()
+  if wl_name in ('batched', 'batched-wide'):
+    # every 16th instance in order (sizes are drawn independently of the
+    # order), stopped after 20 s of CPU work
+    insts = make_batch(wl_name, n_max)
     sample = insts[::PLAIN_SAMPLE_STRIDE]
     t0 = time.perf_counter()
+    done = 0
     for inst in sample:
       oracle.tc(inst['ArcInput'])
+      done += 1
+      if time.perf_counter() - t0 > 20.0:
+        break
     dt = time.perf_counter() - t0
-    return {'value': len(sample) / dt, 'unit': 'queries/s', 'cores': cores, 'kind': 'port',
-            'sample': f'TC of every {PLAIN_SAMPLE_STRIDE}th instance ({len(sample)}), {dt:.2f} s'}
+    return {'value': done / dt, 'unit': 'queries/s', 'cores': cores, 'kind': 'port',
+            'sample': f'TC of the first {done} of every {PLAIN_SAMPLE_STRIDE}th instance '
+                      f'({len(sample)}), {dt:.2f} s'}
   if wl_name == 'triangle':
     t0 = time.perf_counter()
     c = oracle.triangle_count(edges)
@@ -272,10 +287,12 @@ def run_reference(args, rank, world):
   wl = WORKLOADS.get(args.workload, {'desc': SERVE_DESC})
   if rank != 0:
     return
-  edges = None if args.workload == 'served' else make_edges(args.workload)
+  if args.workload == 'batched-wide':
+    wl = dict(wl, desc=wl['desc'].format(n_max=args.batch_n_max))
+  edges = None if args.workload in ('served', 'batched', 'batched-wide') else make_edges(args.workload)
   vals = []
   for i in range(args.warmup + args.steps):
-    cb = cpu_baseline(args.workload, edges)
+    cb = cpu_baseline(args.workload, edges, args.batch_n_max)
     if i >= args.warmup:
       vals.append(cb['value'])
   v = statistics.median(vals)
@@ -488,6 +505,189 @@ def run_primitives(args, rank, world):
   report('set_difference', ms, 8 * (u + sub.numel() + nd), a=u, b=sub.numel(), result=nd)
 
 
+def run_batched(args, rank, world):
+  """Batched fixpoints: every instance of the workload per step, in
+  disjoint-union waves (srdatalog_b200.batch.WaveRun) under a device-memory
+  budget; queries/s against the one-query-at-a-time loop.  Every step
+  reads back each instance's Path size (checked against the plain loop on
+  a sample, iterations too).  N > 1: independent replicas (the instances
+  of a batch share nothing; no collective on the data path)."""
+  import torch
+  dist = None
+  if world > 1:
+    import datetime
+
+    import torch.distributed as dist
+    torch.cuda.set_device(local_of(world))
+    dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+  local = local_of(world)
+  dev = torch.device('cuda', local)
+  torch.cuda.set_device(dev)
+  from srdatalog_b200 import Database, native
+  from srdatalog_b200.batch import WaveRun, make_union
+  wl = dict(WORKLOADS[args.workload])
+  if args.workload == 'batched-wide':
+    wl['desc'] = wl['desc'].format(n_max=args.batch_n_max)
+  plan = load_plan(wl['plan'])
+  insts = make_batch(args.workload, args.batch_n_max)
+  k = len(insts)
+  stream = torch.cuda.current_stream(dev)
+  budget = int(args.batch_budget_gb * 1e9)
+  tuned = None
+  if wl.get('tune'):
+    # untimed: the autotuner times candidate settings on the union of all
+    # instances when they fit one run, else of the first instances whose
+    # closures (at most n^2 tuples each) add up to 3e8
+    from srdatalog_b200.autotune import autotune
+    sample, tot = [], 0
+    for inst in insts:
+      n = int(inst[wl['rel']].max()) + 1
+      if args.workload != 'batched' and sample and tot + n * n > 3e8:
+        break
+      sample.append(inst)
+      tot += n * n
+    tuned = autotune(plan, {wl['rel']: make_union(sample).inputs[wl['rel']]}, device=local, reps=2)
+    plan = tuned.apply(plan)
+  db = Database(plan, device=local)
+  if tuned:
+    tuned.configure(db)
+  db.set_stream(stream.cuda_stream)
+  db.set_profiling(True)
+  wr = WaveRun(plan, insts, db=db, budget_bytes=budget, sizes=[wl['out']])
+  kernels: dict = {}
+  collect = [False]
+
+  def on_wave(d):
+    if collect[0]:
+      for name, st in d.stats()['kernels'].items():
+        agg = kernels.setdefault(name, {'ms': 0.0, 'bytes': 0.0, 'units': 0.0, 'scopes': 0})
+        for f in agg:
+          agg[f] += st[f]
+
+  # first run from host rows settles the wave partition (splits if a wave
+  # outgrows the budget); then every wave's union is staged on the device
+  wr.run(on_wave=on_wave)
+  assert not wr.errors, wr.errors
+  unions = {tuple(w): make_union([insts[j] for j in w]) for w in wr.waves}
+  d_rows = {key: torch.from_numpy(u.inputs[wl['rel']].view(np.int32).reshape(-1)).to(dev)
+            for key, u in unions.items()}
+  rows_of = {id(u): d_rows[key] for key, u in unions.items()}
+
+  def union_of(wave):
+    return unions[tuple(wave)]
+
+  def load_dev(d, u):
+    t = rows_of[id(u)]
+    d.load_device_rows(wl['rel'], t.data_ptr(), t.numel() // 2)
+
+  flush = torch.empty(64 << 20, dtype=torch.int32, device=dev)  # 256 MB > 126 MB L2
+  for _ in range(args.warmup):
+    wr.run(union_of=union_of, load=load_dev, on_wave=on_wave)
+  want = wr.sizes[wl['out']].copy()
+  want_iters = {s: v.copy() for s, v in wr.iterations.items()}
+  waves_before = len(wr.waves)
+
+  def timed(load, tag):
+    ms = []
+    l0 = native.lib().srdl_launch_count()
+    for i in range(args.steps):
+      flush.fill_(i)
+      e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+      e0.record(stream)
+      wr.run(union_of=union_of, load=load, on_wave=on_wave)
+      e1.record(stream)
+      e1.synchronize()
+      ms.append(e0.elapsed_time(e1))
+      assert not wr.errors and len(wr.waves) == waves_before, tag
+      assert np.array_equal(wr.sizes[wl['out']], want), tag
+    return ms, native.lib().srdl_launch_count() - l0
+
+  if dist:
+    dist.barrier()
+  torch.cuda.synchronize(dev)
+  sampler = ClockSampler(local)
+  sampler.start()
+  collect[0] = True
+  step_ms, launches = timed(load_dev, 'device rows')
+  collect[0] = False
+  torch.cuda.synchronize(dev)
+  clocks = sampler.stop()
+  total_ms = max_over_ranks(sum(step_ms), dist, dev)
+  value = replica_throughput(k, args.steps, world, total_ms)
+  tuples = float(want.astype(np.float64).sum())
+
+  # e2e: the same waves from host rows (copied in every step), sizes read back
+  if dist:
+    dist.barrier()
+  e2e_ms, _ = timed(None, 'host rows')
+  e2e_total = max_over_ranks(sum(e2e_ms), dist, dev)
+  h2d = int(sum(u.inputs[wl['rel']].nbytes for u in unions.values()))
+  plain = None
+  if not args.no_cpu_baseline:
+    plain, sizes, iters = plain_loop(plan, insts, PLAIN_SAMPLE_STRIDE, stream.cuda_stream, local)
+    assert [int(x) for x in want[::PLAIN_SAMPLE_STRIDE]] == sizes
+    rec = sorted(want_iters)
+    assert all([int(want_iters[s][j]) for s in rec] == it
+               for j, it in zip(range(0, k, PLAIN_SAMPLE_STRIDE), iters)), 'iterations differ'
+  stats = db.stats()
+  db.close()
+  if dist:
+    dist.barrier()
+    dist.destroy_process_group()
+  if rank != 0:
+    return
+  top = max(kernels.items(), key=lambda kv: kv[1]['ms'])
+  name, kk = top
+  peak, peak_kind = hbm_peak()
+  achieved = (kk['bytes'] / (kk['ms'] / 1e3)) / 1e9 if kk['ms'] else 0.0
+  roof = {'bound': 'hbm', 'kernel': name, 'achieved': achieved, 'peak': peak,
+          'peak_source': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
+          'traffic': None, 'traffic_source': None,
+          'bytes_per_launch': kk['bytes'] / max(1, kk['scopes']),
+          'ms_per_launch': kk['ms'] / max(1, kk['scopes']),
+          'share_of_step': kk['ms'] / total_ms if world == 1 else None}
+  line = {
+    'metric': f'queries/s ({args.workload})', 'value': value, 'unit': 'queries/s', 'n_gpus': world,
+    'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
+    'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'u32',
+    'data': 'synthetic',
+    'config': {'workload': wl['desc'], 'instances': k,
+               'edges': int(sum(i['ArcInput'].shape[0] for i in insts)),
+               'path_tuples_per_step': int(tuples),
+               'tuples_per_s': tuples * args.steps * world / (total_ms / 1e3),
+               'waves': len(wr.waves), 'wave_splits': wr.splits,
+               'budget_bytes': budget, 'peak_bytes': wr.peak_bytes,
+               'bytes_per_bound_tuple': wr.bytes_per_bound,
+               'device_loop': stats.get('device_loop'),
+               'parallelism': f'replicas{world}',
+               'l2': 'flushed between steps (256 MB write)',
+               'inputs': 'HBM-resident for value; host rows for e2e'},
+    'e2e': {'value': replica_throughput(k, args.steps, world, e2e_total), 'unit': 'queries/s',
+            'ms_per_step': e2e_total / args.steps, 'h2d_bytes_per_step': h2d,
+            'd2h_bytes_per_step': 8 * k, 'step_ms': [round(x, 3) for x in e2e_ms]},
+    'step_ms': [round(x, 3) for x in step_ms],
+    'gpu_launches': int(launches),
+    'roofline': roof,
+    'kernels': {k2: {'ms_per_step': v['ms'] / args.steps,
+                     'gbs': (v['bytes'] / (v['ms'] / 1e3) / 1e9) if v['ms'] else 0.0}
+                for k2, v in sorted(kernels.items(), key=lambda kv: -kv[1]['ms'])},
+    'clocks': clocks,
+  }
+  if tuned:
+    line['config']['autotuned'] = dict(tuned.to_json(), trials=len(tuned.trials))
+  if plain:
+    line['plain_loop'] = plain
+    line['speedup_vs_plain_loop'] = value / plain['queries_per_s']
+  if world == 1 and not args.no_cpu_baseline:
+    line['cpu_baseline'] = cpu_baseline(args.workload, None, args.batch_n_max)
+  print(json.dumps(line), flush=True)
+
+
+def local_of(world: int) -> int:
+  import torch
+  return int(os.environ.get('LOCAL_RANK', '0')) % max(1, torch.cuda.device_count())
+
+
 def main():
   ap = argparse.ArgumentParser()
   ap.add_argument('--gpus', type=int, default=1)
@@ -504,6 +704,10 @@ def main():
                   help='served: largest request (input edges) that is unioned with others')
   ap.add_argument('--serve-max-batch', type=int, default=16,
                   help='served: most requests evaluated as one union')
+  ap.add_argument('--batch-n-max', type=int, default=WIDE_N_MAX,
+                  help='batched-wide: the config instances with at most this many nodes')
+  ap.add_argument('--batch-budget-gb', type=float, default=120.0,
+                  help='batched: device memory one wave may hold')
   ap.add_argument('--no-cpu-baseline', action='store_true')
   ap.add_argument('--quick', action='store_true',
                   help='kernel-resident path only (no e2e, no CPU baseline): for profiler runs')
@@ -519,6 +723,8 @@ def main():
     return run_served(args, rank, world)
   if args.workload == 'primitives':
     return run_primitives(args, rank, world)
+  if WORKLOADS[args.workload]['kind'] == 'batched':
+    return run_batched(args, rank, world)
 
   import torch
   dist = None
@@ -586,15 +792,9 @@ def main():
     db.run()
     job_units(db)
   units = job_units(db)
-  batched = wl['kind'] == 'batched'
-  if batched:  # one step answers every instance: the metric counts queries
-    insts, union = make_batch()
-    bounds = union.offsets.astype(np.uint32)
-    per_step = len(insts)
-  else:
-    per_step = units
-  metric_name = f'{"queries" if batched else "tuples"}/s ({args.workload})'
-  unit_name = 'queries/s' if batched else 'tuples/s'
+  per_step = units
+  metric_name = f'tuples/s ({args.workload})'
+  unit_name = 'tuples/s'
   kernels: dict = {}
   step_ms = []
   launches = 0
@@ -656,12 +856,6 @@ def main():
     ev0.record(stream)
     db2.run()
     got = job_units(db2)  # result read back to the host (summed over shards)
-    if batched:  # every instance's size read back
-      per_inst = db2.range_counts(wl['out'], bounds)
-      if sharded:
-        t = torch.from_numpy(per_inst.astype(np.int64)).to(coll)
-        dist.all_reduce(t)
-        per_inst = t.cpu().numpy()
     ev1.record(stream)
     ev1.synchronize()
     e2e_ms.append(ev0.elapsed_time(ev1))
@@ -669,12 +863,6 @@ def main():
   e2e_total = sum(e2e_ms)
   e2e_total = max_over_ranks(e2e_total, dist, coll)
   db2.close()
-  plain = None
-  if batched and not args.no_cpu_baseline:
-    # the one-query-at-a-time loop on a sample, checked instance by instance
-    plain, sizes = plain_loop(plan, insts, PLAIN_SAMPLE_STRIDE, stream.cuda_stream, local)
-    assert [int(x) for x in per_inst[::PLAIN_SAMPLE_STRIDE]] == sizes
-
   if dist:
     dist.barrier()
     dist.destroy_process_group()
@@ -715,7 +903,7 @@ def main():
                'inputs': 'HBM-resident for value; pinned host rows for e2e'},
     'e2e': {'value': replica_throughput(per_step, args.steps, copies, e2e_total), 'unit': unit_name,
             'ms_per_step': e2e_total / args.steps, 'h2d_bytes_per_step': int(n) * 8,
-            'd2h_bytes_per_step': 8 + (8 * per_step if batched else 0),
+            'd2h_bytes_per_step': 8,
             'step_ms': [round(x, 3) for x in e2e_ms]},
     'step_ms': [round(x, 3) for x in step_ms],
     'gpu_launches': int(launches),
@@ -726,9 +914,6 @@ def main():
     'iterations': [s['iterations'] for s in stats['steps']],
     'clocks': clocks,
   }
-  if batched:
-    line['config'].update(instances=per_step,
-                          tuples_per_s=units * args.steps * copies / (total_ms / 1e3))
   if sharded:
     line['config']['sharding'] = {'partitioned': spec.partitioned,
                                   'rules': {r: m for r, m in spec.modes.items() if m},
@@ -737,9 +922,6 @@ def main():
     line['config']['sharding'] = {'replicas': spec.fallback or 'nothing to split'}
   if tuned:
     line['config']['autotuned'] = dict(tuned.to_json(), trials=len(tuned.trials))
-    if plain:
-      line['plain_loop'] = plain
-      line['speedup_vs_plain_loop'] = value / plain['queries_per_s']
   if world == 1 and not args.no_cpu_baseline:
     line['cpu_baseline'] = cpu_baseline(args.workload, edges)
   print(json.dumps(line), flush=True)

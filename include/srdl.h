@@ -170,6 +170,28 @@ int srdl_clear_inputs(srdl_db* db);
 int srdl_range_counts(srdl_db* db, const char* rel, const uint32_t* bounds, uint64_t n_bounds,
                       uint64_t* counts);
 
+/* Instances of a batched run: instance j owns the values [bounds[j],
+ * bounds[j+1]) (host array, non-decreasing, n_bounds = instances + 1; 0
+ * clears).  Every later srdl_run records on the device, for each recursive
+ * step whose computed relations are binary, the iterations each instance's
+ * own run would take (its last iteration with a non-empty delta, plus one,
+ * capped at the step's iterations).  No reference counterpart. */
+int srdl_set_instances(srdl_db* db, const uint32_t* bounds, uint64_t n_bounds);
+
+/* Per-instance iterations of plan step `step` in the last run (out: one
+ * uint32 per instance).  Non-recursive steps give 1.  Status 7 when the
+ * step was not recorded (a computed relation is not binary). */
+int srdl_instance_iterations(srdl_db* db, uint64_t step, uint32_t* out, uint64_t n_instances);
+
+/* Per-range fingerprints of FULL(rel), a binary relation: sums[j] = the sum
+ * mod 2^64, over its rows (x, y) with bounds[j] <= x < bounds[j+1], of
+ * m(x - bounds[j] ^ 0x243F6A8885A308D3) * m(y - bounds[j] ^
+ * 0x13198A2E03707344), m the SplitMix64 output function.  An order-free
+ * digest of each instance's rows in its own values.  No reference
+ * counterpart. */
+int srdl_range_checksums(srdl_db* db, const char* rel, const uint32_t* bounds, uint64_t n_bounds,
+                         uint64_t* sums);
+
 /* Rows currently staged for `rel` by the load calls (host-side count). */
 uint64_t srdl_staged_rows(srdl_db* db, const char* rel);
 

@@ -160,6 +160,166 @@ def dump_hash(rows: np.ndarray) -> str:
 
 
 # ---------------------------------------------------------------------------
+# Order-free fingerprints of binary relations (batched runs)
+# ---------------------------------------------------------------------------
+#
+# The library reports, per instance of a batched run, the sum mod 2^64 of
+# fx(x) * fy(y) over the instance's rows (x, y) in its own values
+# (srdl_range_checksums), fx(v) = m(v ^ 0x243F6A8885A308D3), fy(v) = m(v ^
+# 0x13198A2E03707344), m the SplitMix64 output function.  Because the sum is
+# bilinear, a transitive closure's fingerprint is the sum over sources x of
+# fx(x) * (sum of fy over x's reachability set), which
+# `tc_closure_fingerprint` computes from strongly connected components
+# without listing the |Path| pairs (up to ~4*10^9 for one instance of the
+# batched config) -- an exact check of instances the semi-naive
+# restatement above is too slow for.
+
+def _splitmix64(v: np.ndarray) -> np.ndarray:
+  '''SplitMix64 output function (Steele, Lea and Flood, OOPSLA 2014;
+  Vigna's splitmix64.c constants), elementwise on uint64 (wrapping).'''
+  z = np.asarray(v, np.uint64).copy()
+  with np.errstate(over='ignore'):
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def fp_x(v) -> np.ndarray:
+  return _splitmix64(np.asarray(v, np.uint64) ^ np.uint64(0x243F6A8885A308D3))
+
+
+def fp_y(v) -> np.ndarray:
+  return _splitmix64(np.asarray(v, np.uint64) ^ np.uint64(0x13198A2E03707344))
+
+
+def _wsum(a: np.ndarray) -> int:
+  '''Sum of uint64 values mod 2^64.'''
+  with np.errstate(over='ignore'):
+    return int(np.sum(np.asarray(a, np.uint64), dtype=np.uint64))
+
+
+def row_fingerprint(rows: np.ndarray) -> int:
+  '''Fingerprint of a set of (x, y) rows (uint32, declared column order).'''
+  r = np.asarray(rows, np.uint32).reshape(-1, 2)
+  if not r.shape[0]:
+    return 0
+  with np.errstate(over='ignore'):
+    return _wsum(fp_x(r[:, 0]) * fp_y(r[:, 1]))
+
+
+def tc_closure_fingerprint(edges: np.ndarray, n: int | None = None) -> tuple:
+  '''(|Path|, fingerprint of Path) for Path = the pairs (x, y) joined by a
+  path of one or more edges -- the least fixpoint of the TC program
+  (Path(x,y) <= Edge(x,y); Path(x,z) <= Path(x,y), Edge(y,z)) -- by
+  strongly connected components (Tarjan 1972 via scipy) and their
+  condensation in reverse topological order.  R(S), the nodes reachable in
+  one or more steps from a component S, is S itself when S has a cycle,
+  plus (T u R(T)) for every successor T.  The largest component C is kept
+  implicit: R(S) = [R(C) if S reaches C] + an explicit set of the other
+  nodes, which stays small on graphs with one giant component.'''
+  import scipy.sparse as sp
+  from scipy.sparse.csgraph import breadth_first_order, connected_components
+  e = np.asarray(edges, np.int64).reshape(-1, 2)
+  if n is None:
+    n = int(e.max()) + 1 if e.shape[0] else 0
+  if not e.shape[0]:
+    return 0, 0
+  g = sp.csr_matrix((np.ones(e.shape[0], np.int8), (e[:, 0], e[:, 1])), shape=(n, n))
+  ncomp, lab = connected_components(g, directed=True, connection='strong')
+  lab = lab.astype(np.int64)
+  size = np.bincount(lab, minlength=ncomp)
+  selfloop = np.zeros(ncomp, bool)
+  sl = e[:, 0] == e[:, 1]
+  selfloop[lab[e[sl, 0]]] = True
+  cyclic = (size > 1) | selfloop
+  members = [[] for _ in range(ncomp)]
+  order = np.argsort(lab, kind='stable')
+  cuts = np.searchsorted(lab[order], np.arange(ncomp + 1))
+  for c in range(ncomp):
+    members[c] = order[cuts[c]:cuts[c + 1]]
+  # condensation edges, deduplicated
+  cs, cd = lab[e[:, 0]], lab[e[:, 1]]
+  keep = cs != cd
+  dag = np.unique(cs[keep] * ncomp + cd[keep])
+  ds, dd = dag // ncomp, dag % ncomp
+  succ_cut = np.searchsorted(ds, np.arange(ncomp + 1))
+  # reverse topological order (Kahn on the reversed condensation)
+  outdeg = np.diff(succ_cut).astype(np.int64)
+  pred_order = np.argsort(dd, kind='stable')
+  pred_src = ds[pred_order]
+  pred_cut = np.searchsorted(dd[pred_order], np.arange(ncomp + 1))
+  stack = list(np.nonzero(outdeg == 0)[0])
+  rev_topo = []
+  while stack:
+    c = stack.pop()
+    rev_topo.append(c)
+    for p in pred_src[pred_cut[c]:pred_cut[c + 1]]:
+      outdeg[p] -= 1
+      if outdeg[p] == 0:
+        stack.append(p)
+  hub = int(np.argmax(size))
+  fy_all = fp_y(np.arange(n, dtype=np.uint64))
+  if cyclic[hub]:
+    reach_hub = breadth_first_order(g, int(members[hub][0]), directed=True, return_predecessors=False)
+    in_hub = np.zeros(n, bool)
+    in_hub[reach_hub] = True
+    hub_size, hub_g = int(reach_hub.shape[0]), _wsum(fy_all[reach_hub])
+  else:
+    in_hub = np.zeros(n, bool)
+    hub_size, hub_g = 0, 0
+  flag = np.zeros(ncomp, bool)        # R(S) includes R(hub)
+  explicit = [None] * ncomp           # the rest of R(S)
+  comp_size = np.zeros(ncomp, np.int64)
+  comp_g = np.zeros(ncomp, np.uint64)
+  empty = frozenset()
+  for c in rev_topo:
+    if c == hub and cyclic[hub]:
+      flag[c], explicit[c] = True, empty
+    else:
+      f = False
+      parts = []
+      for t in dd[succ_cut[c]:succ_cut[c + 1]]:
+        f = f or bool(flag[t]) or (t == hub and cyclic[hub])
+        parts.append(members[t])
+        if explicit[t]:
+          parts.append(np.fromiter(explicit[t], np.int64, len(explicit[t])))
+      if cyclic[c]:
+        parts.append(members[c])
+      if parts:
+        s = np.unique(np.concatenate(parts))
+        if f:
+          s = s[~in_hub[s]]
+        ex = frozenset(s.tolist())
+      else:
+        ex = empty
+      flag[c], explicit[c] = f, ex
+    ex = explicit[c]
+    comp_size[c] = (hub_size if flag[c] else 0) + len(ex)
+    g_ex = _wsum(fy_all[np.fromiter(ex, np.int64, len(ex))]) if ex else 0
+    comp_g[c] = np.uint64(((hub_g if flag[c] else 0) + g_ex) & 0xFFFFFFFFFFFFFFFF)
+  total = int(np.sum(comp_size[lab]))
+  with np.errstate(over='ignore'):
+    fpr = _wsum(fp_x(np.arange(n, dtype=np.uint64)) * comp_g[lab])
+  return total, fpr
+
+
+def _tc_fp_job(job):
+  return tc_closure_fingerprint(*job)
+
+
+def tc_closure_fingerprints(jobs: list, workers: int = 0) -> list:
+  """tc_closure_fingerprint over [(edges, n), ...] in a pool of processes
+  started with spawn (safe after the caller has used a GPU)."""
+  import concurrent.futures as cf
+  import multiprocessing as mp
+  workers = workers or min(16, os.cpu_count() or 1)
+  if workers <= 1 or len(jobs) < 8:
+    return [tc_closure_fingerprint(*j) for j in jobs]
+  with cf.ProcessPoolExecutor(workers, mp_context=mp.get_context('spawn')) as ex:
+    return list(ex.map(_tc_fp_job, jobs, chunksize=16))
+
+
+# ---------------------------------------------------------------------------
 # Generic pure-Python plan interpreter (tiny inputs only)
 # ---------------------------------------------------------------------------
 

@@ -235,6 +235,22 @@ int srdl_range_counts(srdl_db* h, const char* rel, const uint32_t* bounds, uint6
   SRDL_GUARD(0, h->db->range_counts(rel, bounds, n_bounds, counts); return 0;)
 }
 
+int srdl_set_instances(srdl_db* h, const uint32_t* bounds, uint64_t n_bounds) {
+  if (!h || (n_bounds && !bounds)) return kErrArg;
+  SRDL_GUARD(0, h->db->set_instances(bounds, n_bounds); return 0;)
+}
+
+int srdl_instance_iterations(srdl_db* h, uint64_t step, uint32_t* out, uint64_t n_instances) {
+  if (!h || (n_instances && !out)) return kErrArg;
+  SRDL_GUARD(0, h->db->instance_iterations(step, out, n_instances); return 0;)
+}
+
+int srdl_range_checksums(srdl_db* h, const char* rel, const uint32_t* bounds, uint64_t n_bounds,
+                         uint64_t* sums) {
+  if (!h || !rel || (n_bounds > 1 && !sums)) return kErrArg;
+  SRDL_GUARD(0, h->db->range_checksums(rel, bounds, n_bounds, sums); return 0;)
+}
+
 uint64_t srdl_staged_rows(srdl_db* h, const char* rel) {
   if (!h || !rel || !h->db->has_rel(rel)) return 0;
   return h->db->staged_rows(rel);

@@ -169,6 +169,8 @@ struct DedupDiffSel {
   const uint64_t* head = nullptr;
   uint64_t n_head = 0;
   const uint64_t* d_n_full = nullptr;  // device loop: FULL's count on the device (n_full = capacity)
+  uint64_t out_cap = ~0ull;             // device loop: room in `out`; a key past it raises *d_overflow
+  unsigned int* d_overflow = nullptr;
 
   __device__ __forceinline__ uint64_t expand(K c) const {
     if (sizeof(K) == 8 && bits == 32) return (uint64_t)c;
@@ -202,7 +204,10 @@ struct DedupDiffSel {
   }
   using value_type = uint64_t;
   __device__ uint64_t value(uint64_t i) const { return expand(a[i]); }
-  __device__ void store(uint64_t pos, uint64_t v) const { out[pos] = v; }
+  __device__ void store(uint64_t pos, uint64_t v) const {
+    if (pos < out_cap) out[pos] = v;
+    else if (d_overflow) *d_overflow = 1u;
+  }
 };
 
 // FULL position of every tile boundary: fpos[t] = lower_bound(FULL, first key

@@ -813,6 +813,7 @@ void Database::run_steps(uint64_t max_iters) {
   reset_alloc_max();
   const AllocStats a0 = alloc_stats();
   upload_inputs();
+  instances_begin();
   {
     OpStats& u = opstats_["upload_inputs"];
     u.ms = u.max_ms =
@@ -850,7 +851,9 @@ void Database::run_steps(uint64_t max_iters) {
           if (loop_on && entries < 3) {
             entries++;
             uint64_t done = 0;
+            loop_marks_ = instance_marks(si);
             const int rc = run_device_loop(st, it, max_iters, &done);
+            loop_marks_ = nullptr;
             step_stats_[si].iterations += done;
             it += done;
             if (rc == kLoopDone) break;
@@ -859,11 +862,19 @@ void Database::run_steps(uint64_t max_iters) {
           }
         }
         exec_ops(st, it);
+        mark_instances(si, st, (uint32_t)(it + 1));
         step_stats_[si].iterations++;
       }
+      instances_end(si, step_stats_[si].iterations);
       // Post-stratum reconstruct: every LSM relation ends as one FULL array.
       for (auto& kv : rels_)
         if (kv.second->head.n) compact_head(*kv.second);
+      // the final FULL sizes size the device loop's buffers in later runs
+      for (auto& n : computed) {
+        Relation& r = rel(n);
+        auto fit = r.v[kFull].idx.find(r.canonical);
+        if (fit != r.v[kFull].idx.end()) full_max_[n] = std::max(full_max_[n], fit->second.n);
+      }
     }
     SRDL_CUDA(cudaStreamSynchronize(L_.stream));
     step_stats_[si].ms =

@@ -101,10 +101,13 @@ void warm_merge_kernels();
 
 // sort_dedup with the input count on the device (device loop): `cap` keys of
 // room in `in`, *d_n present; FULL (room full_cap, count *d_n_full, may be
-// null) is subtracted.  No host decision depends on the counts.
+// null) is subtracted; `out` has room for out_cap keys (more kept keys
+// raise *d_overflow and are not written; *d_nout is still the full count).
+// No host decision depends on the counts.
 void sort_dedup_dev(const Launch& L, const uint64_t* in, uint64_t cap, const uint64_t* d_n,
                     int bits, const uint64_t* full, uint64_t full_cap, const uint64_t* d_n_full,
-                    uint64_t* out, uint64_t* d_nout, Scratch& s);
+                    uint64_t* out, uint64_t out_cap, uint64_t* d_nout, unsigned int* d_overflow,
+                    Scratch& s);
 
 // Trie view pieces for a sorted unique key array (with d_n: n is a capacity
 // and the count is on the device).
@@ -139,6 +142,13 @@ void child_hash_plan(const Launch& L, const uint32_t* dir, uint32_t dir_n, uint3
 void child_hash_build(const Launch& L, const uint64_t* keys, uint64_t n, const uint32_t* dir,
                       uint32_t dir_n, const uint64_t* sizes, const uint64_t* offs, uint32_t* hdir,
                       uint32_t* pool);
+
+// last[j] = max(last[j], base + *iter_dev) for every instance j (values
+// [bounds[j], bounds[j+1]), j < k) with a key in the sorted keys[0..n), n =
+// min(*n_dev, cap) when n_dev is given, else cap; iter_dev may be null.
+void instance_mark(const Launch& L, const uint64_t* keys, uint64_t cap, const uint64_t* n_dev,
+                   const uint32_t* bounds, uint32_t k, uint32_t base, const unsigned long long* iter_dev,
+                   uint32_t* last);
 
 // pos[j] = first row of the sorted keys whose high word is >= bounds[j].
 void bounds_positions(const Launch& L, const uint64_t* keys, uint64_t n, const uint32_t* bounds,

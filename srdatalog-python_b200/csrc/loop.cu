@@ -100,7 +100,7 @@ uint64_t round_cap(uint64_t n) {
 // Buffers of one relation the step computes.
 struct LoopRel {
   Relation* r = nullptr;
-  uint64_t cap_new = 0, cap_full = 0;
+  uint64_t cap_new = 0, cap_delta = 0, cap_full = 0;  // raw NEW, DELTA (<= cap_new), FULL
   int producers = 0;  // execute ops inserting into it
   DevBuf newk, sort_scr, trie_scr;
   DevBuf full[2], delta[2], lo[2], roots[2], dir[2];
@@ -229,14 +229,20 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
       Index& f = ensure_index(r, kFull, r.canonical);  // merges a Device2LevelIndex HEAD
       auto dit = r.v[kDelta].idx.find(r.canonical);
       const uint64_t dn = dit == r.v[kDelta].idx.end() ? 0 : dit->second.n;
-      // room: twice the largest NEW seen; FULL's final size seen before plus
-      // an eighth, or the current FULL plus two NEW rooms
+      // room: twice the largest NEW (before dedup) and DELTA seen; FULL's
+      // final size seen before plus an eighth, or the current FULL plus
+      // four DELTA rooms (overflows redo an iteration on the host path and
+      // re-enter with the sizes it measured)
       const uint64_t seen_new = std::max(new_max_[name], dn);
+      const uint64_t seen_delta = std::max(delta_max_[name], dn);
       lr.cap_new = round_cap(std::max<uint64_t>(2 * seen_new, 1 << 16));
-      lr.cap_full = round_cap(std::max<uint64_t>(full_max_[name] + full_max_[name] / 8, f.n + 2 * lr.cap_new));
+      lr.cap_delta = std::min(lr.cap_new, round_cap(std::max<uint64_t>(2 * seen_delta, 1 << 16)));
+      lr.cap_full =
+          round_cap(std::max<uint64_t>(full_max_[name] + full_max_[name] / 8, f.n + 4 * lr.cap_delta));
       if (opt_loop_cap_limit_) {
         // smaller capacities than the counts seen (tests of the overflow path)
         lr.cap_new = std::max<uint64_t>(std::min(lr.cap_new, opt_loop_cap_limit_), dn + 1);
+        lr.cap_delta = std::min(lr.cap_new, std::max<uint64_t>(std::min(lr.cap_delta, opt_loop_cap_limit_), dn + 1));
         lr.cap_full = std::max<uint64_t>(std::min(lr.cap_full, 16 * opt_loop_cap_limit_), f.n + 1);
       }
       for (const Op* op : execs)
@@ -245,8 +251,8 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
       {
         // the buffers below; leave the step to the host path rather than
         // take most of the free memory (the host path needs far less)
-        const uint64_t need = lr.cap_new * (8 + 16 + 16) + sort_dev_scratch_bytes(lr.cap_new, lr.cap_full, bits_) +
-                              lr.cap_full * 16;
+        const uint64_t need = lr.cap_new * 8 + lr.cap_delta * (16 + 8 + 8) +
+                              sort_dev_scratch_bytes(lr.cap_new, lr.cap_full, bits_) + lr.cap_full * 16;
         size_t free_b = 0, total_b = 0;
         SRDL_CUDA(cudaMemGetInfo(&free_b, &total_b));
         const ArenaUse au = arena_use(L_.stream);
@@ -256,12 +262,12 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
       }
       lr.newk = DevBuf(lr.cap_new * 8, L_.stream);
       lr.sort_scr = DevBuf(sort_dev_scratch_bytes(lr.cap_new, lr.cap_full, bits_), L_.stream);
-      lr.trie_scr = DevBuf(roots_scratch_bytes(lr.cap_new) + 1024, L_.stream);
+      lr.trie_scr = DevBuf(roots_scratch_bytes(lr.cap_delta) + 1024, L_.stream);
       for (int q = 0; q < 2; q++) {
         lr.full[q] = DevBuf(lr.cap_full * 8, L_.stream);
-        lr.delta[q] = DevBuf(lr.cap_new * 8, L_.stream);
-        lr.lo[q] = DevBuf(lr.cap_new * 4, L_.stream);
-        lr.roots[q] = DevBuf(lr.cap_new * 4, L_.stream);
+        lr.delta[q] = DevBuf(lr.cap_delta * 8, L_.stream);
+        lr.lo[q] = DevBuf(lr.cap_delta * 4, L_.stream);
+        lr.roots[q] = DevBuf(lr.cap_delta * 4, L_.stream);
         lr.dir[q] = DevBuf((size_t)X.dir_n * 4, L_.stream);
       }
       X.rels.push_back(std::move(lr));
@@ -321,10 +327,10 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
       SRDL_CUDA(cudaMemcpyAsync(lr.delta[0].as<void>(), dit->second.keys.as<void>(), dn * 8,
                                 cudaMemcpyDeviceToDevice, L_.stream));
     Scratch ts{lr.trie_scr.as<char>(), lr.trie_scr.bytes(), 0};
-    build_lo(L_, lr.delta[0].as<uint64_t>(), lr.cap_new, lr.lo[0].as<uint32_t>(), &c->n_delta[0]);
-    build_roots(L_, lr.delta[0].as<uint64_t>(), lr.cap_new, lr.roots[0].as<uint32_t>(), &c->n_roots[0], ts,
+    build_lo(L_, lr.delta[0].as<uint64_t>(), lr.cap_delta, lr.lo[0].as<uint32_t>(), &c->n_delta[0]);
+    build_roots(L_, lr.delta[0].as<uint64_t>(), lr.cap_delta, lr.roots[0].as<uint32_t>(), &c->n_roots[0], ts,
                 &c->n_delta[0]);
-    build_dir(L_, lr.delta[0].as<uint64_t>(), lr.cap_new, lr.dir[0].as<uint32_t>(), X.dir_n,
+    build_dir(L_, lr.delta[0].as<uint64_t>(), lr.cap_delta, lr.dir[0].as<uint32_t>(), X.dir_n,
               &c->n_delta[0]);
   }
   {
@@ -349,7 +355,7 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
       t.roots = lr.roots[p].as<uint32_t>();
       t.dir = lr.dir[p].as<uint32_t>();
       t.dir_n = X.dir_n;
-      t.n = lr.cap_new;
+      t.n = lr.cap_delta;
       t.n_roots_d = &cnt[i].n_roots[p];
       t.arity = 2;
       dv[lr.r->name] = t;
@@ -441,16 +447,23 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
       Scratch ss{lr.sort_scr.as<char>(), lr.sort_scr.bytes(), 0};
       // DELTA = unique(NEW) - FULL, FULL' = FULL U DELTA, DELTA's trie view
       sort_dedup_dev(L_, lr.newk.as<uint64_t>(), lr.cap_new, &c->n_new, bits_, lr.full[p].as<uint64_t>(),
-                     lr.cap_full, &c->n_full[p], lr.delta[1 - p].as<uint64_t>(), &c->n_delta[1 - p], ss);
+                     lr.cap_full, &c->n_full[p], lr.delta[1 - p].as<uint64_t>(), lr.cap_delta, &c->n_delta[1 - p],
+                     ovf, ss);
       merge_disjoint_dev(L_, lr.full[p].as<uint64_t>(), lr.cap_full, &c->n_full[p],
-                         lr.delta[1 - p].as<uint64_t>(), lr.cap_new, &c->n_delta[1 - p],
+                         lr.delta[1 - p].as<uint64_t>(), lr.cap_delta, &c->n_delta[1 - p],
                          lr.full[1 - p].as<uint64_t>(), lr.cap_full, &c->n_full[1 - p], ovf);
       Scratch ts{lr.trie_scr.as<char>(), lr.trie_scr.bytes(), 0};
-      build_lo(L_, lr.delta[1 - p].as<uint64_t>(), lr.cap_new, lr.lo[1 - p].as<uint32_t>(), &c->n_delta[1 - p]);
-      build_roots(L_, lr.delta[1 - p].as<uint64_t>(), lr.cap_new, lr.roots[1 - p].as<uint32_t>(),
+      build_lo(L_, lr.delta[1 - p].as<uint64_t>(), lr.cap_delta, lr.lo[1 - p].as<uint32_t>(), &c->n_delta[1 - p]);
+      build_roots(L_, lr.delta[1 - p].as<uint64_t>(), lr.cap_delta, lr.roots[1 - p].as<uint32_t>(),
                   &c->n_roots[1 - p], ts, &c->n_delta[1 - p]);
-      build_dir(L_, lr.delta[1 - p].as<uint64_t>(), lr.cap_new, lr.dir[1 - p].as<uint32_t>(), X.dir_n,
+      build_dir(L_, lr.delta[1 - p].as<uint64_t>(), lr.cap_delta, lr.dir[1 - p].as<uint32_t>(), X.dir_n,
                 &c->n_delta[1 - p]);
+      // batched runs: the instances with a delta row in this iteration
+      // (its number is it0 + 1 + the bodies started before it)
+      if (loop_marks_)
+        instance_mark(L_, lr.delta[1 - p].as<uint64_t>(), lr.cap_delta, &c->n_delta[1 - p],
+                      inst_bounds_d_.as<uint32_t>(), (uint32_t)(inst_bounds_.size() - 1), (uint32_t)(it0 + 1),
+                      &X.ctl_d()->bodies, loop_marks_);
     }
     const int ks = 2 * bits_ <= 32 ? 4 : 8;
     const int maxw = L_.radix_bits >= 1 && L_.radix_bits <= 8 ? L_.radix_bits : 8;
@@ -613,7 +626,11 @@ int Database::run_device_loop(const Step& st, uint64_t it0, uint64_t max_iters, 
     loop_stats_.overflows++;
     // the host path redoes the failed iteration and measures the counts
     // that were too large; the next entry sizes from at least twice these
-    for (auto& lr : X.rels) new_max_[lr.r->name] = std::max(new_max_[lr.r->name], lr.cap_new);
+    for (auto& lr : X.rels) {
+      new_max_[lr.r->name] = std::max(new_max_[lr.r->name], lr.cap_new);
+      delta_max_[lr.r->name] = std::max(delta_max_[lr.r->name], lr.cap_delta);
+      full_max_[lr.r->name] = std::max(full_max_[lr.r->name], lr.cap_full);
+    }
     for (size_t k = 0; k < execs.size(); k++) {
       std::vector<uint64_t>& seen = level_max_[execs[k]];
       for (size_t li = 0; li < seen.size() && li < X.pipes[k].size(); li++)

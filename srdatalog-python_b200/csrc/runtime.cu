@@ -278,8 +278,13 @@ Database::~Database() {
     for (auto& kv : rels_)
       for (auto& v : kv.second->v) v.clear();
     for (auto& kv : rels_) kv.second->pending = Index{};
+    for (auto& kv : rels_) kv.second->head = Index{};
     for (auto& kv : rels_) kv.second->dstaged.reset();
     d_small_.reset();
+    // (every buffer of the stream's arena goes back before it closes: a
+    // block returned later would be freed on the destroyed stream)
+    inst_last_.clear();
+    inst_bounds_d_.reset();
     arena_detach(L_.stream);
     cudaStreamSynchronize(L_.stream);
     if (h_small_) cudaFreeHost(h_small_);
@@ -294,6 +299,7 @@ Database::~Database() {
     for (auto e : loop_ev_)
       if (e) cudaEventDestroy(e);
     if (own_stream_) cudaStreamDestroy(L_.stream);
+    (void)cudaGetLastError();  // teardown errors must not surface in a later call
   }
 }
 
@@ -648,7 +654,10 @@ void Database::range_counts(const std::string& name, const uint32_t* bounds, uin
     return;
   }
   SRDL_CUDA(cudaSetDevice(device_));
-  Index& ix = ensure_index(r, kFull, identity_perm(r.arity));
+  if (r.head.n) compact_head(r);
+  // a binary relation's two columns lie in the same range, so any FULL
+  // permutation's high word tells the range (no extra permutation sorted)
+  Index& ix = r.arity == 2 ? binary_full_index(r, nullptr) : ensure_index(r, kFull, identity_perm(r.arity));
   DevBuf d_bounds(n_bounds * 4, L_.stream);
   DevBuf d_pos(n_bounds * 8, L_.stream);
   SRDL_CUDA(cudaMemcpyAsync(d_bounds.as<void>(), bounds, n_bounds * 4, cudaMemcpyHostToDevice,

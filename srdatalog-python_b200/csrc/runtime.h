@@ -258,6 +258,16 @@ class Database {
   // [bounds[j], bounds[j+1]), for j < n_bounds - 1.
   void range_counts(const std::string& rel, const uint32_t* bounds, uint64_t n_bounds,
                     uint64_t* counts);
+  // Instances of a batched run: instance j owns the values [bounds[j],
+  // bounds[j+1]) (n_bounds = instances + 1; 0 clears).  Every later run
+  // records on the device, per recursive step whose computed relations are
+  // binary, the iterations each instance's own run would take.
+  void set_instances(const uint32_t* bounds, uint64_t n_bounds);
+  void instance_iterations(uint64_t step, uint32_t* out, uint64_t n_instances) const;
+  // sums[j] = sum over the rows (x, y) of FULL(rel) with x in [bounds[j],
+  // bounds[j+1]) of mix_a(x - bounds[j]) * mix_b(y - bounds[j]) mod 2^64
+  // (binary relations; the row fingerprint of instances.cu).
+  void range_checksums(const std::string& rel, const uint32_t* bounds, uint64_t n_bounds, uint64_t* sums);
   void set_stream(cudaStream_t s);
   void set_profiling(bool on) { profile_ = on; }
   void set_option(const std::string& name, int64_t value);
@@ -304,6 +314,19 @@ class Database {
   std::map<std::string, std::vector<uint32_t>> group_bounds_;
   std::map<std::string, std::vector<uint64_t>> group_counts_;
   std::vector<StepStats> step_stats_;
+  // batched runs (instances.cu): instance bounds, per recursive step the
+  // last iteration with a delta row of every instance (device), and the
+  // iterations of every instance's own run (host, after the step)
+  std::vector<uint32_t> inst_bounds_;
+  DevBuf inst_bounds_d_;
+  std::map<size_t, DevBuf> inst_last_;
+  std::map<size_t, std::vector<uint32_t>> inst_iters_;
+  uint32_t* loop_marks_ = nullptr;  // the step on the device loop: its instance marks (or null)
+  void instances_begin();
+  uint32_t* instance_marks(size_t si);
+  void mark_instances(size_t si, const Step& st, uint32_t iter);
+  void instances_end(size_t si, uint64_t iters);
+  Index& binary_full_index(Relation& r, bool* swapped);
   uint32_t dom_max_ = 0;
   int bits_ = 1;
   uint64_t derived_ = 0;

@@ -304,7 +304,8 @@ template <typename K>
 static void sort_dedup_t(const Launch& L, const uint64_t* in, uint64_t n, int bits, bool swap,
                          const uint64_t* full, uint64_t n_full, uint64_t* out,
                          uint64_t* d_nout, Scratch& s, const uint64_t* head, uint64_t n_head,
-                         const uint64_t* d_n, const uint64_t* d_n_full) {
+                         const uint64_t* d_n, const uint64_t* d_n_full, uint64_t out_cap = ~0ull,
+                         unsigned int* d_overflow = nullptr) {
   SRDL_REQUIRE(n < (1ull << 32), kErrCapacity, "sort: more than 2^32-1 rows in one index");
   K* a = s.take<K>(n);
   K* b = s.take<K>(n);
@@ -341,6 +342,8 @@ static void sort_dedup_t(const Launch& L, const uint64_t* in, uint64_t n, int bi
   }
   DedupDiffSel<K> sel{a, bits, true, full, n_full, out, head, n_head};
   sel.d_n_full = d_n_full;
+  sel.out_cap = out_cap;
+  sel.d_overflow = d_overflow;
   if (d_n) compact_diff_dev(L, sel, n, d_n, d_nout, s);
   else compact_diff(L, sel, n, d_nout, s);
 }
@@ -380,13 +383,14 @@ void warm_device_loop_kernels(int bits) {
 
 void sort_dedup_dev(const Launch& L, const uint64_t* in, uint64_t cap, const uint64_t* d_n,
                     int bits, const uint64_t* full, uint64_t full_cap, const uint64_t* d_n_full,
-                    uint64_t* out, uint64_t* d_nout, Scratch& s) {
+                    uint64_t* out, uint64_t out_cap, uint64_t* d_nout, unsigned int* d_overflow,
+                    Scratch& s) {
   cap = cap ? cap : 1;
   if (use32(bits))
     sort_dedup_t<uint32_t>(L, in, cap, bits, false, full, full_cap, out, d_nout, s, nullptr, 0, d_n,
-                           d_n_full);
+                           d_n_full, out_cap, d_overflow);
   else sort_dedup_t<uint64_t>(L, in, cap, bits, false, full, full_cap, out, d_nout, s, nullptr, 0,
-                              d_n, d_n_full);
+                              d_n, d_n_full, out_cap, d_overflow);
 }
 
 }  // namespace srdl

@@ -24,7 +24,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .native import Database
+from .native import Database, SrdlError
 from .plan import parse_filter
 
 
@@ -89,20 +89,28 @@ def make_union(instances: list[dict]) -> Union:
 
 
 class BatchRun:
-  '''One disjoint-union evaluation; per-instance sizes and rows on demand.'''
+  '''One disjoint-union evaluation; per-instance sizes, iterations,
+  fingerprints and rows on demand.'''
 
   def __init__(self, plan: dict, instances: list[dict], device: int = 0, max_iters: int = 0,
-               db: Database | None = None, union: Union | None = None):
+               db: Database | None = None, union: Union | None = None, load=None):
+    '''load(db, union): stages the union's inputs (default: load_rows of
+    the host rows; a caller may stage device-resident rows instead).'''
     check_batchable(plan)
+    self.plan = plan
     self.union = union or make_union(instances)
     self.k = len(self.union.offsets) - 1
     self.db = db or Database(plan, device=device)
     self.db.clear_inputs()
-    for rel, rows in self.union.inputs.items():
-      self.db.load_rows(rel, rows)
+    if load is None:
+      for rel, rows in self.union.inputs.items():
+        self.db.load_rows(rel, rows)
+    else:
+      load(self.db, self.union)
     bounds = self.union.offsets.astype(np.uint32)
     for rule in count_rules(plan):
       self.db.set_count_groups(rule, bounds)
+    self.db.set_instances(bounds)
     self.db.run(max_iters)
 
   def counts(self, rule: str) -> np.ndarray:
@@ -113,9 +121,178 @@ class BatchRun:
     '''Per-instance row counts of FULL(rel), computed on the device.'''
     return self.db.range_counts(rel, self.union.offsets.astype(np.uint32))
 
+  def checksums(self, rel: str) -> np.ndarray:
+    '''Per-instance fingerprints of FULL(rel) in the instances' own values
+    (binary relations; srdl_range_checksums).'''
+    return self.db.range_checksums(rel, self.union.offsets.astype(np.uint32))
+
+  def iterations(self) -> dict:
+    '''{step index: per-instance iterations of that recursive step} -- the
+    iterations each instance's own run takes, recorded on the device.'''
+    out = {}
+    for i, st in enumerate(self.plan['steps']):
+      if st.get('recursive'):
+        try:
+          out[i] = self.db.instance_iterations(i)
+        except SrdlError as e:
+          if e.code != 7:  # a step computing a non-binary relation is not recorded
+            raise
+    return out
+
   def split_rows(self, rel: str) -> list[np.ndarray]:
     '''Every instance's rows of FULL(rel), shifted back to its own values.'''
     all_rows = self.db.dump(rel)
     cuts = np.searchsorted(all_rows[:, 0], self.union.offsets.astype(np.int64), side='left')
     return [(all_rows[cuts[j]:cuts[j + 1]].astype(np.uint64) - self.union.offsets[j])
             .astype(np.uint32) for j in range(self.k)]
+
+
+# ---------------------------------------------------------------------------
+# Waves: batches larger than one device
+# ---------------------------------------------------------------------------
+
+def instance_bound(inst: dict, arities: list) -> int:
+  """An upper bound of the tuples an instance's fixpoint can hold: every
+  relation the program derives has at most span^arity tuples over the
+  instance's values [0, span) (Datalog creates no values)."""
+  mx = -1
+  for rows in inst.values():
+    a = np.asarray(rows)
+    if a.size:
+      mx = max(mx, int(a.max()))
+  span = mx + 1 if mx >= 0 else 1
+  return sum(span ** a for a in arities)
+
+
+def derived_arities(plan: dict) -> list:
+  """Arities of the relations the plan's rules insert into."""
+  ar = {r['name']: r['arity'] for r in plan['relations']}
+  heads = set()
+  for st in plan['steps']:
+    for op in st['ops']:
+      if op['op'] == 'execute_pipeline':
+        for p in op['pipeline']:
+          if p['op'] == 'insert_into':
+            heads.add(p['rel'])
+  return [ar[h] for h in sorted(heads)] or [2]
+
+
+def plan_waves(bounds, capacity: float) -> list:
+  """Instances (in order) in consecutive waves whose bounds sum to at most
+  `capacity`; an instance above it forms a wave alone."""
+  waves, cur, tot = [], [], 0.0
+  for j, b in enumerate(bounds):
+    if cur and tot + b > capacity:
+      waves.append(cur)
+      cur, tot = [], 0.0
+    cur.append(j)
+    tot += b
+  if cur:
+    waves.append(cur)
+  return waves
+
+
+class WaveRun:
+  """Batched fixpoints of more instances than one device holds at once.
+
+  The instances go in waves: each wave is one disjoint-union run
+  (BatchRun) on the same database, whose derived tuples are released when
+  the next wave starts.  A wave's size comes from an upper bound of its
+  instances' fixpoints (instance_bound) and a device-memory budget: waves
+  hold instances whose bounds sum to budget / bytes_per_bound, where
+  bytes_per_bound starts at `bytes_per_bound` and is raised to the largest
+  peak bytes per bound tuple any wave has measured (x1.25).  Every run is
+  held to the budget (mem_limit_mb); a wave that outgrows it releases what
+  it built and is split in two, and the halves run in its place; a single
+  instance that outgrows the whole budget is reported in `errors`.  The
+  partition that succeeded is kept (`waves`) for later runs of the same
+  instances, so repeated runs (warm-up, then timed steps) redo no split.
+
+  Results, per instance in input order: `sizes[rel]` (FULL rows),
+  `checksums[rel]` (row fingerprints, binary relations), `iterations[step]`
+  (the iterations its own run takes) and `counts[rule]` (count-only rules).
+  """
+
+  def __init__(self, plan: dict, instances: list, *, device: int = 0, db: Database | None = None,
+               budget_bytes: int | None = None, bytes_per_bound: float = 64.0,
+               sizes=(), checksums=(), max_iters: int = 0):
+    check_batchable(plan)
+    self.plan = plan
+    self.instances = instances
+    self.k = len(instances)
+    self.db = db or Database(plan, device=device)
+    if budget_bytes is None:
+      import torch
+      free, _ = torch.cuda.mem_get_info(device)
+      budget_bytes = int(0.8 * free)
+    self.budget = int(budget_bytes)
+    self.bytes_per_bound = float(bytes_per_bound)
+    self.bounds = np.array([instance_bound(i, derived_arities(plan)) for i in instances], np.float64)
+    self.waves: list | None = None
+    self.want_sizes = list(sizes)
+    self.want_checksums = list(checksums)
+    self.max_iters = max_iters
+    self.splits = 0
+    self.peak_bytes = 0
+
+  def _new_results(self):
+    self.sizes = {r: np.zeros(self.k, np.uint64) for r in self.want_sizes}
+    self.checksums = {r: np.zeros(self.k, np.uint64) for r in self.want_checksums}
+    self.iterations: dict = {}
+    self.counts: dict = {}
+    self.errors: dict = {}
+
+  def run(self, union_of=None, load=None, on_wave=None) -> None:
+    """Evaluate every instance.  union_of(indices) -> Union may supply the
+    waves' unions (cached by the caller); load(db, union) stages one;
+    on_wave(db) is called after every wave that completed (its stats)."""
+    self._new_results()
+    if self.waves is None:
+      cap = self.budget / self.bytes_per_bound
+      self.waves = plan_waves(self.bounds, cap)
+    done, queue = [], list(self.waves)
+    self.db.set_option('mem_limit_mb', max(1, self.budget >> 20))
+    while queue:
+      wave = queue.pop(0)
+      insts = [self.instances[j] for j in wave]
+      union = union_of(wave) if union_of else make_union(insts)
+      try:
+        br = BatchRun(self.plan, insts, db=self.db, union=union, load=load,
+                      max_iters=self.max_iters)
+      except SrdlError as e:
+        if e.code != 5:
+          raise
+        # outgrew the budget: learn the larger bytes per bound tuple, split
+        # this wave and re-plan the ones not yet run with the new size
+        self.bytes_per_bound = max(self.bytes_per_bound,
+                                   1.25 * self.budget / max(1.0, float(self.bounds[wave].sum())))
+        if len(wave) == 1:
+          self.errors[wave[0]] = str(e)
+          done.append(wave)
+          continue
+        self.splits += 1
+        h = len(wave) // 2
+        rest = [j for w in queue for j in w]
+        cap = self.budget / self.bytes_per_bound
+        queue[:] = [wave[:h], wave[h:]] + [[rest[i] for i in w] for w in
+                                           plan_waves(self.bounds[rest], cap)]
+        continue
+      if on_wave:
+        on_wave(self.db)
+      peak = int(self.db.mem_stats()['peak'])
+      self.peak_bytes = max(self.peak_bytes, peak)
+      bound = float(self.bounds[wave].sum())
+      if bound >= 0.25 * self.budget / self.bytes_per_bound or len(wave) == 1:
+        # (small waves' peaks are mostly fixed costs: learn from full ones)
+        self.bytes_per_bound = max(self.bytes_per_bound, 1.25 * peak / max(1.0, bound))
+      idx = np.asarray(wave, np.int64)
+      for r in self.want_sizes:
+        self.sizes[r][idx] = br.sizes(r)
+      for r in self.want_checksums:
+        self.checksums[r][idx] = br.checksums(r)
+      for step, its in br.iterations().items():
+        self.iterations.setdefault(step, np.zeros(self.k, np.uint32))[idx] = its
+      for rule in count_rules(self.plan):
+        self.counts.setdefault(rule, np.zeros(self.k, np.uint64))[idx] = br.counts(rule)
+      done.append(wave)
+    self.waves = done

@@ -45,6 +45,9 @@ SIGNATURES = {
   'srdl_set_count_groups': (ctypes.c_int, [_vp, _cp, _u32p, _u64]),
   'srdl_group_counts': (ctypes.c_int, [_vp, _cp, ctypes.POINTER(_u64), _u64]),
   'srdl_range_counts': (ctypes.c_int, [_vp, _cp, _u32p, _u64, ctypes.POINTER(_u64)]),
+  'srdl_set_instances': (ctypes.c_int, [_vp, _u32p, _u64]),
+  'srdl_instance_iterations': (ctypes.c_int, [_vp, _u64, _u32p, _u64]),
+  'srdl_range_checksums': (ctypes.c_int, [_vp, _cp, _u32p, _u64, ctypes.POINTER(_u64)]),
   'srdl_run': (ctypes.c_int, [_vp, _u64]),
   'srdl_size': (_u64, [_vp, _cp]),
   'srdl_count': (_u64, [_vp, _cp]),
@@ -211,6 +214,33 @@ class Database:
     check(lib().srdl_range_counts(self._h, rel.encode(), b.ctypes.data_as(_u32p), b.shape[0],
                                   out.ctypes.data_as(ctypes.POINTER(_u64))),
           f'srdl_range_counts({rel})')
+    return out
+
+  def set_instances(self, bounds) -> None:
+    '''Instance j of a batched run owns the values [bounds[j], bounds[j+1]);
+    later runs record every instance's own iteration count per recursive
+    step (None or an empty array clears).'''
+    b = np.ascontiguousarray([] if bounds is None else bounds, dtype=np.uint32)
+    self._n_instances = max(0, b.shape[0] - 1)
+    check(lib().srdl_set_instances(self._h, b.ctypes.data_as(_u32p) if b.size else None, b.shape[0]),
+          'srdl_set_instances')
+
+  def instance_iterations(self, step: int) -> np.ndarray:
+    '''Iterations each instance's own run takes in plan step `step` (last run).'''
+    out = np.zeros(getattr(self, '_n_instances', 0), np.uint32)
+    check(lib().srdl_instance_iterations(self._h, step, out.ctypes.data_as(_u32p), out.shape[0]),
+          f'srdl_instance_iterations({step})')
+    return out
+
+  def range_checksums(self, rel: str, bounds) -> np.ndarray:
+    '''Per-range fingerprints of FULL(rel) (binary): the sum mod 2^64 of
+    row_fingerprint(x - bounds[j], y - bounds[j]) over the rows whose first
+    column is in [bounds[j], bounds[j+1]).'''
+    b = np.ascontiguousarray(bounds, dtype=np.uint32)
+    out = np.zeros(max(0, b.shape[0] - 1), np.uint64)
+    check(lib().srdl_range_checksums(self._h, rel.encode(), b.ctypes.data_as(_u32p), b.shape[0],
+                                     out.ctypes.data_as(ctypes.POINTER(_u64))),
+          f'srdl_range_checksums({rel})')
     return out
 
   def staged_rows(self, rel: str) -> int:

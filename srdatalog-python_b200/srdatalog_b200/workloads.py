@@ -115,15 +115,32 @@ def er_instance(n_nodes: int, mean_deg: float, seed: int) -> np.ndarray:
   return _dedup_in_order(s[keep], d[keep])
 
 
-def batched_instances(count: int = 4096, n_lo: int = 64, n_hi: int = 65536,
-                      deg_lo: float = 2.0, deg_hi: float = 8.0, seed0: int = 1000):
-  '''Batched-fixpoint config: instance j has n_j = round(exp(U[ln n_lo, ln n_hi]))
-  nodes and mean out-degree U[deg_lo, deg_hi], generated with seed seed0+j.'''
+def batched_shapes(count: int = 4096, n_lo: int = 64, n_hi: int = 65536,
+                   deg_lo: float = 2.0, deg_hi: float = 8.0, seed0: int = 1000):
+  '''(n_j, c_j) of the batched-fixpoint config: n_j = round(exp(U[ln n_lo,
+  ln n_hi])) nodes and mean out-degree c_j = U[deg_lo, deg_hi], drawn with
+  seed seed0+j.'''
   out = []
   for j in range(count):
     rng = _rng(seed0 + j)
     n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
     c = float(rng.uniform(deg_lo, deg_hi))
+    out.append((n, c))
+  return out
+
+
+def batched_instances(count: int = 4096, n_lo: int = 64, n_hi: int = 65536,
+                      deg_lo: float = 2.0, deg_hi: float = 8.0, seed0: int = 1000,
+                      n_max: int | None = None, only=None):
+  '''Batched-fixpoint config: instance j is a directed Erdos-Renyi graph
+  (er_instance, seed seed0 + j + 10^6) of the shape batched_shapes draws.
+  n_max keeps the instances with n_j <= n_max, `only` the listed j (the
+  config's own draws either way).'''
+  out = []
+  keep = None if only is None else set(only)
+  for j, (n, c) in enumerate(batched_shapes(count, n_lo, n_hi, deg_lo, deg_hi, seed0)):
+    if (n_max is not None and n > n_max) or (keep is not None and j not in keep):
+      continue
     out.append(er_instance(n, c, seed0 + j + 1_000_000))
   return out
 

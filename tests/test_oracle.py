@@ -181,3 +181,35 @@ def test_generators_deterministic():
   assert np.all(r[:, 0] < r[:, 1])
   insts = W.batched_instances(count=3)
   assert all(x.shape[1] == 2 for x in insts)
+
+
+@pytest.mark.parametrize('n,m,seed', [(5, 8, 0), (40, 30, 1), (40, 90, 2), (300, 280, 3),
+                                      (300, 900, 4), (2000, 1900, 5), (2000, 6000, 6)])
+def test_closure_fingerprint_matches_semi_naive(n, m, seed):
+  '''The SCC restatement of TC's fixpoint (used on instances too large for
+  the semi-naive evaluator) gives the semi-naive oracle's size and row
+  fingerprint, on graphs with self-loops, duplicate edges, cycles and
+  isolated parts.'''
+  e = np.random.default_rng(seed).integers(0, n, (m, 2)).astype(np.uint32)
+  keys, _, _ = oracle.tc(np.unique(e, axis=0))
+  rows = oracle.unpack(keys, (1, 0))
+  assert oracle.tc_closure_fingerprint(e, n) == (rows.shape[0], oracle.row_fingerprint(rows))
+
+
+def test_closure_fingerprint_shapes():
+  chain = np.array([[i, i + 1] for i in range(50)], np.uint32)
+  assert oracle.tc_closure_fingerprint(chain)[0] == 50 * 51 // 2
+  loops = np.array([[0, 0], [1, 2], [2, 1], [3, 3], [3, 4]], np.uint32)
+  rows = np.array([[0, 0], [1, 1], [1, 2], [2, 1], [2, 2], [3, 3], [3, 4]], np.uint32)
+  assert oracle.tc_closure_fingerprint(loops) == (7, oracle.row_fingerprint(rows))
+  assert oracle.tc_closure_fingerprint(np.zeros((0, 2), np.uint32)) == (0, 0)
+  # the fingerprint is order-free and sensitive to one row
+  assert oracle.row_fingerprint(rows[::-1]) == oracle.row_fingerprint(rows)
+  assert oracle.row_fingerprint(rows[1:]) != oracle.row_fingerprint(rows)
+
+
+def test_closure_fingerprints_pool():
+  jobs = [(np.random.default_rng(s).integers(0, 200, (400, 2)).astype(np.uint32), 200)
+          for s in range(12)]
+  assert oracle.tc_closure_fingerprints(jobs, workers=2) == [oracle.tc_closure_fingerprint(*j)
+                                                              for j in jobs]
