@@ -308,6 +308,19 @@ def gen_jit_triangle_program() -> Program:
   return _triangle3(('Edge', 'Edge', 'Edge', 'Z'), 'Triangle')
 
 
+def triangle_db_program() -> Program:
+  '''examples/triangle.py: ZRel(x,y,z) <= RRel(x,y), SRel(y,z,h), TRel(z,x,f)
+  -- the third columns of the ternary SRel and TRel are projected away.'''
+  r_rel = Relation('RRel', 2, column_types=(int, int))
+  s_rel = Relation('SRel', 3, column_types=(int, int, int))
+  t_rel = Relation('TRel', 3, column_types=(int, int, int))
+  z_rel = Relation('ZRel', 3, column_types=(int, int, int))
+  f, h, x, y, z = Var('f'), Var('h'), Var('x'), Var('y'), Var('z')
+  return Program(rules=[
+    (z_rel(x, y, z) <= r_rel(x, y) & s_rel(y, z, h) & t_rel(z, x, f)).named('Triangle')
+    .with_plan(var_order=['x', 'y', 'z'])])
+
+
 def tc_2level_bg_program() -> Program:
   '''examples/tc_2level_bg.py: TC with Path as a Device2LevelIndex and the
   recursive rule planned y, x, z with the block-group hint.'''
@@ -489,6 +502,7 @@ PROGRAMS = {
   'debug_triangle': (debug_triangle_program, 'DebugTrianglePlan',
                      'integration/debug_triangle.mir.sexpr'),
   'gen_jit_triangle': (gen_jit_triangle_program, 'GenJitPlan', 'integration/gen_jit_code.mir.sexpr'),
+  'triangle_db': (triangle_db_program, 'TriangleDBPlan', 'integration/triangle.mir.sexpr'),
   'tc_2level_bg': (tc_2level_bg_program, 'Tc2LevelBgPlan', 'integration/tc_2level_bg.mir.sexpr'),
   'print_mir': (print_mir_program, 'PrintMirPlan', 'integration/print_mir.mir.sexpr'),
   'rewrite_consts': (rewrite_consts_program, 'RewriteConstsPlan', 'rewrite_consts.mir.sexpr'),

@@ -477,6 +477,28 @@ def test_arity3_triangle_programs(n, m, seed):
   assert oracle.dump_hash(db.dump('Z')) == oracle.dump_hash(want)
 
 
+@pytest.mark.parametrize('n,m,seed', [(40, 150, 0), (300, 2500, 1), (2000, 12000, 2)])
+def test_triangle_db_program(n, m, seed):
+  '''examples/triangle.py: ZRel(x,y,z) <= RRel(x,y), SRel(y,z,h), TRel(z,x,f)
+  (the ternary relations' third columns projected away), against the plan
+  interpreter.'''
+  rng = np.random.default_rng(seed)
+  r = W.uniform_edges(n, m, seed + 1)
+  s = rng.integers(0, n, (m, 3)).astype(np.uint32)
+  t = rng.integers(0, n, (m, 3)).astype(np.uint32)
+  inp = {'RRel': r, 'SRel': s, 'TRel': t}
+  # the directed-triangle oracle over the projections (y,z) of SRel and
+  # (z,x) of TRel; the plan interpreter agrees on the smallest input
+  w = np.array(oracle.triangle3(r, np.unique(s[:, :2], axis=0), np.unique(t[:, :2], axis=0)),
+               np.uint32).reshape(-1, 3)
+  if n <= 40:
+    want, _ = oracle.run_plan(load_plan('triangle_db'), inp)
+    assert oracle.dump_hash(np.array(sorted(want['ZRel']), np.uint32).reshape(-1, 3)) == oracle.dump_hash(w)
+  db = run('triangle_db', inp)
+  assert db.size('ZRel') == w.shape[0] > 0
+  assert oracle.dump_hash(db.dump('ZRel')) == oracle.dump_hash(w)
+
+
 def test_tc_2level_bg_program(expected):
   exp = expected['tc_mid']
   db = run('tc_2level_bg', {'ArcInput': W.uniform_edges(2000, 6000, 7)})
