@@ -529,6 +529,7 @@ def run_batched(args, rank, world):
   if args.workload == 'batched-wide':
     wl['desc'] = wl['desc'].format(n_max=args.batch_n_max)
   plan = load_plan(wl['plan'])
+  plain_plan = plan  # the one-query-at-a-time loop runs the plan as given
   insts = make_batch(args.workload, args.batch_n_max)
   k = len(insts)
   stream = torch.cuda.current_stream(dev)
@@ -537,12 +538,12 @@ def run_batched(args, rank, world):
   if wl.get('tune'):
     # untimed: the autotuner times candidate settings on the union of all
     # instances when they fit one run, else of the first instances whose
-    # closures (at most n^2 tuples each) add up to 3e8
+    # closures (at most n^2 tuples each) add up to 1e9 (about one wave)
     from srdatalog_b200.autotune import autotune
     sample, tot = [], 0
     for inst in insts:
       n = int(inst[wl['rel']].max()) + 1
-      if args.workload != 'batched' and sample and tot + n * n > 3e8:
+      if args.workload != 'batched' and sample and tot + n * n > 1e9:
         break
       sample.append(inst)
       tot += n * n
@@ -624,7 +625,7 @@ def run_batched(args, rank, world):
   h2d = int(sum(u.inputs[wl['rel']].nbytes for u in unions.values()))
   plain = None
   if not args.no_cpu_baseline:
-    plain, sizes, iters = plain_loop(plan, insts, PLAIN_SAMPLE_STRIDE, stream.cuda_stream, local)
+    plain, sizes, iters = plain_loop(plain_plan, insts, PLAIN_SAMPLE_STRIDE, stream.cuda_stream, local)
     assert [int(x) for x in want[::PLAIN_SAMPLE_STRIDE]] == sizes
     rec = sorted(want_iters)
     assert all([int(want_iters[s][j]) for s in rec] == it
