@@ -443,9 +443,12 @@ def run_plan(plan: dict, inputs: dict, max_iters: int = 0):
       elif k == 'negation':
         # keep a binding iff no tuple of the relation starts (in index order)
         # with the prefix values
-        idx, pre = p['index'], p['prefix']
-        present = {tuple(t[idx[i]] for i in range(len(pre))) for t in db[(p['rel'], p['ver'])]}
-        nb = [b for b in binds if tuple(b[v] for v in pre) not in present]
+        # (constant arguments first: their columns lead the index,
+        # src/srdatalog/hir/plan.py:284-286)
+        idx, pre, cp = p['index'], p['prefix'], tuple(p.get('const_prefix', []))
+        k = len(cp) + len(pre)
+        present = {tuple(t[idx[i]] for i in range(k)) for t in db[(p['rel'], p['ver'])]}
+        nb = [b for b in binds if cp + tuple(b[v] for v in pre) not in present]
       elif k == 'insert_into':
         if op['count']:
           counts[op['rule']] = counts.get(op['rule'], 0) + len(binds)

@@ -191,13 +191,32 @@ PipePlan Database::plan_pipeline(const Op& op, bool recursive, uint64_t iteratio
       SRDL_REQUIRE(lv.nfilt < kMaxFilt, kErrUnsupported, "too many filter terms");
       const SourceDesc& d = po.sources[0];
       Relation& nr = rel(d.rel);
-      SRDL_REQUIRE(nr.arity <= 2, kErrUnsupported, "negation over relation " + nr.name + " of arity > 2");
+      SRDL_REQUIRE(nr.arity <= 3, kErrUnsupported, "negation over relation " + nr.name + " of arity > 3");
+      // the probed prefix: the constants (their columns lead the index), then the variables
+      struct Val {
+        int slot;
+        uint32_t c;
+      };
+      std::vector<Val> vals;
+      for (uint32_t c : po.const_prefix) vals.push_back({-1, c});
+      for (auto& v : d.prefix) vals.push_back({slot_of(v), 0});
+      SRDL_REQUIRE(!vals.empty() && vals.size() <= (size_t)std::min(nr.arity, 2), kErrUnsupported,
+                   "negation on " + nr.name + ": one or two bound values (constants or variables)");
       FiltSpec f;
       f.negation = true;
-      f.a_slot = slot_of(d.prefix[0]);
-      f.b_slot = d.prefix.size() > 1 ? slot_of(d.prefix[1]) : -1;
-      SRDL_REQUIRE(f.b_slot < 0 || nr.arity == 2, kErrPlan, "negation prefix longer than " + nr.name);
-      f.neg = view(nr, ensure_index(nr, d.ver, d.index));
+      f.neg_n = (int)vals.size();
+      f.a_slot = vals[0].slot;
+      f.a_const = vals[0].c;
+      if (vals.size() > 1) {
+        f.b_slot = vals[1].slot;
+        f.b_const = vals[1].c;
+      }
+      if (nr.arity == 3) {
+        // the pair view (c0, c1) of the relation in the negation's column order
+        f.neg = view2(ternary(d).pair);
+      } else {
+        f.neg = view(nr, ensure_index(nr, d.ver, d.index));
+      }
       lv.filt[lv.nfilt++] = f;
       continue;
     }

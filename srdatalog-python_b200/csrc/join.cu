@@ -215,7 +215,7 @@ __device__ __forceinline__ uint64_t gallop_row(const uint64_t* offs, uint64_t lo
 
 __device__ __forceinline__ bool filt_ok(const FiltSpec& f, uint32_t a, uint32_t b) {
   if (f.shard_world) return shard_owner(a, f.shard_world) == f.b_const;
-  if (f.negation) return f.b_slot < 0 ? !trie_has_root(f.neg, a) : !trie_child_contains(f.neg, a, b);
+  if (f.negation) return f.neg_n == 1 ? !trie_has_root(f.neg, a) : !trie_child_contains(f.neg, a, b);
   switch (f.op) {
     case kNe: return a != b;
     case kEq: return a == b;

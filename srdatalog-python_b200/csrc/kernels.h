@@ -216,8 +216,11 @@ struct FiltSpec {
   uint32_t a_const = 0, b_const = 0;
   int op = kNe;
   // Negation (MIR `negation`, mir/types.py:189): keep the binding iff the
-  // tuple (a) -- or (a, b) when b_slot >= 0 -- is not a key prefix of `neg`.
+  // tuple (a) -- (a, b) when neg_n is 2 -- is not a key prefix of `neg`
+  // (a ternary relation is probed through its pair view in the negation's
+  // column order).  Values come from slots or constants (a_const, b_const).
   bool negation = false;
+  int neg_n = 1;
   TrieView neg;
   // Shard filter: keep the binding iff shard_owner(a, shard_world) == b_const
   // (0: not a shard filter).

@@ -380,8 +380,15 @@ void Database::parse_plan(const std::string& plan_json) {
           } else if (pk == "negation") {
             po.kind = PipeOp::Negation;
             po.sources.push_back(parse_source(pj));
-            SRDL_REQUIRE(!po.sources[0].prefix.empty() && po.sources[0].prefix.size() <= 2,
-                         kErrUnsupported, "plan: negation needs one or two bound variables");
+            if (pj.has("const_prefix"))
+              for (auto& cj : pj.at("const_prefix").a()) {
+                const long long v = cj.i();
+                SRDL_REQUIRE(v >= 0 && v <= 0xFFFFFFFFll, kErrPlan, "plan: negation constant out of range");
+                po.const_prefix.push_back((uint32_t)v);
+              }
+            const size_t nb = po.const_prefix.size() + po.sources[0].prefix.size();
+            SRDL_REQUIRE(nb >= 1 && nb <= 2, kErrUnsupported,
+                         "plan: negation needs one or two bound values");
           } else if (pk == "filter") {
             po.kind = PipeOp::Filter;
             po.vars = pj.at("vars").strs();

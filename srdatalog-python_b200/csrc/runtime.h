@@ -178,6 +178,7 @@ struct PipeOp {
   std::string code;                          // filter
   std::string rel;                           // insert
   std::vector<int> index;                    // insert dedup index
+  std::vector<uint32_t> const_prefix;        // negation: constant values leading the probed prefix
 };
 
 struct Op {

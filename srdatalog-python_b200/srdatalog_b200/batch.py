@@ -57,6 +57,8 @@ def check_batchable(plan: dict) -> None:
           for a, _, b in parse_filter(p['code'], bound):
             if a.isdigit() or b.isdigit():
               raise BatchError(f'rule {op["rule"]}: a filter constant prevents value shifting')
+        elif p['op'] == 'negation' and p.get('const_prefix'):
+          raise BatchError(f'rule {op["rule"]}: a negation constant prevents value shifting')
 
 
 @dataclass

@@ -78,12 +78,18 @@ def _pipeline_op(node: Any) -> dict:
   if kind == 'Filter':
     return {'op': 'filter', 'vars': list(node.vars), 'code': node.code}
   if kind == 'Negation':
-    # anti-join on bound variables (mir/types.py:189); constant arguments
-    # would need a constant-bound probe, which this runtime does not have
-    if getattr(node, 'const_args', None):
-      raise PlanError(f'negation on {node.rel_name} with constant arguments is not supported')
-    return {'op': 'negation', 'rel': node.rel_name, 'ver': _ver(node.version),
-            'index': [int(c) for c in node.index], 'prefix': list(node.prefix_vars)}
+    # anti-join (mir/types.py:189): the probed prefix is the constant
+    # arguments' values (their columns lead the index, hir/plan.py:284-286)
+    # followed by the bound variables
+    d = {'op': 'negation', 'rel': node.rel_name, 'ver': _ver(node.version),
+         'index': [int(c) for c in node.index], 'prefix': list(node.prefix_vars)}
+    consts = [int(v) for _, v in (getattr(node, 'const_args', None) or [])]
+    for v in consts:
+      if not 0 <= v <= 0xFFFFFFFF:
+        raise PlanError(f'negation on {node.rel_name}: constant {v} is not a uint32 value')
+    if consts:
+      d['const_prefix'] = consts
+    return d
   if kind == 'ConstantBind':
     # binding v to a literal = joining with the one-tuple relation {(value)}
     value = _const_literal(node)
@@ -299,8 +305,11 @@ def validate_plan(plan: dict) -> None:
         elif k == 'negation':
           if p['rel'] not in arity:
             raise PlanError(f'unknown relation {p["rel"]}')
-          if not 1 <= len(p['prefix']) <= min(2, arity[p['rel']]):
-            raise PlanError(f'negation on {p["rel"]}: needs 1..2 bound variables')
+          ar = arity[p['rel']]
+          nb = len(p.get('const_prefix', [])) + len(p['prefix'])
+          if ar > 3 or not 1 <= nb <= min(ar, 2):
+            raise PlanError(f'negation on {p["rel"]}: needs 1..2 bound values (constants or '
+                            f'variables) of a relation of arity <= 3')
           for v in p['prefix']:
             if v not in bound:
               raise PlanError(f'negation on {p["rel"]}: unbound var {v} in {op["rule"]}')

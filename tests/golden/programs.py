@@ -321,6 +321,25 @@ def triangle_db_program() -> Program:
     .with_plan(var_order=['x', 'y', 'z'])])
 
 
+def neg_forms_program() -> Program:
+  '''Negation with constant arguments and over a ternary relation (the
+  forms of examples/reg_scc.py and crdt.py on relations of arity <= 3):
+  a constant in a binary negation, two bound columns of a ternary one
+  around a wildcard, a constant plus a variable, one bound column.'''
+  e = Relation('Edge', 2, column_types=(int, int))
+  b = Relation('Blocked', 2, column_types=(int, int))
+  t = Relation('Tern', 3, column_types=(int, int, int))
+  outs = [Relation(n, 2, column_types=(int, int)) for n in
+          ('OutConst', 'OutTern2', 'OutTernConst', 'OutTern1')]
+  x, y, w1, w2 = Var('x'), Var('y'), Var('_'), Var('_')
+  return Program(rules=[
+    (outs[0](x, y) <= e(x, y) & ~b(x, 3)).named('NegConst'),
+    (outs[1](x, y) <= e(x, y) & ~t(x, w1, y)).named('NegTern2'),
+    (outs[2](x, y) <= e(x, y) & ~t(5, y, w1)).named('NegTernConst'),
+    (outs[3](x, y) <= e(x, y) & ~t(w1, w2, x)).named('NegTern1'),
+  ])
+
+
 def tc_2level_bg_program() -> Program:
   '''examples/tc_2level_bg.py: TC with Path as a Device2LevelIndex and the
   recursive rule planned y, x, z with the block-group hint.'''
@@ -503,6 +522,7 @@ PROGRAMS = {
                      'integration/debug_triangle.mir.sexpr'),
   'gen_jit_triangle': (gen_jit_triangle_program, 'GenJitPlan', 'integration/gen_jit_code.mir.sexpr'),
   'triangle_db': (triangle_db_program, 'TriangleDBPlan', 'integration/triangle.mir.sexpr'),
+  'neg_forms': (neg_forms_program, 'NegFormsPlan', None),
   'tc_2level_bg': (tc_2level_bg_program, 'Tc2LevelBgPlan', 'integration/tc_2level_bg.mir.sexpr'),
   'print_mir': (print_mir_program, 'PrintMirPlan', 'integration/print_mir.mir.sexpr'),
   'rewrite_consts': (rewrite_consts_program, 'RewriteConstsPlan', 'rewrite_consts.mir.sexpr'),

@@ -499,6 +499,25 @@ def test_triangle_db_program(n, m, seed):
   assert oracle.dump_hash(db.dump('ZRel')) == oracle.dump_hash(w)
 
 
+@pytest.mark.parametrize('n,m,seed', [(20, 60, 0), (60, 400, 1), (3000, 40000, 2)])
+def test_negation_forms_program(n, m, seed):
+  '''Negation with a constant argument and over a ternary relation (one or
+  two bound columns, around a wildcard, with a constant): every output
+  equals the plan interpreter's.'''
+  from test_negation_forms import expected, inputs
+  inp = inputs(n, m, seed)
+  want = expected(inp)
+  if n <= 60:
+    got, _ = oracle.run_plan(load_plan('neg_forms'), inp)
+    for rel, rows in want.items():
+      assert set(got[rel]) == rows, rel
+  db = run('neg_forms', inp)
+  for rel, rows in want.items():
+    w = np.array(sorted(rows), np.uint32).reshape(-1, 2)
+    assert db.size(rel) == w.shape[0], rel
+    assert oracle.dump_hash(db.dump(rel)) == oracle.dump_hash(w), rel
+
+
 def test_tc_2level_bg_program(expected):
   exp = expected['tc_mid']
   db = run('tc_2level_bg', {'ArcInput': W.uniform_edges(2000, 6000, 7)})
