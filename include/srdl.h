@@ -91,6 +91,12 @@ int srdl_set_profiling(srdl_db* db, int enable);
  *   "join_chunk"       largest chunk of candidates a warp of the two-source
  *                      column join takes from its queue, 64..2^20 (default
  *                      4096): smaller chunks keep the rows in flight closer
+ *   "pivot_min"        count-only two-source joins: rows whose probed list
+ *                      belongs to the table's first (sorted) column, has a
+ *                      bitmap and at least this many values are counted by
+ *                      a kernel holding that bitmap in shared memory
+ *                      (default 0: off -- on the R-MAT triangle the cj2
+ *                      kernel's L2-resident bitmap probes measured faster)
  *   "device_loop"      1 (default; SRDL_DEVICE_LOOP=0 changes it) runs the
  *                      iterations of a qualifying recursive step after the
  *                      first as one CUDA graph that loops on the device

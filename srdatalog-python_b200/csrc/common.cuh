@@ -73,6 +73,7 @@ struct TrieView {
   const uint32_t* bdir = nullptr;
   const uint32_t* bpool = nullptr;
   uint32_t bwords = 0;
+  uint32_t bslots = 0;  // bitmaps in bpool
   uint64_t n = 0;
   const uint64_t* n_roots_d = nullptr;  // device-resident root count
   uint32_t dir_n = 0;

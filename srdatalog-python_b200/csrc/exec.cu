@@ -357,12 +357,34 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
     DevBuf wscr(join_work_scratch_bytes(cur.n), L_.stream);
     Scratch s{wscr.as<char>(), wscr.bytes(), 0};
     size_t pid = prof_begin("join_count");
+    // the last level of a count-only rule: rows probing a long bitmapped
+    // list of the table's first column go to the pivot kernel (join.cu)
+    lv.pivot_src = -1;
+    if (last && op.count && opt_pivot_min_ > 0 && !(sharded && op.shard == Op::Work) &&
+        !group_bounds_.count(op.rule) && lv.kind == kColumnJoin && lv.nsrc == 2 && lv.nfilt == 0 &&
+        !lv.wide && cur.n > 0) {
+      for (int ps = 0; ps < 2; ps++) {
+        const SrcSpec& P = lv.src[ps];
+        const SrcSpec& D = lv.src[1 - ps];
+        if (P.prefix_slot == 0 && D.prefix_slot != 0 && P.mode == kSrcPlain && D.mode == kSrcPlain &&
+            P.t.bdir && P.t.bpool && P.t.bwords && P.t.bslots && P.t.dir_n &&
+            join_pivot_smem_bytes(P.t.bwords) <= kPivotSmemMax) {
+          lv.pivot_src = ps;
+          lv.pivot_min = (uint32_t)std::min<int64_t>(opt_pivot_min_, 0xffffffffll);
+          lv.pivot_slots = P.t.bslots;
+          break;
+        }
+      }
+    }
     JoinWork w = join_count(L_, lv, cur, s);
     prof_end(pid, 8.0 * cur.n * (lv.n_in_slots + 3), (double)cur.n);
     SRDL_CUDA(cudaMemcpyAsync(h_small_ + 3, w.offs + cur.n, 8, cudaMemcpyDeviceToHost, L_.stream));
+    if (w.poffs)
+      SRDL_CUDA(cudaMemcpyAsync(h_small_ + 6, w.poffs + cur.n, 8, cudaMemcpyDeviceToHost, L_.stream));
     SRDL_CUDA(cudaMemsetAsync(d_small_.as<uint64_t>() + 2, 0, 8, L_.stream));
     SRDL_CUDA(cudaStreamSynchronize(L_.stream));
     uint64_t total = h_small_[3];
+    const uint64_t pivot_total = w.poffs ? h_small_[6] : 0;  // the pivot kernel's candidates
     seen[li] = std::max(seen[li], total);
     if (sharded && op.shard == Op::Work && li == work_split) {
       // Deal this level's work items out in segments, kSegsPerShard per
@@ -375,7 +397,8 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
       total = seg_owned(total, lv.seg, shard_world_, shard_rank_);
     }
     // the expand pass's own scratch, sized for this level's candidates
-    DevBuf xscr(join_expand_scratch_bytes(L_, total), L_.stream);
+    DevBuf xscr(join_expand_scratch_bytes(L_, total) + (w.poffs ? join_pivot_scratch_bytes(lv.pivot_slots) : 0),
+                L_.stream);
     Scratch xs{xscr.as<char>(), xscr.bytes(), 0};
     if (last) {
       if (op.count) {
@@ -408,7 +431,7 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
           for (size_t g = 0; g < h.size(); g++) acc[g] += h[g];
         }
         // per candidate: its value (4 B) and one probed word of each other list (4 B)
-        prof_end(pid, 4.0 * total * std::max(1, lv.nsrc), (double)total);
+        prof_end(pid, 4.0 * (total + pivot_total) * std::max(1, lv.nsrc), (double)(total + pivot_total));
         counts_[op.rule] += read_scalar(2);
       } else {
         lv.emit = kEmitKeys;

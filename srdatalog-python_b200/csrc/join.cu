@@ -101,7 +101,8 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
                                                                uint8_t* __restrict__ drv,
                                                                uint32_t* __restrict__ beg,
                                                                uint2* __restrict__ orange,
-                                                               uint32_t* __restrict__ obm) {
+                                                               uint32_t* __restrict__ obm,
+                                                               uint64_t* __restrict__ pwork) {
   // A table written by the previous level may fill only part of its
   // capacity; its true size is on the device and the rest expands to nothing.
   const uint64_t nrows = in.d_n ? min(in.n, *in.d_n) : in.n;
@@ -109,6 +110,7 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
        r += (uint64_t)gridDim.x * blockDim.x) {
     if (r >= nrows) {
       work[r] = 0;
+      if (pwork) pwork[r] = 0;
       continue;
     }
     if (lv.kind == kColumnJoin && lv.nsrc == 2) {
@@ -142,6 +144,14 @@ __global__ void __launch_bounds__(kJThreads) join_count_kernel(LevelSpec lv, Tab
         const uint32_t* obd = bd ? lv.src[0].t.bdir : lv.src[1].t.bdir;
         const int ops = bd ? lv.src[0].prefix_slot : lv.src[1].prefix_slot;
         obm[r] = (obd && ops >= 0) ? obd[in.col[ops][r]] : kNoBitmap;
+        if (pwork) {
+          // a pivot row: the probed list is the pivot source's, bitmapped
+          // and long; its candidates move from cj2 to the pivot kernel
+          const bool piv = bd != lv.pivot_src && obm[r] != kNoBitmap &&
+                           (lv.pivot_src == 0 ? n0 : n1) >= lv.pivot_min;
+          pwork[r] = piv ? (uint64_t)(de - db) : 0;
+          if (piv) work[r] = 0;
+        }
       }
     } else if (lv.kind == kColumnJoin) {
       uint32_t best = 0xffffffffu, bb = 0;
@@ -747,9 +757,11 @@ __global__ void __launch_bounds__(kJThreads) join_cart2_kernel(
 
 size_t join_work_scratch_bytes(uint64_t rows) {
   rows = rows ? rows : 1;
+  // (+ the pivot rows' work, offsets and their scan)
   return ((rows * 8 + 255) & ~size_t(255)) + ((rows + 1) * 8 + 255) + ((rows + 255) & ~size_t(255)) +
          2 * ((rows * 4 + 255) & ~size_t(255)) + ((rows * 8 + 255) & ~size_t(255)) +
-         scan_scratch_bytes(rows) + 1024;
+         scan_scratch_bytes(rows) + 1024 + ((rows * 8 + 255) & ~size_t(255)) + ((rows + 1) * 8 + 511) +
+         scan_scratch_bytes(rows) + 512;
 }
 
 static int jgrid(uint64_t n, const Launch& L) {
@@ -795,6 +807,147 @@ static int cj2_blocks_per_sm(bool seg, int emit) {
                   seg ? cj2_occ<kModeTableWrite, true>() : cj2_occ<kModeTableWrite, false>());
 }
 
+// ---- pivot count kernel ------------------------------------------------------
+//
+// Count-only two-source column join, pivot rows only (join_count marks them):
+// rows (a, ...) whose driver list is the other source's and whose probed
+// list is a's, a long list with a bitmap.  Rows are sorted by a, so the
+// pivot rows of one a form a run: pivot_runs_kernel finds every bitmapped
+// value's run (two binary searches in the table's first column, one thread
+// per value) and splits it into pieces of kPvPiece candidates.  A block (one
+// per SM, 1024 threads) takes pieces in order from a device counter, copies
+// the piece's bitmap into shared memory (again only when the value changes),
+// and its 32 warps walk the piece's candidates as the cj2 kernel does, each
+// candidate a bit test in shared memory instead of a probe of the bitmap in
+// global memory.
+constexpr int kPvThreads = 1024;
+constexpr uint64_t kPvPiece = 1u << 19;  // candidates per piece
+
+// First i in [lo, hi) with a[i] >= x (a sorted).
+__device__ __forceinline__ uint64_t pv_lower(const uint32_t* a, uint64_t lo, uint64_t hi, uint32_t x) {
+  while (lo < hi) {
+    const uint64_t m = lo + (hi - lo) / 2;
+    if (a[m] < x) lo = m + 1;
+    else hi = m;
+  }
+  return lo;
+}
+
+// Per bitmap slot (a bitmapped value v): the rows of v in the table (first
+// column pcol, true row count min(cap, *d_n)), their pivot candidates
+// [cand_lo, cand_hi) and the number of pieces they make.
+__global__ void pivot_runs_kernel(const uint32_t* __restrict__ bdir, uint32_t nv, const uint32_t* __restrict__ pcol,
+                                  uint64_t cap, const uint64_t* __restrict__ d_n, const uint64_t* __restrict__ poffs,
+                                  uint32_t nslots, uint64_t* __restrict__ run_lo, uint64_t* __restrict__ run_hi,
+                                  uint64_t* __restrict__ cand_lo, uint64_t* __restrict__ cand_hi,
+                                  uint64_t* __restrict__ pieces) {
+  const uint64_t nrows = dev_size(cap, d_n);
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+    const uint32_t slot = bdir[v];
+    if (slot == kNoBitmap || slot >= nslots) continue;
+    const uint64_t lo = pv_lower(pcol, 0, nrows, v);
+    const uint64_t hi = pv_lower(pcol, lo, nrows, v + 1);
+    const uint64_t cl = poffs[lo], ch = poffs[hi];
+    run_lo[slot] = lo;
+    run_hi[slot] = hi;
+    cand_lo[slot] = cl;
+    cand_hi[slot] = ch;
+    pieces[slot] = (ch - cl + kPvPiece - 1) / kPvPiece;
+  }
+}
+
+__global__ void __launch_bounds__(kPvThreads, 1) join_pivot_count_kernel(
+    const uint32_t* __restrict__ dvals, const uint64_t* __restrict__ poffs, const uint32_t* __restrict__ beg,
+    const uint64_t* __restrict__ run_lo, const uint64_t* __restrict__ run_hi,
+    const uint64_t* __restrict__ cand_lo, const uint64_t* __restrict__ cand_hi,
+    const uint64_t* __restrict__ piece_offs, uint32_t nslots, const uint32_t* __restrict__ bpool,
+    uint32_t bwords, unsigned long long* __restrict__ queue, unsigned long long* __restrict__ d_out_n) {
+  extern __shared__ __align__(16) uint32_t bm[];
+  __shared__ uint64_t s_c0, s_c1, s_rl, s_rh;
+  __shared__ uint32_t s_slot;
+  __shared__ int s_done;
+  __shared__ unsigned long long s_sum[kPvThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const uint64_t npieces = piece_offs[nslots];
+  uint32_t loaded = kNoBitmap;
+  unsigned long long counted = 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const unsigned long long k = atomicAdd(queue, 1ull);
+      s_done = k >= npieces;
+      if (k < npieces) {
+        // the slot of piece k: the last slot with piece_offs[slot] <= k
+        uint32_t lo = 0, hi = nslots;
+        while (hi - lo > 1) {
+          const uint32_t m = lo + (hi - lo) / 2;
+          if (piece_offs[m] <= k) lo = m;
+          else hi = m;
+        }
+        const uint64_t j = k - piece_offs[lo];
+        const uint64_t c0 = cand_lo[lo] + j * kPvPiece;
+        s_slot = lo;
+        s_c0 = c0;
+        s_c1 = c0 + kPvPiece < cand_hi[lo] ? c0 + kPvPiece : cand_hi[lo];
+        s_rl = run_lo[lo];
+        s_rh = run_hi[lo];
+      }
+    }
+    __syncthreads();
+    if (s_done) break;
+    const uint32_t slot = s_slot;
+    const uint64_t c0 = s_c0, c1 = s_c1, rl = s_rl, rh = s_rh;
+    if (slot != loaded) {
+      // (word loads: a bitmap starts at slot * bwords words, not always on
+      // a 16-byte boundary)
+      const uint32_t* src = bpool + (uint64_t)slot * bwords;
+      for (uint32_t i = threadIdx.x; i < bwords; i += kPvThreads) bm[i] = src[i];
+      __syncthreads();
+      loaded = slot;
+    }
+    // warp wid walks its share of the piece in rounds of 32 candidates; the
+    // row of the round's first candidate is kept while the warp stays in it
+    const uint64_t len = c1 - c0;
+    const uint64_t wb = c0 + len * wid / (kPvThreads / 32);
+    const uint64_t we = c0 + len * (wid + 1) / (kPvThreads / 32);
+    if (wb < we) {
+      uint64_t r0 = warp_partition_point(rl, rh, [&](uint64_t i) { return poffs[i] <= wb; }) - 1;
+      uint64_t crow = ~0ull, c_off = 0, c_end = 0;
+      uint32_t cbeg = 0;
+      for (uint64_t base = wb; base < we; base += 32) {
+        const uint64_t w = base + lane;
+        const bool ok = w < we;
+        if (r0 != crow) {
+          crow = r0;
+          c_off = poffs[r0];
+          c_end = poffs[r0 + 1];
+          cbeg = beg[r0];
+        }
+        uint32_t v = 0;
+        if (base + 31 < c_end) {
+          if (ok) v = dvals[cbeg + (uint32_t)(w - c_off)];
+        } else if (ok) {
+          const uint64_t r = gallop_row(poffs, r0, rh, w);
+          v = dvals[beg[r] + (uint32_t)(w - poffs[r])];
+        }
+        if (ok) counted += (bm[v >> 5] >> (v & 31)) & 1u;
+        // the next round's first row (the row of its first candidate)
+        const uint64_t nb = base + 32;
+        if (nb < we && nb >= c_end) r0 = gallop_row(poffs, r0, rh, nb);
+      }
+    }
+    __syncthreads();  // (the bitmap and s_* are rewritten by the next piece)
+  }
+  // block total -> the level's count
+  const unsigned long long ws = warp_sum(counted);
+  if (lane == 0) s_sum[wid] = ws;
+  __syncthreads();
+  if (wid == 0) {
+    unsigned long long t = lane < kPvThreads / 32 ? s_sum[lane] : 0ull;
+    t = warp_sum(t);
+    if (lane == 0 && t) atomicAdd(d_out_n, t);
+  }
+}
+
 JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scratch& s) {
   JoinWork w;
   uint64_t* work = s.take<uint64_t>(in.n ? in.n : 1);
@@ -804,22 +957,73 @@ JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scrat
   w.orange = s.take<uint2>(in.n ? in.n : 1);
   if (lv.kind == kColumnJoin && lv.nsrc == 2 && !lv.wide && (lv.src[0].t.bdir || lv.src[1].t.bdir))
     w.obm = s.take<uint32_t>(in.n ? in.n : 1);
+  uint64_t* pwork = nullptr;
+  if (w.obm && lv.pivot_src >= 0 && in.n) {
+    pwork = s.take<uint64_t>(in.n);
+    w.poffs = s.take<uint64_t>(in.n + 1);
+  }
   if (in.n) {
     join_count_kernel<<<jgrid(in.n, L), kJThreads, 0, L.stream>>>(lv, in, work, w.drv,
-                                                                          w.beg, w.orange, w.obm);
+                                                                          w.beg, w.orange, w.obm, pwork);
     SRDL_CUDA(cudaGetLastError());
     count_launches(1);
   }
   exclusive_scan_u64(L, work, in.n, w.offs, s);
+  if (pwork) exclusive_scan_u64(L, pwork, in.n, w.poffs, s);
   return w;
+}
+
+size_t join_pivot_smem_bytes(uint32_t bwords) { return (size_t)bwords * 4; }
+
+size_t join_pivot_scratch_bytes(uint32_t nslots) {
+  return 7 * ((size_t)(nslots + 1) * 8 + 511) + scan_scratch_bytes(nslots) + 2048;
+}
+
+// The pivot rows' count (count mode; w.poffs set): the runs of the
+// bitmapped values, their pieces, then one block per SM over the pieces.
+static void join_pivot_count(const Launch& L, const LevelSpec& lv, const Table& in, const JoinWork& w,
+                             unsigned long long* d_out_n, Scratch& s) {
+  const int ps = lv.pivot_src, ds = 1 - ps;
+  const SrcSpec& P = lv.src[ps];
+  const SrcSpec& D = lv.src[ds];
+  const uint32_t* dvals = D.prefix_slot < 0 ? D.t.roots : D.t.lo;
+  const uint32_t nslots = lv.pivot_slots;
+  if (!nslots || !P.t.dir_n) return;
+  const size_t smem = join_pivot_smem_bytes(P.t.bwords);
+  static size_t attr = 0;
+  if (smem > attr) {
+    SRDL_CUDA(cudaFuncSetAttribute(join_pivot_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    attr = smem;
+  }
+  uint64_t* run_lo = s.take<uint64_t>(nslots);
+  uint64_t* run_hi = s.take<uint64_t>(nslots);
+  uint64_t* cand_lo = s.take<uint64_t>(nslots);
+  uint64_t* cand_hi = s.take<uint64_t>(nslots);
+  uint64_t* pieces = s.take<uint64_t>(nslots);
+  uint64_t* piece_offs = s.take<uint64_t>(nslots + 1);
+  unsigned long long* q = s.take<unsigned long long>(1);
+  SRDL_CUDA(cudaMemsetAsync(pieces, 0, nslots * 8, L.stream));
+  SRDL_CUDA(cudaMemsetAsync(q, 0, sizeof(unsigned long long), L.stream));
+  const uint32_t nv = P.t.dir_n - 1;
+  pivot_runs_kernel<<<(int)std::min<uint64_t>((nv + 255) / 256, (uint64_t)L.num_sms * 8), 256, 0, L.stream>>>(
+      P.t.bdir, nv, in.col[P.prefix_slot], in.n, in.d_n, w.poffs, nslots, run_lo, run_hi, cand_lo, cand_hi,
+      pieces);
+  exclusive_scan_u64(L, pieces, nslots, piece_offs, s);
+  join_pivot_count_kernel<<<L.num_sms, kPvThreads, smem, L.stream>>>(
+      dvals, w.poffs, w.beg, run_lo, run_hi, cand_lo, cand_hi, piece_offs, nslots, P.t.bpool, P.t.bwords, q,
+      d_out_n);
+  SRDL_CUDA(cudaGetLastError());
+  count_launches(2);
 }
 
 void join_expand(const Launch& L, const LevelSpec& lv, const Table& in, const JoinWork& w,
                  uint64_t total, Table* out_table, uint64_t* out_keys, uint64_t* d_out_n,
                  Scratch& s, const JoinDev* dev) {
+  auto* cnt = reinterpret_cast<unsigned long long*>(d_out_n);
+  if (w.poffs && lv.emit == kEmitCount) join_pivot_count(L, lv, in, w, cnt, s);
   if (total == 0) return;
   const JoinDev jd = dev ? *dev : JoinDev{};
-  auto* cnt = reinterpret_cast<unsigned long long*>(d_out_n);
   const int g = jgrid(total, L);
   const uint64_t warps = (uint64_t)g * (kJThreads / 32);
   const uint64_t chunk = ((total + warps - 1) / warps + 31) & ~uint64_t(31);

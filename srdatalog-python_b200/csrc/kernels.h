@@ -247,6 +247,14 @@ struct LevelSpec {
   const uint32_t* grp_bounds = nullptr;  // n_groups + 1 sorted entries
   uint32_t n_groups = 0;
   unsigned long long* grp_counts = nullptr;
+  // Count-only two-source column joins: rows whose driver is the other
+  // source's list and whose probed list -- source pivot_src's, indexed by
+  // the table's first (sorted) column -- has a bitmap and at least
+  // pivot_min values are counted by the pivot kernel (the bitmap of the
+  // rows' common first value held in shared memory) instead of cj2.
+  int pivot_src = -1;
+  uint32_t pivot_min = 0;
+  uint32_t pivot_slots = 0;  // bitmaps of the pivot source
   // Sharded work: expand only segments seg_rank, seg_rank + seg_world, ...
   // of `seg` work items each (seg a multiple of 32; 0: every item).
   uint64_t seg = 0;
@@ -270,8 +278,16 @@ struct JoinWork {
   uint32_t* beg = nullptr;   // column join: driver list begin per row
   uint2* orange = nullptr;   // two-source column join: the other list [x, y) per row
   uint32_t* obm = nullptr;   // two-source column join: bitmap slot of the other list, or kNoBitmap
+  uint64_t* poffs = nullptr; // pivot rows (lv.pivot_src): prefix sums of their candidates, rows + 1
 };
 JoinWork join_count(const Launch& L, const LevelSpec& lv, const Table& in, Scratch& s);
+
+// Shared memory the pivot kernel needs for one bitmap of `bwords` words;
+// levels whose bitmaps need more than kPivotSmemMax keep the cj2 kernel.
+size_t join_pivot_smem_bytes(uint32_t bwords);
+// Scratch the pivot pass adds to a level's expand scratch.
+size_t join_pivot_scratch_bytes(uint32_t nslots);
+constexpr size_t kPivotSmemMax = 200 * 1024;
 
 // Pass 2: expands `total` work items (all of the count pass's items, or
 // with lv.seg set this shard's segments of them, total = seg_owned(...));

@@ -936,6 +936,9 @@ void Database::set_option(const std::string& name, int64_t value) {
   } else if (name == "join_blocks_per_sm") {
     SRDL_REQUIRE(value >= 1 && value <= 64, kErrArg, "set_option: join_blocks_per_sm out of [1, 64]");
     L_.join_bpsm = (int)value;
+  } else if (name == "pivot_min") {
+    SRDL_REQUIRE(value >= 0 && value <= (1ll << 32), kErrArg, "set_option: pivot_min out of [0, 2^32]");
+    opt_pivot_min_ = value;
   }
   else throw Error{kErrArg, "set_option: unknown option " + name};
 }
@@ -1028,6 +1031,7 @@ TrieView Database::view2(Index& ix) {
   t.bdir = ix.bdir.bytes() ? ix.bdir.as<uint32_t>() : nullptr;
   t.bpool = ix.bpool.bytes() ? ix.bpool.as<uint32_t>() : nullptr;
   t.bwords = ix.bwords;
+  t.bslots = ix.bwords ? (uint32_t)(ix.bpool.bytes() / ((size_t)ix.bwords * 4)) : 0;
   t.n = ix.n;
   t.n_roots_d = ix.nroots_d.as<uint64_t>();
   t.dir_n = ix.dir_n;
@@ -1090,6 +1094,7 @@ TrieView Database::view(Relation& r, Index& ix) {
   t.bdir = ix.bdir.bytes() ? ix.bdir.as<uint32_t>() : nullptr;
   t.bpool = ix.bpool.bytes() ? ix.bpool.as<uint32_t>() : nullptr;
   t.bwords = ix.bwords;
+  t.bslots = ix.bwords ? (uint32_t)(ix.bpool.bytes() / ((size_t)ix.bwords * 4)) : 0;
   t.n = ix.n;
   t.n_roots_d = ix.nroots_d.as<uint64_t>();
   t.dir_n = ix.dir_n;

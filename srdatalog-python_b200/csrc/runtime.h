@@ -339,6 +339,7 @@ class Database {
   int64_t opt_hash_min_ = -1;       // -1: SRDL_HASH_MIN or off
   int64_t opt_lsm_pct_ = 10;        // HEAD -> FULL merge threshold (% of FULL)
   uint64_t opt_mem_limit_ = 0;      // bytes a run may hold on the device (0: no limit)
+  int64_t opt_pivot_min_ = 0;       // count joins: shortest bitmapped list the pivot kernel takes (0: off)
   ArenaUse mem_run_{};              // the last run's arena use (peak: its most held)
   int64_t shard_rank_ = 0, shard_world_ = 1;  // this database's shard among shard_world_
   srdl_exchange_fn xfn_ = nullptr;  // moves tuples between shards (exchange ops)

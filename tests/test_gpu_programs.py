@@ -147,6 +147,20 @@ def test_library_hash_matches_oracle(expected):
   assert t.hash('Knows') == oracle.dump_hash(t.dump('Knows'))
 
 
+@pytest.mark.parametrize('pivot_min', [512, 4096])
+def test_triangle_pivot_kernel(expected, pivot_min):
+  '''The pivot kernel (option pivot_min: rows probing a long bitmapped list
+  of the table's first column counted with that bitmap in shared memory)
+  gives the same counts as the default path, on R-MAT scale 14 and 20.'''
+  for name, scale, draws, seed in (('triangle_rmat14', 14, 1 << 18, 5), ('triangle_rmat20', 20, 1 << 24, 3)):
+    e = W.rmat_edges(scale, draws, seed=seed)
+    db = native.Database(load_plan('triangle'))
+    db.set_option('pivot_min', pivot_min)
+    db.load_rows('KnowsInput', e)
+    db.run()
+    assert db.count('TriangleJoin') == expected[name]['count'], name
+
+
 def test_triangle_large_ids_sparse_path():
   '''Ids spread over the whole uint32 range leave the dense directory (and the
   hashed child lists) unused: lookups binary-search the keys.  Relabelling
