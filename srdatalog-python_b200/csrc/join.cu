@@ -454,6 +454,33 @@ __global__ void __launch_bounds__(kJThreads) join_cj2_kernel(
         crg = orange[r0];
         cslot = obm ? obm[r0] : kNoBitmap;
       }
+      if (MODE == kModeCount && !SEG && abase + 63 < c_end && base + 63 < c1 && !lv.grp_bounds) {
+        // count only: two rounds at once while both lie in the cached row,
+        // so each lane has two independent loads and probes in flight
+        auto probe = [&](uint32_t x) -> bool {
+          const uint32_t* odir = cd == 0 ? dir1 : dir0;
+          if (odir) {
+            const uint32_t odn = cd == 0 ? dn1 : dn0;
+            return x + 1u < odn && odir[x] < odir[x + 1];
+          }
+          if (cslot != kNoBitmap) {
+            const uint32_t* bm = cd == 0 ? bp1 : bp0;
+            const uint32_t bw = cd == 0 ? bw1 : bw0;
+            return (bm[(uint64_t)cslot * bw + (x >> 5)] >> (x & 31)) & 1u;
+          }
+          const uint32_t* ov = cd == 0 ? vals1 : vals0;
+          const uint32_t p = lower_bound_bf(ov, crg.x, crg.y, x);
+          return p < crg.y && ov[p] == x;
+        };
+        const uint32_t* dv = cd == 0 ? vals0 : vals1;
+        const uint32_t i0 = cbeg + (uint32_t)(w - c_off);
+        const uint32_t va = dv[i0], vb = dv[i0 + 32];
+        const bool oa = probe(va), ob = probe(vb);
+        running += __popc(__ballot_sync(kAllLanes, oa)) + __popc(__ballot_sync(kAllLanes, ob));
+        base += 32;  // (the loop adds the second round's 32)
+        sw.next();
+        continue;    // r0 stays: both rounds lie in its row
+      }
       if (abase + 31 < c_end) {
         if (ok) {
           v = (cd == 0 ? vals0 : vals1)[cbeg + (uint32_t)(w - c_off)];
