@@ -441,6 +441,25 @@ void Database::exec_pipeline(const Op& op, bool recursive, uint64_t iteration) {
         for (int c = 0; c < target->arity; c++) lv.key_slot[c] = pp.key_slot[c];
         Chunk ch;
         ch.order = pp.insert->index;
+        if (levels.size() == 1 && lv.kind == kScan && lv.nsrc == 1 && !lv.wide && lv.src[0].prefix_slot < 0 &&
+            lv.nfilt == 0 && !sharded && target->arity == 2 && lv.src[0].t.arity == 2 && lv.src[0].t.keys &&
+            pp.key_slot[0] == lv.scan_slot[0] && pp.key_slot[1] == lv.scan_slot[1]) {
+          // A rule that copies a whole binary index in its own column order
+          // (Knows(x,y) <= KnowsInput(x,y)): the keys are that index's,
+          // already sorted and unique -- copied, and never sorted again.
+          const uint64_t nk = lv.src[0].t.n;
+          ch.keys = DevBuf(std::max<uint64_t>(nk, 1) * 8, L_.stream);
+          pid = prof_begin("join_expand_keys");
+          if (nk)
+            SRDL_CUDA(cudaMemcpyAsync(ch.keys.as<void>(), lv.src[0].t.keys, nk * 8, cudaMemcpyDeviceToDevice,
+                                      L_.stream));
+          prof_end(pid, 16.0 * nk, (double)nk);
+          ch.n = nk;
+          ch.sorted = true;
+          derived_ += ch.n;
+          target->v[kNew].chunks.push_back(std::move(ch));
+          break;
+        }
         ch.keys = DevBuf(std::max<uint64_t>(total, 1) * 8, L_.stream);
         pid = prof_begin("join_expand_keys");
         join_expand(L_, lv, cur, w, total, nullptr, ch.keys.as<uint64_t>(),
@@ -533,6 +552,40 @@ void Database::op_rebuild(const Step& st, size_t pos, const Op& op) {
       if (o.kind == Op::Clear && o.rel == op.rel && o.ver == kDelta) continue;
       break;
     }
+  }
+  if (rv.chunks.size() == 1 && rv.chunks[0].sorted && rv.chunks[0].order == op.index && r.arity <= 2 &&
+      !(r.lsm && r.head.n)) {
+    // a copied index: sorted and unique already
+    Chunk& c = rv.chunks[0];
+    Index fresh;
+    fresh.n = c.n;
+    if (fuse && r.v[kFull].has_index()) {
+      const Index& full = r.lsm ? full_base(r, op.index) : ensure_index(r, kFull, op.index);
+      fresh.keys = DevBuf(std::max<uint64_t>(c.n, 1) * 8, L_.stream);
+      if (full.n && c.n) {
+        DevBuf ds(diff_scratch_bytes(c.n) + 1024, L_.stream);
+        Scratch s2{ds.as<char>(), ds.bytes(), 0};
+        size_t pid = prof_begin("sort_dedup_diff");
+        set_difference(L_, c.keys.as<uint64_t>(), c.n, full.keys.as<uint64_t>(), full.n,
+                       fresh.keys.as<uint64_t>(), d_small_.as<uint64_t>(), s2);
+        fresh.n = read_scalar(0);
+        prof_end(pid, 8.0 * (c.n + full.n + fresh.n), (double)c.n);
+      } else if (c.n) {
+        SRDL_CUDA(cudaMemcpyAsync(fresh.keys.as<void>(), c.keys.as<void>(), c.n * 8, cudaMemcpyDeviceToDevice,
+                                  L_.stream));
+      }
+    } else {
+      fresh.keys = std::move(c.keys);
+    }
+    rv.chunks.clear();
+    rv.idx.clear();
+    if (fuse) {
+      r.pending = std::move(fresh);
+      r.pending_delta = true;
+    } else {
+      rv.idx[op.index] = std::move(fresh);
+    }
+    return;
   }
   if (fuse) {
     const Index* full = nullptr;

@@ -107,6 +107,7 @@ struct Chunk {
   DevBuf keys;
   uint64_t n = 0;
   std::vector<int> order;  // index permutation the keys are packed in
+  bool sorted = false;     // already sorted and unique in `order` (a copied index)
 };
 
 struct RelVersion {
