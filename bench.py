@@ -280,7 +280,8 @@ def cpu_baseline(wl_name: str, edges, n_max: int = WIDE_N_MAX) -> dict:
     dt = time.perf_counter() - t0
     value = keys.shape[0] / dt
     sample = f'full fixpoint ({dt:.2f} s, {keys.shape[0]} tuples)'
-  return {'value': value, 'unit': 'tuples/s', 'cores': cores, 'kind': 'port', 'sample': sample}
+  return {'value': value, 'unit': 'tuples/s', 'cores': cores, 'kind': 'port', 'sample': sample,
+          'seconds': dt}
 
 
 def run_reference(args, rank, world):
@@ -290,17 +291,21 @@ def run_reference(args, rank, world):
   if args.workload == 'batched-wide':
     wl = dict(wl, desc=wl['desc'].format(n_max=args.batch_n_max))
   edges = None if args.workload in ('served', 'batched', 'batched-wide') else make_edges(args.workload)
-  vals = []
+  vals, secs = [], []
   for i in range(args.warmup + args.steps):
     cb = cpu_baseline(args.workload, edges, args.batch_n_max)
     if i >= args.warmup:
       vals.append(cb['value'])
+      if 'seconds' in cb:  # a step is one whole run (triangle, tc, sg)
+        secs.append(cb.pop('seconds'))
   v = statistics.median(vals)
   cb['value'] = v
+  cb.pop('seconds', None)
   unit = cb['unit']
   line = {'impl': 'reference', 'metric': f'{unit} ({args.workload})', 'value': v,
           'unit': unit, 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
-          'ms_per_step': None, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+          'ms_per_step': statistics.median(secs) * 1e3 if secs else None,
+          'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
           'dtype': 'u32', 'data': 'synthetic',
           'config': {'workload': wl['desc']}, 'cpu_baseline': cb,
           'e2e': {'value': v, 'unit': unit, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
@@ -925,6 +930,7 @@ def main():
     line['config']['autotuned'] = dict(tuned.to_json(), trials=len(tuned.trials))
   if world == 1 and not args.no_cpu_baseline:
     line['cpu_baseline'] = cpu_baseline(args.workload, edges)
+    line['cpu_baseline'].pop('seconds', None)
   print(json.dumps(line), flush=True)
 
 
