@@ -85,7 +85,25 @@ __global__ void __launch_bounds__(kRsThreads) rs_hist(const K* __restrict__ keys
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = begin + chunk < n ? begin + chunk : n;
   const uint32_t mask = nbins - 1;
-  for (uint64_t i = begin + threadIdx.x; i < end; i += kRsThreads)
+  // 16-byte loads: the chunk starts a multiple of kRsTile keys into a
+  // 256-byte aligned array; a ragged tail is read key by key.
+  constexpr uint64_t kPer = 16 / sizeof(K);
+  const uint64_t vend = begin < end ? begin + (end - begin) / kPer * kPer : begin;
+  const uint4* vec = reinterpret_cast<const uint4*>(keys + begin);
+  for (uint64_t q = threadIdx.x; begin + q * kPer < vend; q += kRsThreads) {
+    const uint4 v = __ldg(vec + q);
+    if constexpr (sizeof(K) == 8) {
+      const uint64_t k0 = ((uint64_t)v.y << 32) | v.x, k1 = ((uint64_t)v.w << 32) | v.z;
+      atomicAdd(&h[(uint32_t)(k0 >> shift) & mask], 1u);
+      atomicAdd(&h[(uint32_t)(k1 >> shift) & mask], 1u);
+    } else {
+      atomicAdd(&h[(v.x >> shift) & mask], 1u);
+      atomicAdd(&h[(v.y >> shift) & mask], 1u);
+      atomicAdd(&h[(v.z >> shift) & mask], 1u);
+      atomicAdd(&h[(v.w >> shift) & mask], 1u);
+    }
+  }
+  for (uint64_t i = vend + threadIdx.x; i < end; i += kRsThreads)
     atomicAdd(&h[(uint32_t)(keys[i] >> shift) & mask], 1u);
   __syncthreads();
   for (int d = threadIdx.x; d < nbins; d += kRsThreads) counts[(uint64_t)d * gridDim.x + blockIdx.x] = h[d];
